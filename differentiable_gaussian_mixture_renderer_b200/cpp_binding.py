@@ -1,0 +1,139 @@
+"""The reference's torch extension surface, over the C ABI.
+
+Mirrors ``cpp_binding.forward`` / ``cpp_binding.backward`` of
+python_bindings/vol_marcher.cu:217-304: same argument order and meaning, same
+13-entry cache (vol_marcher.cu:109-122), same gradient list.  Differences,
+all deliberate:
+
+* errors raise (TypeError / ValueError / DgmrError) instead of printing and
+  returning an empty list (vol_marcher.cu:253-255);
+* an empty frame (no visible Gaussian) renders the background and returns a
+  valid cache with an empty point list, where the reference returns undefined
+  cache tensors and a zero image (vol_marcher_forward.cu:194-195);
+* SH coefficients are not concatenated to 16 on the device: the kernels read
+  coefficients past the caller's count as 0 (forward) / 1 (backward), the
+  values the reference pads with (vol_marcher.cu:92, :177).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+def _f32(v: float) -> float:
+    # the reference's binding takes tan_fov as C float (vol_marcher.cu:228-229)
+    return float(np.float32(v))
+
+
+def _check_inputs(tensors, names):
+    dt = tensors[0].dtype
+    for t, n in zip(tensors, names):
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"{n} must be a torch.Tensor")
+        if t.dtype != dt:
+            raise TypeError("All input vectors must be of the same type (float32 or float64)")
+    if dt not in (torch.float32, torch.float64):
+        raise TypeError("All input vectors must be of the same type (float32 or float64)")
+    dev = tensors[0].device
+    if dev.type != "cuda":
+        raise ValueError("vol_marcher runs on CUDA tensors only")
+    for t, n in zip(tensors[:5], names[:5]):
+        if t.device != dev:
+            raise ValueError(f"{n} is on {t.device}, expected {dev}")
+    return dt, dev
+
+
+def _contig(t):
+    return t if t.is_contiguous() else t.contiguous()
+
+
+def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
+            background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int):
+    names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
+             "cam_position", "background")
+    dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
+                             cam_position, background], names)
+    lib = N.lib()
+    W, H = int(render_width), int(render_height)
+    n = int(weights.shape[0])
+    sh_params, weights, centroids = _contig(sh_params), _contig(weights), _contig(centroids)
+    cov_scales, cov_rotations = _contig(cov_scales), _contig(cov_rotations)
+    with torch.cuda.device(dev):
+        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree)
+        cam = N.make_camera(view_matrix, proj_matrix, cam_position, background, W, H, _f32(tan_fovx), _f32(tan_fovy))
+        gx, gy = (W + 15) // 16, (H + 15) // 16
+        opt = dict(device=dev)
+        cache = [torch.empty((3, H, W), dtype=dt, **opt),
+                 torch.empty((n, 2), dtype=torch.int32, **opt),
+                 torch.empty((n, 3), dtype=dt, **opt),
+                 torch.empty((n, 3), dtype=torch.bool, **opt),
+                 torch.empty((n,), dtype=dt, **opt),
+                 torch.empty((n, 2), dtype=dt, **opt),
+                 torch.empty((n, 6), dtype=dt, **opt),
+                 torch.empty((n,), dtype=dt, **opt),
+                 torch.empty((n,), dtype=torch.int32, **opt),
+                 torch.empty((n,), dtype=torch.int32, **opt),
+                 torch.empty((gx * gy, 2), dtype=torch.int32, **opt),
+                 None,
+                 torch.empty((H, W), dtype=dt, **opt)]
+        c = N.VmCache(*[N.ptr(t) for t in cache])
+        stream = N.stream_handle()
+        dcode = N.dtype_code(dt)
+        ws_pre = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, 0, dcode), dtype=torch.uint8, **opt)
+        N.check(lib.dgmr_vm_forward_preprocess(scene, cam, c, N.ptr(ws_pre), ws_pre.numel(), None, stream),
+                "vol_marcher forward preprocess")
+        # the pair count sizes b_point_list, as in the reference (.item(), vol_marcher_forward.cu:193)
+        n_pairs = int(cache[9][-1].item()) if n > 0 else 0
+        cache[11] = torch.empty((n_pairs,), dtype=torch.int32, **opt)
+        c.b_point_list = N.ptr(cache[11]) if n_pairs > 0 else None
+        ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, n_pairs, dcode), dtype=torch.uint8, **opt)
+        N.check(lib.dgmr_vm_forward_render(scene, cam, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
+                "vol_marcher forward render")
+    return cache
+
+
+def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
+             background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
+             grad_framebuffer, cache_vector):
+    names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
+             "cam_position", "background")
+    dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
+                             cam_position, background], names)
+    if grad_framebuffer.dtype != dt:
+        raise TypeError("grad_framebuffer must have the inputs' dtype")
+    lib = N.lib()
+    W, H = int(render_width), int(render_height)
+    n = int(weights.shape[0])
+    sh_params, weights, centroids = _contig(sh_params), _contig(weights), _contig(centroids)
+    cov_scales, cov_rotations = _contig(cov_scales), _contig(cov_rotations)
+    grad_framebuffer = _contig(grad_framebuffer)
+    cache = [_contig(t) if t is not None else None for t in cache_vector]
+    with torch.cuda.device(dev):
+        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree)
+        cam = N.make_camera(view_matrix, proj_matrix, cam_position, background, W, H, _f32(tan_fovx), _f32(tan_fovy))
+        opt = dict(device=dev, dtype=dt)
+        k = int(sh_params.shape[1])
+        g_sh = torch.empty((n, k, 3), **opt)
+        g_w = torch.empty((n, 1), **opt)
+        g_mu = torch.empty((n, 3), **opt)
+        g_s = torch.empty((n, 3), **opt)
+        g_q = torch.empty((n, 4), **opt)
+        c = N.VmCache(*[N.ptr(t) if (t is not None and t.numel() > 0) else None for t in cache])
+        if c.b_point_list is None:
+            c.b_point_list = N.ptr(cache[9])  # never read: the tile ranges are all empty
+        ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, 0, N.dtype_code(dt)), dtype=torch.uint8, device=dev)
+        N.check(lib.dgmr_vm_backward(scene, cam, c, N.ptr(grad_framebuffer), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
+                                     N.ptr(g_s), N.ptr(g_q), N.ptr(ws), ws.numel(), None, N.stream_handle()),
+                "vol_marcher backward")
+    return [g_sh, g_w, g_mu, g_s, g_q]
+
+
+def set_const_samples(sections) -> None:
+    """Gradient-check mode (the reference's DGMR_TORCH_GRAD_CHECK_CONST_SAMPLES):
+    fixed (start, end, delta_t) sample sections; [] restores adaptive sampling."""
+    arr = np.ascontiguousarray(np.asarray(sections, dtype=np.float64).reshape(-1))
+    lib = N.load()
+    N.check(lib.dgmr_vm_set_const_samples(len(sections), arr.ctypes.data if arr.size else None),
+            "set_const_samples")

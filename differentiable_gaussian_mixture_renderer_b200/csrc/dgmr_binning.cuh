@@ -1,0 +1,185 @@
+// Tile binning shared by the splat renderer and the volume marcher.
+//
+// The reference emits one 64-bit key (tile << 32 | float bits of depth) per
+// (tile, Gaussian) pair and radix-sorts all pairs over 32 + msb(tiles) bits
+// (splat_forward.cu:222-274).  The sorted order it produces is the order of
+// (tile, depth bits, Gaussian index).  Here the same order is reached with
+// far less traffic: the N Gaussians are stably sorted once by their 32-bit
+// depth bits (N << pairs), pairs are emitted in that depth order, and a
+// stable sort over only the msb(tiles) tile bits finishes the job.  The
+// result -- point list and tile ranges -- is identical bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dgmr_device_math.cuh"
+#include "dgmr_sort.cuh"
+
+namespace dgmr {
+
+// util.h:56-70: next-highest bit of the MSB
+inline uint32_t higher_msb(uint32_t n)
+{
+    uint32_t msb = sizeof(n) * 4;
+    uint32_t step = msb;
+    while (step > 1) {
+        step /= 2;
+        if (n >> msb)
+            msb += step;
+        else
+            msb -= step;
+    }
+    if (n >> msb)
+        msb++;
+    return msb;
+}
+
+inline size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
+
+// Linear workspace carving with 256-byte alignment.
+struct Carver {
+    size_t off = 0;
+    char* base = nullptr;
+    template <class P>
+    P* take(size_t count)
+    {
+        const size_t o = off;
+        off = align_up(off + count * sizeof(P));
+        return base ? reinterpret_cast<P*>(base + o) : nullptr;
+    }
+};
+
+// Scratch of the binning stage.
+struct BinningBuffers {
+    uint32_t* depth_key; // [N]
+    uint32_t* perm; // [N]  (holds iota on entry, the depth order on exit)
+    uint32_t* key_tmp; // [N]
+    uint32_t* perm_tmp; // [N]
+    uint32_t* cnt_sorted; // [N]
+    uint32_t* off_sorted; // [N]
+    uint32_t* pair_tile[2]; // [cap]
+    uint32_t* pair_val[2]; // [cap]
+    uint32_t* scan_tmp; // scan_temp_bytes(N)
+    void* sort_tmp; // radix_temp_bytes(max(N, cap))
+    uint32_t* n_sort; // [1] pairs to sort = min(P, cap)
+};
+
+inline void carve_binning(Carver& c, BinningBuffers& b, uint32_t N, uint32_t cap)
+{
+    b.depth_key = c.take<uint32_t>(N);
+    b.perm = c.take<uint32_t>(N);
+    b.key_tmp = c.take<uint32_t>(N);
+    b.perm_tmp = c.take<uint32_t>(N);
+    b.cnt_sorted = c.take<uint32_t>(N);
+    b.off_sorted = c.take<uint32_t>(N);
+    for (int i = 0; i < 2; ++i) {
+        b.pair_tile[i] = c.take<uint32_t>(cap);
+        b.pair_val[i] = c.take<uint32_t>(cap);
+    }
+    b.scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
+    b.sort_tmp = c.take<char>(radix_temp_bytes(N > cap ? N : cap));
+    b.n_sort = c.take<uint32_t>(4);
+}
+
+// parity of the buffer that holds the tile-sorted pairs
+inline int tile_sort_parity(uint32_t n_tiles)
+{
+    const int bits = int(higher_msb(n_tiles));
+    return ((bits + 7) / 8) & 1;
+}
+
+static __global__ void k_pair_count(const uint32_t* __restrict__ point_offsets, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, uint32_t* __restrict__ n_sort)
+{
+    const uint32_t P = N ? point_offsets[N - 1] : 0u;
+    stats[0] = P;
+    if (P > cap)
+        atomicOr(&stats[1], 1u);
+    *n_sort = P < cap ? P : cap;
+}
+
+static __global__ void k_gather_counts(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tiles_touched, uint32_t N, uint32_t* __restrict__ cnt_sorted)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < N)
+        cnt_sorted[j] = tiles_touched[perm[j]];
+}
+
+// Pairs in depth order: for the j-th Gaussian by depth, one entry per tile
+// its rectangle touches (util.h:42-52 applied to the cached rect + centroid).
+template <class T>
+static __global__ void k_emit_pairs(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ cnt_sorted, const uint32_t* __restrict__ off_sorted,
+    const int32_t* __restrict__ rects, const T* __restrict__ xy, uint32_t N, unsigned gx, unsigned gy, uint32_t cap, uint32_t* __restrict__ pair_tile,
+    uint32_t* __restrict__ pair_val)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N)
+        return;
+    const uint32_t c = cnt_sorted[j];
+    if (c == 0)
+        return;
+    const uint32_t g = perm[j];
+    uint32_t off = off_sorted[j] - c;
+    const TileRect r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], gx, gy);
+    for (unsigned y = r.y0; y < r.y1; ++y)
+        for (unsigned x = r.x0; x < r.x1; ++x) {
+            if (off < cap) {
+                pair_tile[off] = y * gx + x;
+                pair_val[off] = g;
+            }
+            ++off;
+        }
+}
+
+// splat_forward.cu:281-302 on the tile-sorted list (ranges zeroed beforehand)
+static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, const uint32_t* __restrict__ n_dev, int32_t* __restrict__ ranges)
+{
+    const uint32_t n = *n_dev;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const uint32_t cur = tiles_sorted[idx];
+        if (idx == 0)
+            ranges[2 * cur] = 0;
+        else {
+            const uint32_t prev = tiles_sorted[idx - 1];
+            if (cur != prev) {
+                ranges[2 * prev + 1] = int32_t(idx);
+                ranges[2 * cur] = int32_t(idx);
+            }
+        }
+        if (idx == n - 1)
+            ranges[2 * cur + 1] = int32_t(n);
+    }
+}
+
+// Full binning: point_offsets (inclusive scan, reference order), depth sort,
+// emission, tile sort and ranges.  Returns the buffer index holding the
+// sorted (tile, Gaussian) pairs.  Requires b.perm = iota and b.depth_key
+// filled by the preprocess.
+template <class T>
+inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* tiles_touched, uint32_t* point_offsets, const int32_t* rects, const T* xy,
+    uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s)
+{
+    const uint32_t n_tiles = gx * gy;
+    cudaMemsetAsync(ranges, 0, size_t(n_tiles) * 2 * sizeof(int32_t), s);
+    if (N == 0) {
+        cudaMemsetAsync(b.n_sort, 0, sizeof(uint32_t), s);
+        return tile_sort_parity(n_tiles);
+    }
+    inclusive_scan_u32(tiles_touched, point_offsets, N, b.scan_tmp, s);
+    k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
+    const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s);
+    const uint32_t* perm = dpar ? b.perm_tmp : b.perm;
+    const uint32_t blocks = (N + 255) / 256;
+    k_gather_counts<<<blocks, 256, 0, s>>>(perm, tiles_touched, N, b.cnt_sorted);
+    inclusive_scan_u32(b.cnt_sorted, b.off_sorted, N, b.scan_tmp, s);
+    k_emit_pairs<T><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, gx, gy, cap, b.pair_tile[0], b.pair_val[0]);
+    const int bits = int(higher_msb(n_tiles));
+    const int par = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort, 0, cap, bits, b.sort_tmp, n_sms, s);
+    if (cap > 0) {
+        const uint32_t want = (cap + 255) / 256, limit = uint32_t(n_sms) * 16;
+        k_tile_ranges<<<want < limit ? want : limit, 256, 0, s>>>(b.pair_tile[par], b.n_sort, ranges);
+    }
+    return par;
+}
+
+} // namespace dgmr

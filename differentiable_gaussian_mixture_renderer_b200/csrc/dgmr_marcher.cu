@@ -1,0 +1,771 @@
+// Volume ray marcher: forward (src/dgmr/vol_marcher_forward.cu:42-503) and
+// backward (src/dgmr/vol_marcher_backward.cu:53-386), float and double,
+// behind the C ABI of include/dgmr_b200.h.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dgmr_b200.h"
+#include "dgmr_abi_common.h"
+#include "dgmr_binning.cuh"
+#include "dgmr_device_grad.cuh"
+#include "dgmr_marching.cuh"
+
+namespace dgmr {
+
+template <class T>
+struct ConstSamplesT {
+    int n;
+    T s[4][3];
+};
+
+static ConstSamplesT<double> g_const_samples = { 0, {} };
+
+template <class T>
+inline ConstSamplesT<T> const_samples()
+{
+    ConstSamplesT<T> c;
+    c.n = g_const_samples.n;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 3; ++j)
+            c.s[i][j] = T(g_const_samples.s[i][j]);
+    return c;
+}
+
+// Workspace: [stats | preprocess scan scratch | backward accumulators |
+// binning].  The first two come first so the preprocess can run on a
+// workspace sized for pair_capacity = 0, before the pair count is known.
+template <class T>
+struct VmLayout {
+    uint32_t* stats;
+    uint32_t* pre_scan_tmp;
+    T* acc; // [N,10]: mass, rgb(3), inverse covariance(6)
+    BinningBuffers bin;
+    size_t pre_bytes;
+    size_t bytes;
+};
+
+template <class T>
+inline VmLayout<T> vm_layout(uint32_t N, uint32_t cap, void* base)
+{
+    VmLayout<T> L;
+    Carver c;
+    c.base = static_cast<char*>(base);
+    L.stats = c.take<uint32_t>(4);
+    L.pre_scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
+    L.pre_bytes = c.off;
+    L.acc = c.take<T>(size_t(N) * 10);
+    carve_binning(c, L.bin, N, cap);
+    L.bytes = c.off;
+    return L;
+}
+
+// depth keys (float bits of the cached depth) and the identity permutation
+template <class T>
+__global__ void k_depth_keys(const T* __restrict__ depths, uint32_t N, uint32_t* __restrict__ depth_key, uint32_t* __restrict__ perm)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) {
+        depth_key[i] = __float_as_uint(float(depths[i]));
+        perm[i] = i;
+    }
+}
+
+template <class T>
+struct VmPre {
+    uint32_t N;
+    const T* centroids;
+    const T* sh;
+    int sh_stride, sh_degree;
+    const T* weights;
+    const T* scales;
+    const T* rotations;
+    int32_t* rects;
+    T* rgb;
+    uint8_t* clamped;
+    T* depths;
+    T* xy;
+    T* inv_cov;
+    T* masses;
+    uint32_t* tiles_touched;
+    T aa; // filter_kernel_SD * 2 * tan_fovx / width
+};
+
+// vol_marcher_forward.cu:98-176
+template <class T>
+__global__ void __launch_bounds__(128) k_vm_preprocess(VmPre<T> p, CameraT<T> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N)
+        return;
+    p.tiles_touched[i] = 0;
+    p.rects[2 * i] = 0;
+    p.rects[2 * i + 1] = 0;
+    p.xy[2 * i] = T(0);
+    p.xy[2 * i + 1] = T(0);
+    p.depths[i] = T(0);
+    p.masses[i] = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p.rgb[3 * i + k] = T(0);
+        p.clamped[3 * i + k] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        p.inv_cov[6 * i + k] = T(0);
+    const V3<T> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
+    if (view_z(cam.view, mu) < T(0.2f))
+        return;
+    const T w = p.weights[i];
+    const V3<T> sc = mul3(V3<T> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
+    const T* q = p.rotations + 4 * size_t(i);
+    const M3<T> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
+    const V3<T> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const T dist = len3(sub3(campos, mu));
+    const S3<T> cov3 = compute_cov(sc, R);
+    const T fks = dist * p.aa;
+    const T fks2 = fks * fks;
+    S3<T> filtered = cov3;
+    filtered.v[0] = filtered.v[0] + fks2;
+    filtered.v[3] = filtered.v[3] + fks2;
+    filtered.v[5] = filtered.v[5] + fks2;
+    const T mass = w * integrate_exponential_cov2(affine_transform_and_cut(cov3, upper3(cam.view)));
+    if (mass <= T(0))
+        return;
+    const Gaussian2d<T> g = splat_project<Formulation::Opacity>(w, mu, sc, R, cam, T(kFilterSD * kFilterSD));
+    const auto iso = [](T wt, T var, T isoline) {
+        const T sv = T(-2) * dgmr_fm::log_f(isoline / wt);
+        if (sv <= T(0))
+            return T(0);
+        return dgmr_fm::sqrt_f(sv * var);
+    };
+    const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[0], T(1.f / 255.f))));
+    const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[2], T(1.f / 255.f))));
+    p.rects[2 * i] = ex;
+    p.rects[2 * i + 1] = ey;
+    const TileRect r = get_rect(float(g.centroid.x), float(g.centroid.y), ex, ey, cam.gx, cam.gy);
+    const unsigned touched = (r.x1 - r.x0) * (r.y1 - r.y0);
+    if (touched == 0)
+        return;
+    p.tiles_touched[i] = touched;
+    p.xy[2 * i] = g.centroid.x;
+    p.xy[2 * i + 1] = g.centroid.y;
+    const S3<T> inv = inverse_sym3(filtered);
+    const T smax = max_f(sc.x, max_f(sc.y, sc.z));
+    const T depth = dist - (smax * T(kRelevanceSigma)) / T(2);
+    p.depths[i] = depth;
+    const V3<T> dir = { (mu.x - campos.x) / dist, (mu.y - campos.y) / dist, (mu.z - campos.z) / dist };
+    uint8_t mask[3];
+    const V3<T> col = sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, mask);
+    p.rgb[3 * i] = col.x;
+    p.rgb[3 * i + 1] = col.y;
+    p.rgb[3 * i + 2] = col.z;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        p.clamped[3 * i + k] = mask[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        p.inv_cov[6 * i + k] = inv.v[k];
+    p.masses[i] = mass;
+}
+
+// Ray through the pixel centre (vol_marcher_forward.cu:308-315)
+template <class T>
+__device__ __forceinline__ V3<T> pixel_dir(const CameraT<T>& cam, unsigned px, unsigned py)
+{
+    const T pxc = T(px) + T(0.5);
+    const T pyc = T(py) + T(0.5);
+    const T nx = (pxc * T(2)) / T(float(cam.W)) - T(1);
+    const T ny = (pyc * T(2)) / T(float(cam.H)) - T(1);
+    const T* m = cam.inv_proj;
+    const T z = T(0), o = T(1);
+    T vx = ((m[0] * nx + m[4] * ny) + m[8] * z) + m[12] * o;
+    T vy = ((m[1] * nx + m[5] * ny) + m[9] * z) + m[13] * o;
+    T vz = ((m[2] * nx + m[6] * ny) + m[10] * z) + m[14] * o;
+    const T vw = ((m[3] * nx + m[7] * ny) + m[11] * z) + m[15] * o;
+    vx = vx / vw;
+    vy = vy / vw;
+    vz = vz / vw;
+    const V3<T> d = { vx - cam.campos[0], vy - cam.campos[1], vz - cam.campos[2] };
+    const T il = T(1) / dgmr_fm::sqrt_f(dot3(d, d));
+    return mul3(d, il);
+}
+
+template <class T>
+struct VmMarch {
+    const int32_t* ranges;
+    const int32_t* list;
+    const T* centroids;
+    const T* inv_cov;
+    const T* masses;
+    const T* rgb;
+    const T* depths;
+    T* fb;
+    T* remaining_T;
+    const T* grad_fb; // backward only
+    T* acc; // backward only: [N,10]
+    T* g_centroids; // backward only: [N,3]
+    uint32_t* stats;
+    ConstSamplesT<T> cs;
+};
+
+template <class T>
+struct MarchShared {
+    uint32_t id[256];
+    T mu[3][256];
+    T Q[6][256];
+    T mass[256];
+    T rgb[3][256];
+    T depth[256];
+};
+
+template <class T>
+__device__ __forceinline__ void load_batch(MarchShared<T>& sh, const VmMarch<T>& a, int32_t k, int32_t e)
+{
+    if (k < e) {
+        const uint32_t id = uint32_t(a.list[k]);
+        sh.id[threadIdx.x] = id;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            sh.mu[c][threadIdx.x] = a.centroids[3 * size_t(id) + c];
+            sh.rgb[c][threadIdx.x] = a.rgb[3 * size_t(id) + c];
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            sh.Q[c][threadIdx.x] = a.inv_cov[6 * size_t(id) + c];
+        sh.mass[threadIdx.x] = a.masses[id];
+        sh.depth[threadIdx.x] = a.depths[id];
+    }
+}
+
+template <class T>
+__device__ __forceinline__ S3<T> shared_Q(const MarchShared<T>& sh, int j)
+{
+    return S3<T> { { sh.Q[0][j], sh.Q[1][j], sh.Q[2][j], sh.Q[3][j], sh.Q[4][j], sh.Q[5][j] } };
+}
+
+// Pass 1 of a large step: sample sections from the Gaussians on the ray
+// (vol_marcher_forward.cu:351-403), block-synchronous over batches.
+template <class T>
+__device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done,
+    V3<T> o, V3<T> d)
+{
+    if (a.cs.n > 0) {
+        if (!done)
+            for (int i = 0; i < a.cs.n; ++i)
+                sec.put(Section<T> { a.cs.s[i][0], a.cs.s[i][1], a.cs.s[i][2] });
+        return;
+    }
+    bool done1 = done;
+    for (int32_t base = b; base < e; base += 256) {
+        if (__syncthreads_count(done1) == 256)
+            break;
+        load_batch(sh, a, base + int32_t(threadIdx.x), e);
+        __syncthreads();
+        if (done1)
+            continue;
+        const int n = min(256, e - base);
+        for (int j = 0; j < n; ++j) {
+            const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
+            const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
+            const T sd = dgmr_fm::sqrt_f(g.C);
+            if (sec.hi < sh.depth[j]) {
+                done1 = true;
+                break;
+            }
+            const T mor = g.weight * sh.mass[j];
+            if (mor <= T(1.0f / 255.f) || mor > T(1000))
+                continue;
+            if (g.C <= T(0))
+                continue;
+            if (dgmr_fm::isnan_f(g.centre))
+                continue;
+            const T start = g.centre - sd * T(kRelevanceSigma);
+            const T end = g.centre + sd * T(kRelevanceSigma);
+            const T delta_t = ((sd * T(kRelevanceSigma)) * T(2)) / T(float(kStepsPerGaussian - 1));
+            sec.put(Section<T> { start, end, delta_t });
+        }
+    }
+}
+
+// Pass 2: CDF-difference bin masses of every Gaussian in the tile list
+template <class T>
+__device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done, V3<T> o,
+    V3<T> d)
+{
+    for (int32_t base = b; base < e; base += 256) {
+        if (__syncthreads_count(done) == 256)
+            break;
+        load_batch(sh, a, base + int32_t(threadIdx.x), e);
+        __syncthreads();
+        if (done)
+            continue;
+        const int n = min(256, e - base);
+        for (int j = 0; j < n; ++j) {
+            const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
+            const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
+            sample_gaussian(g, sh.mass[j], V3<T> { sh.rgb[0][j], sh.rgb[1][j], sh.rgb[2][j] }, borders, bins);
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_vm_march(VmMarch<T> a, CameraT<T> cam)
+{
+    __shared__ MarchShared<T> sh;
+    const unsigned tile = blockIdx.x;
+    const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = px < cam.W && py < cam.H;
+    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<T> d = pixel_dir(cam, px, py);
+    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    bool done = !inside;
+    V3<T> colour = { T(0), T(0), T(0) };
+    T tr = T(1);
+    T start = T(0);
+    SectionSet<kLargeSteps, T> sec;
+    T borders[kSmallSteps];
+    Bin<T> bins[kBins];
+    for (unsigned step = 0;; ++step) {
+        if (__syncthreads_count(done) == 256)
+            break;
+        if (step >= kMaxLargeSteps) {
+            if (!done)
+                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
+            break;
+        }
+        sec.reset(start);
+        collect_sections(sec, sh, a, b, e, done, o, d);
+        sample_positions(sec, borders);
+        for (unsigned k = 0; k < kBins; ++k)
+            bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
+        fill_bins(bins, borders, sh, a, b, e, done, o, d);
+        if (!done) {
+            integrate_bins(colour, tr, bins);
+            done = sec.n == 0 || tr < T(1.f / 255.f);
+        }
+        start = borders[kSmallSteps - 1];
+    }
+    if (!inside)
+        return;
+    const size_t pix = size_t(py) * cam.W + px;
+    const size_t plane = size_t(cam.W) * cam.H;
+    a.fb[pix] = colour.x + tr * cam.bg[0];
+    a.fb[plane + pix] = colour.y + tr * cam.bg[1];
+    a.fb[2 * plane + pix] = colour.z + tr * cam.bg[2];
+    a.remaining_T[pix] = tr;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum_t(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// vol_marcher_backward.cu:115-319.  The 10 per-(pixel, Gaussian) atomics of
+// the reference are replaced by a warp-level shuffle sum and one atomic per
+// value per warp.
+template <class T>
+__global__ void __launch_bounds__(256) k_vm_march_bwd(VmMarch<T> a, CameraT<T> cam)
+{
+    __shared__ MarchShared<T> sh;
+    const unsigned tile = blockIdx.x;
+    const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = px < cam.W && py < cam.H;
+    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<T> d = pixel_dir(cam, px, py);
+    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    const size_t pix = size_t(py) * cam.W + px;
+    const size_t plane = size_t(cam.W) * cam.H;
+    bool done = !inside;
+    V3<T> gc = { T(0), T(0), T(0) };
+    V3<T> colour = { T(0), T(0), T(0) };
+    T final_T = T(1), gt = T(0);
+    if (inside) {
+        final_T = a.remaining_T[pix];
+        colour = { a.fb[pix] - final_T * cam.bg[0], a.fb[plane + pix] - final_T * cam.bg[1], a.fb[2 * plane + pix] - final_T * cam.bg[2] };
+        gc = { a.grad_fb[pix], a.grad_fb[plane + pix], a.grad_fb[2 * plane + pix] };
+        gt = (gc.x * cam.bg[0] + gc.y * cam.bg[1]) + gc.z * cam.bg[2];
+    }
+    T tr = T(1);
+    T start = T(0);
+    const int lane = threadIdx.x & 31;
+    SectionSet<kLargeSteps, T> sec;
+    T borders[kSmallSteps];
+    Bin<T> bins[kBins];
+    Bin<T> gbins[kBins];
+    for (unsigned step = 0;; ++step) {
+        if (__syncthreads_count(done) == 256)
+            break;
+        if (step >= kMaxLargeSteps) {
+            if (!done)
+                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
+            break;
+        }
+        sec.reset(start);
+        collect_sections(sec, sh, a, b, e, done, o, d);
+        sample_positions(sec, borders);
+        for (unsigned k = 0; k < kBins; ++k)
+            bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
+        fill_bins(bins, borders, sh, a, b, e, done, o, d);
+        if (!done)
+            grad_integrate_bins(colour, tr, final_T, bins, gc, gt, gbins);
+        // pass 3: adjoint of the bin masses, per Gaussian
+        for (int32_t base = b; base < e; base += 256) {
+            if (__syncthreads_count(done) == 256)
+                break;
+            load_batch(sh, a, base + int32_t(threadIdx.x), e);
+            __syncthreads();
+            const int n = min(256, e - base);
+            for (int j = 0; j < n; ++j) {
+                T v[10];
+                V3<T> gmu = { T(0), T(0), T(0) };
+#pragma unroll
+                for (int q = 0; q < 10; ++q)
+                    v[q] = T(0);
+                if (!done) {
+                    const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
+                    V3<T> grgb = { T(0), T(0), T(0) };
+                    S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
+                    grad_sample_gaussian(mu, shared_Q(sh, j), o, d, sh.mass[j], V3<T> { sh.rgb[0][j], sh.rgb[1][j], sh.rgb[2][j] }, borders, gbins, &v[0], &grgb,
+                        &gmu, &gQ);
+                    v[1] = grgb.x;
+                    v[2] = grgb.y;
+                    v[3] = grgb.z;
+#pragma unroll
+                    for (int q = 0; q < 6; ++q)
+                        v[4 + q] = gQ.v[q];
+                }
+                bool any = false;
+#pragma unroll
+                for (int q = 0; q < 10; ++q)
+                    any = any || v[q] != T(0);
+                any = any || gmu.x != T(0) || gmu.y != T(0) || gmu.z != T(0);
+                if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+                    for (int q = 0; q < 10; ++q)
+                        v[q] = warp_sum_t(v[q]);
+                    gmu.x = warp_sum_t(gmu.x);
+                    gmu.y = warp_sum_t(gmu.y);
+                    gmu.z = warp_sum_t(gmu.z);
+                    if (lane == 0) {
+                        const uint32_t id = sh.id[j];
+                        T* dst = a.acc + size_t(id) * 10;
+#pragma unroll
+                        for (int q = 0; q < 10; ++q)
+                            if (v[q] != T(0))
+                                atomicAdd(dst + q, v[q]);
+                        T* gm = a.g_centroids + size_t(id) * 3;
+                        if (gmu.x != T(0))
+                            atomicAdd(gm, gmu.x);
+                        if (gmu.y != T(0))
+                            atomicAdd(gm + 1, gmu.y);
+                        if (gmu.z != T(0))
+                            atomicAdd(gm + 2, gmu.z);
+                    }
+                }
+            }
+        }
+        if (!done)
+            done = sec.n == 0 || tr < T(1.f / 255.f);
+        start = borders[kSmallSteps - 1];
+    }
+}
+
+template <class T>
+struct VmBwdGauss {
+    uint32_t N;
+    const T* centroids;
+    const T* sh;
+    int sh_stride, sh_degree;
+    const T* weights;
+    const T* scales;
+    const T* rotations;
+    const uint8_t* clamped;
+    const int32_t* tiles_touched;
+    const T* acc;
+    T* g_sh;
+    T* g_weights;
+    T* g_centroids; // accumulated onto the march's contribution
+    T* g_scales;
+    T* g_rotations;
+    T aa;
+};
+
+// vol_marcher_backward.cu:321-384
+template <class T>
+__global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, CameraT<T> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N)
+        return;
+    for (int k = 0; k < p.sh_stride * 3; ++k)
+        p.g_sh[size_t(i) * p.sh_stride * 3 + k] = T(0);
+    p.g_weights[i] = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        p.g_scales[3 * i + k] = T(0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        p.g_rotations[4 * i + k] = T(0);
+    if (p.tiles_touched[i] == 0)
+        return;
+    const V3<T> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
+    if (view_z(cam.view, mu) < T(0.2))
+        return;
+    const T w = p.weights[i];
+    // the reference does not apply cov_scale_multiplier in the backward (vol_marcher_backward.cu:342)
+    const V3<T> sc = { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] };
+    const T* q = p.rotations + 4 * size_t(i);
+    const M3<T> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
+    const V3<T> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<T> delta = sub3(mu, campos);
+    const T dist = len3(delta);
+    const S3<T> cov3 = compute_cov(sc, R);
+    const T fks = dist * p.aa;
+    S3<T> filtered = cov3;
+    filtered.v[0] = filtered.v[0] + fks * fks;
+    filtered.v[3] = filtered.v[3] + fks * fks;
+    filtered.v[5] = filtered.v[5] + fks * fks;
+    const M3<T> W3 = upper3(cam.view);
+    const S2<T> cov2d = affine_transform_and_cut(cov3, W3);
+    const T mass = w * integrate_exponential_cov2(cov2d);
+    if (mass <= T(0))
+        return;
+    const V3<T> dir = { delta.x / dist, delta.y / dist, delta.z / dist };
+    const T* a = p.acc + size_t(i) * 10;
+    const V3<T> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<T> { a[1], a[2], a[3] }, p.clamped + 3 * size_t(i), T(1), p.g_sh);
+    V3<T> g_mu = mul3(g_dir, T(1) / dist);
+    T g_dist = -dot3(g_dir, delta) / (dist * dist);
+    S3<T> g_inv;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        g_inv.v[k] = a[4 + k];
+    const S3<T> g_filtered = grad_inverse_sym3(filtered, g_inv);
+    const T g_mass = a[0];
+    const T dcov = det2(cov2d);
+    const T i2 = integrate_exponential_cov2(cov2d);
+    const T g_w = g_mass * i2;
+    const T g_i2 = g_mass * w;
+    const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
+    const S2<T> g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
+    S3<T> g_cov3 = g_filtered;
+    const T g_fks2 = (g_filtered.v[0] + g_filtered.v[3]) + g_filtered.v[5];
+    g_dist = g_dist + (g_fks2 * T(2) * fks) * p.aa;
+    grad_affine_transform_and_cut(cov3, W3, g_cov2d, &g_cov3, static_cast<M3<T>*>(nullptr));
+    V3<T> g_s = { T(0), T(0), T(0) };
+    T g_q[4] = { T(0), T(0), T(0), T(0) };
+    grad_compute_cov(sc, q[0], q[1], q[2], q[3], g_cov3, &g_s, g_q);
+    g_mu = add3(g_mu, mul3(delta, g_dist / dist));
+    p.g_weights[i] = g_w;
+    p.g_scales[3 * i] = g_s.x;
+    p.g_scales[3 * i + 1] = g_s.y;
+    p.g_scales[3 * i + 2] = g_s.z;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        p.g_rotations[4 * i + k] = g_q[k];
+    p.g_centroids[3 * i] += g_mu.x;
+    p.g_centroids[3 * i + 1] += g_mu.y;
+    p.g_centroids[3 * i + 2] += g_mu.z;
+}
+
+template <class T>
+inline T aa_multiplier(const CameraT<T>& cam)
+{
+    return ((T(kFilterSD) * cam.tan_fovx) * T(2)) / T(float(cam.W));
+}
+
+template <class T>
+dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* c, void* workspace, size_t workspace_bytes,
+    dgmr_frame_stats* stats, cudaStream_t s)
+{
+    const uint32_t N = uint32_t(scene->n_gaussians);
+    const VmLayout<T> Lw = vm_layout<T>(N, 0, workspace);
+    if (workspace_bytes < Lw.pre_bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<T> cam = make_camera<T>(*camera);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : Lw.stats;
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    if (N == 0)
+        return launch_status();
+    VmPre<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
+        static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rects, static_cast<T*>(c->rgb),
+        c->rgb_sh_clamped, static_cast<T*>(c->depths), static_cast<T*>(c->points_xy_image), static_cast<T*>(c->inverse_filtered_cov3d),
+        static_cast<T*>(c->filtered_masses), reinterpret_cast<uint32_t*>(c->tiles_touched), aa_multiplier(cam) };
+    k_vm_preprocess<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    inclusive_scan_u32(reinterpret_cast<uint32_t*>(c->tiles_touched), reinterpret_cast<uint32_t*>(c->point_offsets), N, Lw.pre_scan_tmp, s);
+    k_pair_count<<<1, 1, 0, s>>>(reinterpret_cast<uint32_t*>(c->point_offsets), N, 0xffffffffu, st_dev, Lw.pre_scan_tmp);
+    return launch_status();
+}
+
+template <class T>
+dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* c, int64_t cap64, void* workspace, size_t workspace_bytes,
+    dgmr_frame_stats* stats, cudaStream_t s)
+{
+    const uint32_t N = uint32_t(scene->n_gaussians), cap = uint32_t(cap64);
+    const VmLayout<T> L = vm_layout<T>(N, cap, workspace);
+    if (workspace_bytes < L.bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<T> cam = make_camera<T>(*camera);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    BinningBuffers bin = L.bin;
+    if (N > 0)
+        k_depth_keys<T><<<(N + 255) / 256, 256, 0, s>>>(static_cast<const T*>(c->depths), N, bin.depth_key, bin.perm);
+    const int par = run_binning<T>(N, cam.gx, cam.gy, reinterpret_cast<uint32_t*>(c->tiles_touched), reinterpret_cast<uint32_t*>(c->point_offsets), c->rects,
+        static_cast<T*>(c->points_xy_image), cap, bin, c->i_ranges, st_dev, num_sms(), s);
+    if (cap > 0)
+        cudaMemcpyAsync(c->b_point_list, bin.pair_val[par], size_t(cap) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    VmMarch<T> a {};
+    a.ranges = c->i_ranges;
+    a.list = c->b_point_list;
+    a.centroids = static_cast<const T*>(scene->centroids);
+    a.inv_cov = static_cast<const T*>(c->inverse_filtered_cov3d);
+    a.masses = static_cast<const T*>(c->filtered_masses);
+    a.rgb = static_cast<const T*>(c->rgb);
+    a.depths = static_cast<const T*>(c->depths);
+    a.fb = static_cast<T*>(c->framebuffer);
+    a.remaining_T = static_cast<T*>(c->remaining_transparency);
+    a.stats = st_dev;
+    a.cs = const_samples<T>();
+    k_vm_march<T><<<cam.gx * cam.gy, 256, 0, s>>>(a, cam);
+    return launch_status();
+}
+
+template <class T>
+dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* c, const void* grad_fb, void* g_sh, void* g_weights,
+    void* g_centroids, void* g_scales, void* g_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, cudaStream_t s)
+{
+    const uint32_t N = uint32_t(scene->n_gaussians);
+    const VmLayout<T> L = vm_layout<T>(N, 0, workspace);
+    if (workspace_bytes < L.bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<T> cam = make_camera<T>(*camera);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    if (N == 0)
+        return DGMR_OK;
+    cudaMemsetAsync(L.acc, 0, size_t(N) * 10 * sizeof(T), s);
+    cudaMemsetAsync(g_centroids, 0, size_t(N) * 3 * sizeof(T), s);
+    VmMarch<T> a {};
+    a.ranges = c->i_ranges;
+    a.list = c->b_point_list;
+    a.centroids = static_cast<const T*>(scene->centroids);
+    a.inv_cov = static_cast<const T*>(c->inverse_filtered_cov3d);
+    a.masses = static_cast<const T*>(c->filtered_masses);
+    a.rgb = static_cast<const T*>(c->rgb);
+    a.depths = static_cast<const T*>(c->depths);
+    a.fb = static_cast<T*>(c->framebuffer);
+    a.remaining_T = static_cast<T*>(c->remaining_transparency);
+    a.grad_fb = static_cast<const T*>(grad_fb);
+    a.acc = L.acc;
+    a.g_centroids = static_cast<T*>(g_centroids);
+    a.stats = st_dev;
+    a.cs = const_samples<T>();
+    k_vm_march_bwd<T><<<cam.gx * cam.gy, 256, 0, s>>>(a, cam);
+    VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
+        static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
+        c->tiles_touched, L.acc, static_cast<T*>(g_sh), static_cast<T*>(g_weights), static_cast<T*>(g_centroids), static_cast<T*>(g_scales),
+        static_cast<T*>(g_rotations), aa_multiplier(cam) };
+    k_vm_bwd_gaussians<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    return launch_status();
+}
+
+inline bool cache_ok(const dgmr_vm_cache* c, bool need_list)
+{
+    return c && c->framebuffer && c->rects && c->rgb && c->rgb_sh_clamped && c->depths && c->points_xy_image && c->inverse_filtered_cov3d
+        && c->filtered_masses && c->tiles_touched && c->point_offsets && c->i_ranges && c->remaining_transparency && (!need_list || c->b_point_list);
+}
+
+} // namespace dgmr
+
+using namespace dgmr;
+
+extern "C" {
+
+size_t dgmr_vm_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, int32_t dtype)
+{
+    if (n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return 0;
+    if (dtype == DGMR_F64)
+        return vm_layout<double>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes;
+    return vm_layout<float>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes;
+}
+
+dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, void* workspace, size_t workspace_bytes,
+    dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, -1);
+    if (st != DGMR_OK)
+        return st;
+    if (!cache_ok(cache, false) || !workspace)
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (scene->dtype == DGMR_F64)
+        return vm_preprocess<double>(scene, camera, cache, workspace, workspace_bytes, stats, s);
+    return vm_preprocess<float>(scene, camera, cache, workspace, workspace_bytes, stats, s);
+}
+
+dgmr_status dgmr_vm_forward_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace,
+    size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, -1);
+    if (st != DGMR_OK)
+        return st;
+    if (!cache_ok(cache, pair_capacity > 0) || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (scene->dtype == DGMR_F64)
+        return vm_render<double>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s);
+    return vm_render<float>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s);
+}
+
+dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* cache, const void* grad_framebuffer, void* grad_sh,
+    void* grad_weights, void* grad_centroids, void* grad_scales, void* grad_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats,
+    dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, -1);
+    if (st != DGMR_OK)
+        return st;
+    if (!cache_ok(cache, false) || !workspace || !grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations)
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (scene->dtype == DGMR_F64)
+        return vm_backward<double>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
+            workspace_bytes, stats, s);
+    return vm_backward<float>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
+        workspace_bytes, stats, s);
+}
+
+dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections)
+{
+    if (n_sections < 0 || n_sections > 4 || (n_sections > 0 && !sections))
+        return DGMR_ERR_BAD_ARG;
+    g_const_samples.n = n_sections;
+    for (int i = 0; i < n_sections; ++i)
+        for (int j = 0; j < 3; ++j)
+            g_const_samples.s[i][j] = sections[3 * i + j];
+    return DGMR_OK;
+}
+
+const char* dgmr_status_string(dgmr_status status)
+{
+    switch (status) {
+    case DGMR_OK:
+        return "ok";
+    case DGMR_ERR_BAD_ARG:
+        return "invalid argument";
+    case DGMR_ERR_WORKSPACE:
+        return "workspace too small";
+    case DGMR_ERR_CUDA:
+        return "CUDA launch error";
+    }
+    return "unknown status";
+}
+
+const char* dgmr_version(void) { return "dgmr_b200 0.1 sm_100a"; }
+
+} // extern "C"

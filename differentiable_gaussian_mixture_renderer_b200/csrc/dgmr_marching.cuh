@@ -1,0 +1,299 @@
+// Per-ray state of the volume marcher: the capacity-bounded section set that
+// chooses sample positions, the 128-sample walk over it, and the per-bin
+// accumulation / blending helpers with their adjoints.
+//
+// Semantics follow src/dgmr/marching_steps.h:35-220 (DensityArray, sample),
+// src/dgmr/math.h:412-468 (integrate_bins, sample_gaussian) and
+// src/dgmr/grad/math.h:529-620 (their adjoints).  The section-insertion steps
+// are kept step for step because which sections survive when the set is full
+// is part of the rendered result (the reference's known-answer tests pin it).
+#pragma once
+
+#include "dgmr_device_math.cuh"
+
+namespace dgmr {
+
+constexpr unsigned kLargeSteps = 16; // vol_marcher.h:61 -- sections per large step
+constexpr unsigned kSmallSteps = 128; // vol_marcher.h:62 -- samples per large step
+constexpr unsigned kBins = kSmallSteps - 1;
+constexpr unsigned kStepsPerGaussian = 32; // vol_marcher.h:63
+constexpr float kRelevanceSigma = 3.f; // vol_marcher.h:65
+constexpr float kFilterSD = 0.55f; // vol_marcher.h:60
+constexpr unsigned kMaxLargeSteps = 4096; // a ray that makes no progress stops here and flags it
+
+template <class T>
+struct Section {
+    T start, end, delta_t;
+};
+
+template <unsigned MAX, class T>
+struct SectionSet {
+    unsigned n;
+    T lo, hi;
+    Section<T> e[MAX];
+
+    __device__ __forceinline__ void reset(T start)
+    {
+        n = 0;
+        lo = start;
+        hi = T(1) / T(0);
+    }
+
+    __device__ __forceinline__ static void combine(const Section<T>& a, const Section<T>& b, Section<T> out[3])
+    {
+        if (a.start < b.start)
+            out[0] = { a.start, min_f(a.end, b.start), a.delta_t };
+        else
+            out[0] = { b.start, min_f(b.end, a.start), b.delta_t };
+        if (b.end < a.end)
+            out[2] = { b.end, a.end, a.delta_t };
+        else
+            out[2] = { a.end, b.end, b.delta_t };
+        out[1] = { out[0].end, out[2].start, min_f(a.delta_t, b.delta_t) };
+    }
+
+    __device__ __noinline__ void put(Section<T> s)
+    {
+        if (s.end <= lo)
+            return;
+        if (s.start >= hi)
+            return;
+        s.start = max_f(lo, s.start);
+        s.end = min_f(hi, s.end);
+        unsigned first = n;
+        for (unsigned i = 0; i < n; ++i)
+            if (e[i].end > s.start) {
+                first = i;
+                break;
+            }
+        if (first >= n) {
+            if (first < MAX)
+                e[n++] = s;
+            else
+                hi = s.start;
+            return;
+        }
+        unsigned last = n;
+        for (unsigned i = first; i < n; ++i)
+            if (e[i].end > s.end) {
+                last = i;
+                break;
+            }
+        if (last < n && e[last].start < s.end)
+            ++last;
+        Section<T> ring[MAX];
+        unsigned r_read = 0, r_write = 0;
+        unsigned i_read = first, i_write = first;
+        unsigned grown = 0;
+        while (i_read < last + grown && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            if (r_read >= r_write)
+                break;
+            const Section<T> head = ring[r_read % MAX];
+            if (head.end <= s.start) {
+                e[i_write++] = ring[(r_read++) % MAX];
+                continue;
+            }
+            if (head.start >= s.end)
+                break;
+            Section<T> p[3];
+            combine(ring[(r_read++) % MAX], s, p);
+            if (p[0].delta_t == p[1].delta_t) {
+                p[1].start = p[0].start;
+                p[0].end = p[0].start;
+            }
+            s = p[2];
+            if (p[0].end - p[0].start <= T(0)) {
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                e[i_write++] = p[1];
+            } else {
+                e[i_write++] = p[0];
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                ++grown;
+                ring[(--r_read) % MAX] = p[1];
+            }
+        }
+        if (s.end - s.start > T(0) && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            e[i_write++] = s;
+        }
+        while (r_write - r_read && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            e[i_write++] = ring[(r_read++) % MAX];
+        }
+        n = i_write + n - i_read;
+        if (n == MAX)
+            hi = min_f(hi, e[n - 1].end);
+    }
+};
+
+// marching_steps.h:202-220: kSmallSteps monotone sample positions
+template <unsigned MAX, class T>
+__device__ __forceinline__ void sample_positions(const SectionSet<MAX, T>& d, T* out)
+{
+    if (d.n == 0) {
+        for (unsigned i = 0; i < kSmallSteps; ++i)
+            out[i] = T(0);
+        return;
+    }
+    out[0] = d.e[0].start;
+    unsigned cur = 0;
+    T prev = out[0];
+    for (unsigned i = 1; i < kSmallSteps; ++i) {
+        const T v = min_f(d.e[cur].end, prev + d.e[cur].delta_t);
+        out[i] = v;
+        prev = v;
+        if (cur < d.n - 1 && v == d.e[cur].end)
+            ++cur;
+    }
+}
+
+template <class T>
+struct alignas(sizeof(T) * 4) Bin {
+    T r, g, b, m;
+};
+
+// Early-outs of math.h:442-454.  Returns false when the Gaussian adds nothing.
+template <class T>
+__device__ __forceinline__ bool gaussian_on_ray(const Gauss1d<T>& g, T mass, T* sd_out, T* mor_out)
+{
+    const T sd = dgmr_fm::sqrt_f(g.C);
+    const T mor = g.weight * mass;
+    *sd_out = sd;
+    *mor_out = mor;
+    if (dgmr_fm::isnan_f(g.centre))
+        return false;
+    if (mor < T(1.0f / 255.f) || mor > T(1000))
+        return false;
+    if (sd <= T(0.0001) || dgmr_fm::isnan_f(sd) || dgmr_fm::isnan_f(mor) || mor > T(100000))
+        return false;
+    return true;
+}
+
+// math.h:430-468
+template <class T>
+__device__ __forceinline__ void sample_gaussian(const Gauss1d<T>& g, T mass, V3<T> rgb, const T* borders, Bin<T>* bins)
+{
+    T sd, mor;
+    if (!gaussian_on_ray(g, mass, &sd, &mor))
+        return;
+    const T inv_sd = T(1) / sd;
+    const T centre = g.centre;
+    const T mib = mor * (cdf_inv_SD(centre, inv_sd, borders[kBins]) - cdf_inv_SD(centre, inv_sd, borders[0]));
+    if (mib < T(0.0001f))
+        return;
+    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[0]);
+    for (unsigned k = 0; k < kBins; ++k) {
+        const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
+        const T m = max_f(T(0), (cdf_end - cdf_start) * mor);
+        cdf_start = cdf_end;
+        if (m < T(0.00001f))
+            continue;
+        Bin<T> b = bins[k];
+        b.r = b.r + rgb.x * m;
+        b.g = b.g + rgb.y * m;
+        b.b = b.b + rgb.z * m;
+        b.m = b.m + m;
+        bins[k] = b;
+    }
+}
+
+// math.h:412-428
+template <class T>
+__device__ __forceinline__ void integrate_bins(V3<T>& colour, T& transparency, const Bin<T>* bins)
+{
+    for (unsigned k = 0; k < kBins; ++k) {
+        const Bin<T> b = bins[k];
+        const T tk = dgmr_fm::exp_f(-b.m);
+        colour.x = colour.x + b.r * transparency;
+        colour.y = colour.y + b.g * transparency;
+        colour.z = colour.z + b.b * transparency;
+        transparency = transparency * tk;
+        if (transparency < T(1. / 255.))
+            break;
+    }
+}
+
+// grad/math.h:529-557 (colour peeling, front to back); gbins fully written
+template <class T>
+__device__ __forceinline__ void grad_integrate_bins(V3<T>& colour, T& transparency, T final_transparency, const Bin<T>* bins, V3<T> gc, T gt, Bin<T>* gbins)
+{
+    unsigned k = 0;
+    for (; k < kBins; ++k) {
+        const Bin<T> b = bins[k];
+        Bin<T> gb;
+        gb.r = transparency * gc.x;
+        gb.g = transparency * gc.y;
+        gb.b = transparency * gc.z;
+        const T tk = dgmr_fm::exp_f(-b.m);
+        const T inv_tk = min_f(T(255), T(1) / tk);
+        colour.x = (colour.x - b.r) * inv_tk;
+        colour.y = (colour.y - b.g) * inv_tk;
+        colour.z = (colour.z - b.b) * inv_tk;
+        const T g_tk = (final_transparency * inv_tk) * gt + dot3(gc, colour) * transparency;
+        gb.m = T(0) - g_tk * tk;
+        gbins[k] = gb;
+        transparency = transparency * tk;
+        if (transparency < T(1. / 255.)) {
+            ++k;
+            break;
+        }
+    }
+    for (; k < kBins; ++k)
+        gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
+}
+
+// grad/math.h:559-620; accumulates into the outputs
+template <class T>
+__device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V3<T> o, V3<T> d, T mass, V3<T> rgb, const T* borders, const Bin<T>* gbins,
+    T* g_mass, V3<T>* g_rgb, V3<T>* g_mu, S3<T>* g_Q)
+{
+    const Gauss1d<T> g = intersect_with_ray_inv_C(mu, Q, o, d);
+    T sd, mor;
+    if (!gaussian_on_ray(g, mass, &sd, &mor))
+        return;
+    const T inv_sd = T(1) / sd;
+    const T centre = g.centre;
+    const T mib = mor * (cdf_inv_SD(centre, inv_sd, borders[kBins]) - cdf_inv_SD(centre, inv_sd, borders[0]));
+    if (mib < T(0.0001f))
+        return;
+    T g_centre = 0, g_inv_sd = 0, g_mor = 0;
+    V3<T> grgb = { 0, 0, 0 };
+    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[0]);
+    for (unsigned k = 0; k < kBins; ++k) {
+        const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
+        const T delta = cdf_end - cdf_start;
+        const T m = max_f(T(0), delta * mor);
+        cdf_start = cdf_end;
+        if (m < T(0.00001f))
+            continue;
+        const Bin<T> gb = gbins[k];
+        grgb.x = grgb.x + gb.r * m;
+        grgb.y = grgb.y + gb.g * m;
+        grgb.z = grgb.z + gb.b * m;
+        const T g_m = ((gb.r * rgb.x + gb.g * rgb.y) + gb.b * rgb.z) + gb.m;
+        if (delta * mor <= T(0))
+            continue;
+        g_mor = g_mor + g_m * delta;
+        const T g_delta = g_m * mor;
+        grad_cdf_inv_SD(centre, inv_sd, borders[k], -g_delta, &g_centre, &g_inv_sd);
+        grad_cdf_inv_SD(centre, inv_sd, borders[k + 1], g_delta, &g_centre, &g_inv_sd);
+    }
+    const T g_w1d = g_mor * mass;
+    *g_mass = *g_mass + g_mor * g.weight;
+    const T g_sd = -g_inv_sd / (sd * sd);
+    const T g_var = g_sd / (T(2) * sd);
+    *g_rgb = add3(*g_rgb, grgb);
+    grad_intersect_with_ray_inv_C(mu, Q, o, d, g_w1d, g_centre, g_var, g_mu, g_Q);
+}
+
+} // namespace dgmr

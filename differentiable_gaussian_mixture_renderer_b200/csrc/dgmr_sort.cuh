@@ -1,0 +1,352 @@
+// Device-wide building blocks of the binning stage: an inclusive scan of u32
+// counts and a stable LSD radix sort of (u32 key, u32 value) pairs.  Both
+// read the element count from device memory (so a frame needs no host
+// round trip between its preprocess and its sort) and bound it by the
+// capacity the buffers were sized for.
+//
+// They replace the reference's cub::DeviceScan::InclusiveSum and
+// cub::DeviceRadixSort::SortPairs (splat_forward.cu:187-202, :256-274).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dgmr {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItemsPerThread = 8;
+constexpr int kSortTile = kSortThreads * kSortItemsPerThread; // 2048 items per tile
+constexpr int kSortBins = 256; // 8-bit digits
+
+__device__ __forceinline__ uint32_t dev_count(const uint32_t* n_dev, uint32_t n_static, uint32_t capacity)
+{
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    return n < capacity ? n : capacity;
+}
+
+// ---------------------------------------------------------------- scan
+// per-tile sums of `in` (tile = kSortTile items)
+static __global__ void k_scan_tile_sums(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ tile_sums)
+{
+    __shared__ uint32_t warp_sums[kSortWarps];
+    const uint32_t tile = blockIdx.x;
+    const uint32_t base = tile * kSortTile;
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kSortItemsPerThread; ++i) {
+        const uint32_t idx = base + i * kSortThreads + threadIdx.x;
+        if (idx < n)
+            s += in[idx];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0)
+        warp_sums[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kSortWarps; ++w)
+            t += warp_sums[w];
+        tile_sums[tile] = t;
+    }
+}
+
+// exclusive scan of the tile sums in one block (tile counts are small)
+static __global__ void k_scan_tile_offsets(uint32_t* __restrict__ tile_sums, uint32_t n_tiles)
+{
+    __shared__ uint32_t carry;
+    __shared__ uint32_t warp_tot[32];
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n_tiles; base += blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        const uint32_t v = idx < n_tiles ? tile_sums[idx] : 0;
+        uint32_t x = v;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            const int nw = blockDim.x / 32;
+            uint32_t t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o)
+                    t += y;
+            }
+            if (lane < nw)
+                warp_tot[lane] = t; // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t warp_excl = warp == 0 ? 0 : warp_tot[warp - 1];
+        const uint32_t excl = carry + warp_excl + x - v;
+        if (idx < n_tiles)
+            tile_sums[idx] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1)
+            carry = excl + v;
+        __syncthreads();
+    }
+}
+
+// inclusive scan within each tile plus the tile's offset
+static __global__ void k_scan_apply(const uint32_t* __restrict__ in, uint32_t n, const uint32_t* __restrict__ tile_offsets, uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t warp_tot[kSortWarps];
+    __shared__ uint32_t carry;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t base = tile * kSortTile;
+    if (threadIdx.x == 0)
+        carry = tile_offsets[tile];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = 0; i < kSortItemsPerThread; ++i) {
+        const uint32_t idx = base + i * kSortThreads + threadIdx.x;
+        const uint32_t v = idx < n ? in[idx] : 0;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_tot[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t t = warp_tot[w];
+            wex += (w < warp) ? t : 0;
+            tot += t;
+        }
+        if (idx < n)
+            out[idx] = carry + wex + x;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            carry += tot;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- radix sort
+// Histogram of one digit per tile: hist[d * tile_stride + tile].
+static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask,
+    uint32_t* __restrict__ hist, uint32_t tile_stride)
+{
+    __shared__ uint32_t h[kSortWarps][kSortBins];
+    const uint32_t n = dev_count(n_dev, n_static, capacity);
+    const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        for (int i = threadIdx.x; i < kSortWarps * kSortBins; i += kSortThreads)
+            (&h[0][0])[i] = 0;
+        __syncthreads();
+        const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+        for (int r = 0; r < kSortItemsPerThread; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
+            const bool valid = idx < n;
+            const uint32_t d = valid ? ((keys[idx] >> shift) & mask) : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1)
+                h[warp][d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+            t += h[w][threadIdx.x];
+        hist[threadIdx.x * tile_stride + tile] = t;
+        __syncthreads();
+    }
+}
+
+// Exclusive scan of each digit's row over tiles; row totals to digit_total.
+static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, uint32_t tile_stride,
+    uint32_t* __restrict__ digit_total)
+{
+    __shared__ uint32_t warp_tot[kSortWarps];
+    __shared__ uint32_t carry;
+    const uint32_t n = dev_count(n_dev, n_static, capacity);
+    const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* row = hist + size_t(blockIdx.x) * tile_stride;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t b = 0; b < n_tiles; b += kSortThreads) {
+        const uint32_t idx = b + threadIdx.x;
+        const uint32_t v = idx < n_tiles ? row[idx] : 0;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_tot[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t t = warp_tot[w];
+            wex += (w < warp) ? t : 0;
+            tot += t;
+        }
+        if (idx < n_tiles)
+            row[idx] = carry + wex + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        digit_total[blockIdx.x] = carry;
+}
+
+// Stable scatter: warp w of a tile owns a contiguous 256-item slice and ranks
+// its items in order with __match_any_sync, so equal digits keep input order.
+static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask, const uint32_t* __restrict__ hist,
+    uint32_t tile_stride, const uint32_t* __restrict__ digit_total)
+{
+    __shared__ uint32_t wcount[kSortWarps][kSortBins];
+    __shared__ uint32_t gbase[kSortBins];
+    __shared__ uint32_t dbase[kSortBins];
+    __shared__ uint32_t warp_tot[kSortWarps];
+    const uint32_t n = dev_count(n_dev, n_static, capacity);
+    const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+
+    // digit bases: exclusive scan of the 256 digit totals
+    {
+        const uint32_t v = digit_total[threadIdx.x];
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_tot[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+            wex += (w < warp) ? warp_tot[w] : 0;
+        dbase[threadIdx.x] = wex + x - v;
+        __syncthreads();
+    }
+
+    for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        for (int i = threadIdx.x; i < kSortWarps * kSortBins; i += kSortThreads)
+            (&wcount[0][0])[i] = 0;
+        __syncthreads();
+        const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+        uint32_t k[kSortItemsPerThread], v[kSortItemsPerThread], rank[kSortItemsPerThread];
+#pragma unroll
+        for (int r = 0; r < kSortItemsPerThread; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
+            const bool valid = idx < n;
+            k[r] = valid ? keys_in[idx] : 0u;
+            v[r] = valid ? vals_in[idx] : 0u;
+            const uint32_t d = valid ? ((k[r] >> shift) & mask) : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            rank[r] = (valid ? wcount[warp][d] : 0u) + __popc(peers & lt_mask);
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1)
+                wcount[warp][d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        {
+            const uint32_t d = threadIdx.x;
+            uint32_t run = 0;
+#pragma unroll
+            for (int w = 0; w < kSortWarps; ++w) {
+                const uint32_t t = wcount[w][d];
+                wcount[w][d] = run;
+                run += t;
+            }
+            gbase[d] = dbase[d] + hist[d * tile_stride + tile];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kSortItemsPerThread; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
+            if (idx < n) {
+                const uint32_t d = (k[r] >> shift) & mask;
+                const uint32_t pos = gbase[d] + wcount[warp][d] + rank[r];
+                keys_out[pos] = k[r];
+                vals_out[pos] = v[r];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Temporary storage for sort_pairs over at most `capacity` items.
+inline size_t radix_temp_bytes(uint32_t capacity)
+{
+    const size_t tiles = (size_t(capacity) + kSortTile - 1) / kSortTile;
+    return (size_t(kSortBins) * (tiles + 1) + kSortBins) * sizeof(uint32_t);
+}
+
+// Stable sort of (keys, vals) by key bits [0, end_bit).  The data ping-pongs
+// between (k0, v0) and (k1, v1); returns 0 if the result is in k0/v0, 1 if in
+// k1/v1.  n comes from *n_dev (device) when non-null, else n_static.
+inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int end_bit,
+    void* temp, int n_sms, cudaStream_t stream)
+{
+    const uint32_t tiles = (capacity + kSortTile - 1) / kSortTile;
+    if (tiles == 0)
+        return 0;
+    const uint32_t stride = tiles + 1;
+    uint32_t* hist = static_cast<uint32_t*>(temp);
+    uint32_t* dtotal = hist + size_t(kSortBins) * stride;
+    const uint32_t grid = tiles < uint32_t(n_sms * 8) ? tiles : uint32_t(n_sms * 8);
+    int cur = 0;
+    for (int shift = 0; shift < end_bit; shift += 8) {
+        const int bits = (end_bit - shift) < 8 ? (end_bit - shift) : 8;
+        const uint32_t mask = (1u << bits) - 1u;
+        uint32_t* ki = cur ? k1 : k0;
+        uint32_t* vi = cur ? v1 : v0;
+        uint32_t* ko = cur ? k0 : k1;
+        uint32_t* vo = cur ? v0 : v1;
+        k_radix_hist<<<grid, kSortThreads, 0, stream>>>(ki, n_dev, n_static, capacity, shift, mask, hist, stride);
+        k_radix_scan_rows<<<kSortBins, kSortThreads, 0, stream>>>(hist, n_dev, n_static, capacity, stride, dtotal);
+        k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal);
+        cur ^= 1;
+    }
+    return cur;
+}
+
+inline size_t scan_temp_bytes(uint32_t n) { return ((size_t(n) + kSortTile - 1) / kSortTile + 1) * sizeof(uint32_t); }
+
+// inclusive scan of n u32 (n known on the host)
+inline void inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, void* temp, cudaStream_t stream)
+{
+    if (n == 0)
+        return;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* sums = static_cast<uint32_t*>(temp);
+    k_scan_tile_sums<<<tiles, kSortThreads, 0, stream>>>(in, n, sums);
+    k_scan_tile_offsets<<<1, 1024, 0, stream>>>(sums, tiles);
+    k_scan_apply<<<tiles, kSortThreads, 0, stream>>>(in, n, sums, out);
+}
+
+} // namespace dgmr

@@ -1,0 +1,487 @@
+// Tile-based EWA splat renderer: forward (src/dgmr/splat_forward.cu:93-401)
+// and a reverse-order backward (no reference kernel), behind the C ABI of
+// include/dgmr_b200.h.
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "../../include/dgmr_b200.h"
+#include "dgmr_abi_common.h"
+#include "dgmr_binning.cuh"
+#include "dgmr_device_grad.cuh"
+
+namespace dgmr {
+
+struct SplatLayout {
+    int32_t* rects;
+    float* rgb;
+    uint8_t* clamped;
+    float* depths;
+    float* xy;
+    float* conic_opacity;
+    uint32_t* tiles_touched;
+    uint32_t* point_offsets;
+    int32_t* ranges;
+    float* final_T;
+    int32_t* n_contrib;
+    float* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3)
+    uint32_t* stats; // [4] used when the caller passes none
+    BinningBuffers bin;
+    size_t bytes;
+};
+
+inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void* base)
+{
+    SplatLayout L;
+    Carver c;
+    c.base = static_cast<char*>(base);
+    const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+    L.rects = c.take<int32_t>(size_t(N) * 2);
+    L.rgb = c.take<float>(size_t(N) * 3);
+    L.clamped = c.take<uint8_t>(size_t(N) * 3);
+    L.depths = c.take<float>(N);
+    L.xy = c.take<float>(size_t(N) * 2);
+    L.conic_opacity = c.take<float>(size_t(N) * 4);
+    L.tiles_touched = c.take<uint32_t>(N);
+    L.point_offsets = c.take<uint32_t>(N);
+    L.ranges = c.take<int32_t>(size_t(gx) * gy * 2);
+    L.final_T = c.take<float>(size_t(W) * H);
+    L.n_contrib = c.take<int32_t>(size_t(W) * H);
+    L.grad_acc = c.take<float>(size_t(N) * 9);
+    L.stats = c.take<uint32_t>(4);
+    carve_binning(c, L.bin, N, cap);
+    L.bytes = c.off;
+    return L;
+}
+
+struct SplatPre {
+    uint32_t N;
+    const float* centroids;
+    const float* sh;
+    int sh_stride, sh_degree;
+    const float* weights;
+    const float* scales;
+    const float* rotations;
+    int32_t* rects;
+    float* rgb;
+    uint8_t* clamped;
+    float* depths;
+    float* xy;
+    float* conic_opacity;
+    uint32_t* tiles_touched;
+    uint32_t* depth_key;
+    uint32_t* perm;
+};
+
+// splat_forward.cu:137-180
+__global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<float> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N)
+        return;
+    p.tiles_touched[i] = 0;
+    p.perm[i] = i;
+    p.depth_key[i] = 0;
+    p.rects[2 * i] = 0;
+    p.rects[2 * i + 1] = 0;
+    p.xy[2 * i] = 0.f;
+    p.xy[2 * i + 1] = 0.f;
+    p.depths[i] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        p.rgb[3 * i + c] = 0.f;
+        p.clamped[3 * i + c] = 0;
+    }
+    reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
+    if (view_z(cam.view, mu) < 0.2f)
+        return;
+    const float w = p.weights[i];
+    const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
+    const float* q = p.rotations + 4 * size_t(i);
+    const M3<float> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
+    const Gaussian2d<float> g = splat_project<Formulation::Ots>(w, mu, sc, R, cam, 0.3f);
+    const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
+    const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
+    p.rects[2 * i] = ex;
+    p.rects[2 * i + 1] = ey;
+    const TileRect r = get_rect(g.centroid.x, g.centroid.y, ex, ey, cam.gx, cam.gy);
+    const unsigned touched = (r.x1 - r.x0) * (r.y1 - r.y0);
+    if (touched == 0)
+        return;
+    p.tiles_touched[i] = touched;
+    p.xy[2 * i] = g.centroid.x;
+    p.xy[2 * i + 1] = g.centroid.y;
+    const V3<float> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const float depth = len3(sub3(campos, mu));
+    p.depths[i] = depth;
+    p.depth_key[i] = __float_as_uint(depth);
+    const V3<float> v = sub3(mu, campos);
+    const V3<float> dir = mul3(v, 1.f / dgmr_fm::sqrt_f(dot3(v, v)));
+    uint8_t mask[3];
+    const V3<float> col = sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, mask);
+    p.rgb[3 * i] = col.x;
+    p.rgb[3 * i + 1] = col.y;
+    p.rgb[3 * i + 2] = col.z;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        p.clamped[3 * i + c] = mask[c];
+    const S2<float> con = inverse2(g.cov);
+    reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(con.v[0], con.v[1], con.v[2], g.weight);
+}
+
+// (pixel, splat) evaluation of splat_forward.cu:365-370
+__device__ __forceinline__ float splat_gauss(float4 co, float2 xy, float px, float py, float* dx_o, float* dy_o)
+{
+    const float dx = px - xy.x;
+    const float dy = py - xy.y;
+    const float q = ((co.x * dx) * dx + (co.z * dy) * dy) + ((2.f * co.y) * dx) * dy;
+    *dx_o = dx;
+    *dy_o = dy;
+    return dgmr_fm::exp_f(-0.5f * q);
+}
+
+// One 16x16 tile per block, one pixel per thread; batches of 256 splats staged
+// in shared memory; the block stops when every pixel is saturated.
+__global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float* __restrict__ xy,
+    const float* __restrict__ conic_opacity, const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib,
+    unsigned W, unsigned H, unsigned gx, float bg0, float bg1, float bg2)
+{
+    __shared__ float2 s_xy[256];
+    __shared__ float4 s_co[256];
+    __shared__ float s_rgb[3][256];
+    const unsigned tile = blockIdx.x;
+    const unsigned tx = tile % gx, ty = tile / gx;
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = px < W && py < H;
+    bool done = !inside;
+    const int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
+    float Tr = 1.f, C0 = 0.f, C1 = 0.f, C2 = 0.f;
+    int32_t last = 0;
+    const float fpx = float(px), fpy = float(py);
+    for (int32_t base = b; base < e; base += 256) {
+        if (__syncthreads_count(done) == 256)
+            break;
+        const int32_t k = base + int32_t(threadIdx.x);
+        if (k < e) {
+            const uint32_t id = list[k];
+            s_xy[threadIdx.x] = reinterpret_cast<const float2*>(xy)[id];
+            s_co[threadIdx.x] = reinterpret_cast<const float4*>(conic_opacity)[id];
+            s_rgb[0][threadIdx.x] = rgb[3 * id];
+            s_rgb[1][threadIdx.x] = rgb[3 * id + 1];
+            s_rgb[2][threadIdx.x] = rgb[3 * id + 2];
+        }
+        __syncthreads();
+        if (done)
+            continue;
+        const int n = min(256, e - base);
+        for (int j = 0; j < n; ++j) {
+            float dx, dy;
+            const float4 co = s_co[j];
+            const float g = splat_gauss(co, s_xy[j], fpx, fpy, &dx, &dy);
+            const float alpha = min_f(0.99f, co.w * g);
+            if (alpha < 1.0f / 255.0f)
+                continue;
+            const float test_T = Tr * (1.f - alpha);
+            if (test_T < 0.0001f) {
+                done = true;
+                break;
+            }
+            C0 = C0 + (s_rgb[0][j] * alpha) * Tr;
+            C1 = C1 + (s_rgb[1][j] * alpha) * Tr;
+            C2 = C2 + (s_rgb[2][j] * alpha) * Tr;
+            Tr = test_T;
+            last = base + j - b + 1;
+        }
+    }
+    if (!inside)
+        return;
+    const size_t pix = size_t(py) * W + px;
+    fb[pix] = C0 + Tr * bg0;
+    fb[size_t(W) * H + pix] = C1 + Tr * bg1;
+    fb[2 * size_t(W) * H + pix] = C2 + Tr * bg2;
+    final_T[pix] = Tr;
+    n_contrib[pix] = last;
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Reverse-order blend adjoint: each pixel walks its contributors back to
+// front, recovering T_i = T_{i+1} / (1 - alpha_i); per-splat gradients are
+// summed over the warp with shuffles before one atomic per value.
+__global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
+    const float* __restrict__ xy, const float* __restrict__ conic_opacity, const float* __restrict__ rgb, const float* __restrict__ final_T,
+    const int32_t* __restrict__ n_contrib, const float* __restrict__ grad_fb, float* __restrict__ acc, unsigned W, unsigned H, unsigned gx, float bg0, float bg1,
+    float bg2)
+{
+    __shared__ float2 s_xy[256];
+    __shared__ float4 s_co[256];
+    __shared__ float s_rgb[3][256];
+    __shared__ uint32_t s_id[256];
+    __shared__ int s_max;
+    const unsigned tile = blockIdx.x;
+    const unsigned tx = tile % gx, ty = tile / gx;
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = px < W && py < H;
+    const int32_t b = ranges[2 * tile];
+    const size_t pix = size_t(py) * W + px;
+    const int32_t my_n = inside ? n_contrib[pix] : 0;
+    if (threadIdx.x == 0)
+        s_max = 0;
+    __syncthreads();
+    atomicMax(&s_max, my_n);
+    __syncthreads();
+    const int32_t max_n = s_max;
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f, Tf = 1.f;
+    if (inside) {
+        g0 = grad_fb[pix];
+        g1 = grad_fb[size_t(W) * H + pix];
+        g2 = grad_fb[2 * size_t(W) * H + pix];
+        Tf = final_T[pix];
+    }
+    const float bg_dot = (bg0 * g0 + bg1 * g1) + bg2 * g2;
+    float Tr = Tf;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f; // accumulated colour behind the current splat
+    const float fpx = float(px), fpy = float(py);
+    const int lane = threadIdx.x & 31;
+    for (int32_t hi = max_n; hi > 0; hi -= 256) {
+        const int32_t lo = hi > 256 ? hi - 256 : 0;
+        __syncthreads();
+        const int32_t k = lo + int32_t(threadIdx.x);
+        if (k < hi) {
+            const uint32_t id = list[b + k];
+            s_id[threadIdx.x] = id;
+            s_xy[threadIdx.x] = reinterpret_cast<const float2*>(xy)[id];
+            s_co[threadIdx.x] = reinterpret_cast<const float4*>(conic_opacity)[id];
+            s_rgb[0][threadIdx.x] = rgb[3 * id];
+            s_rgb[1][threadIdx.x] = rgb[3 * id + 1];
+            s_rgb[2][threadIdx.x] = rgb[3 * id + 2];
+        }
+        __syncthreads();
+        for (int32_t kk = hi - 1; kk >= lo; --kk) {
+            const int j = kk - lo;
+            float v[9] = { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f };
+            bool any = false;
+            if (kk < my_n) {
+                float dx, dy;
+                const float4 co = s_co[j];
+                const float g = splat_gauss(co, s_xy[j], fpx, fpy, &dx, &dy);
+                const float alpha = min_f(0.99f, co.w * g);
+                if (!(alpha < 1.0f / 255.0f)) {
+                    any = true;
+                    Tr = Tr / (1.f - alpha);
+                    const float c0 = s_rgb[0][j], c1 = s_rgb[1][j], c2 = s_rgb[2][j];
+                    const float aT = alpha * Tr;
+                    v[6] = aT * g0;
+                    v[7] = aT * g1;
+                    v[8] = aT * g2;
+                    const float g_alpha = Tr * (((c0 - a0) * g0 + (c1 - a1) * g1) + (c2 - a2) * g2) - Tf * bg_dot / (1.f - alpha);
+                    a0 = alpha * c0 + (1.f - alpha) * a0;
+                    a1 = alpha * c1 + (1.f - alpha) * a1;
+                    a2 = alpha * c2 + (1.f - alpha) * a2;
+                    if (co.w * g < 0.99f) {
+                        v[5] = g_alpha * g;
+                        const float g_q = -0.5f * g * (g_alpha * co.w);
+                        v[2] = g_q * dx * dx;
+                        v[3] = g_q * 2.f * dx * dy;
+                        v[4] = g_q * dy * dy;
+                        v[0] = -(g_q * (2.f * co.x * dx + 2.f * co.y * dy));
+                        v[1] = -(g_q * (2.f * co.z * dy + 2.f * co.y * dx));
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    v[q] = warp_sum(v[q]);
+                if (lane == 0) {
+                    float* dst = acc + size_t(s_id[j]) * 9;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        if (v[q] != 0.f)
+                            atomicAdd(dst + q, v[q]);
+                }
+            }
+        }
+    }
+}
+
+struct SplatBwdGauss {
+    uint32_t N;
+    const float* centroids;
+    const float* sh;
+    int sh_stride, sh_degree;
+    const float* weights;
+    const float* scales;
+    const float* rotations;
+    const uint8_t* clamped;
+    const uint32_t* tiles_touched;
+    const float* acc;
+    float* g_sh;
+    float* g_weights;
+    float* g_centroids;
+    float* g_scales;
+    float* g_rotations;
+};
+
+// per-Gaussian chain rule: conic -> 2-D covariance -> projection adjoint, SH
+__global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, CameraT<float> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N)
+        return;
+    for (int k = 0; k < p.sh_stride * 3; ++k)
+        p.g_sh[size_t(i) * p.sh_stride * 3 + k] = 0.f;
+    p.g_weights[i] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p.g_centroids[3 * i + k] = 0.f;
+        p.g_scales[3 * i + k] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        p.g_rotations[4 * i + k] = 0.f;
+    if (p.tiles_touched[i] == 0)
+        return;
+    const float* a = p.acc + size_t(i) * 9;
+    const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
+    const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
+    const float* q = p.rotations + 4 * size_t(i);
+    const M3<float> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
+    const Gaussian2d<float> g2 = splat_project<Formulation::Ots>(p.weights[i], mu, sc, R, cam, 0.3f);
+    const S2<float> M = inverse2(g2.cov);
+    const float G00 = a[2], G01 = a[3] * 0.5f, G11 = a[4];
+    // H = -M G M (2x2 symmetric)
+    const float MG00 = M.v[0] * G00 + M.v[1] * G01, MG01 = M.v[0] * G01 + M.v[1] * G11;
+    const float MG10 = M.v[1] * G00 + M.v[2] * G01, MG11 = M.v[1] * G01 + M.v[2] * G11;
+    const float H00 = -(MG00 * M.v[0] + MG01 * M.v[1]);
+    const float H01 = -(MG00 * M.v[1] + MG01 * M.v[2]);
+    const float H11 = -(MG10 * M.v[1] + MG11 * M.v[2]);
+    const S2<float> g_cov = { { H00, 2.f * H01, H11 } };
+    float g_weight = 0.f;
+    V3<float> g_mu = { 0.f, 0.f, 0.f }, g_s = { 0.f, 0.f, 0.f };
+    float g_q[4] = { 0.f, 0.f, 0.f, 0.f };
+    grad_splat_ots(p.weights[i], mu, sc, q[0], q[1], q[2], q[3], cam, 0.3f, a[5], V2<float> { a[0], a[1] }, g_cov, &g_weight, &g_mu, &g_s, g_q);
+    const V3<float> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<float> v = sub3(mu, campos);
+    const float vl = dgmr_fm::sqrt_f(dot3(v, v));
+    const V3<float> dir = mul3(v, 1.f / vl);
+    const V3<float> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<float> { a[6], a[7], a[8] }, p.clamped + 3 * size_t(i), 0.f, p.g_sh);
+    const float gd = dot3(g_dir, dir);
+    g_mu = add3(g_mu, mul3(sub3(g_dir, mul3(dir, gd)), 1.f / vl));
+    p.g_weights[i] = g_weight;
+    p.g_centroids[3 * i] = g_mu.x;
+    p.g_centroids[3 * i + 1] = g_mu.y;
+    p.g_centroids[3 * i + 2] = g_mu.z;
+    p.g_scales[3 * i] = g_s.x * cam.cov_scale_multiplier;
+    p.g_scales[3 * i + 1] = g_s.y * cam.cov_scale_multiplier;
+    p.g_scales[3 * i + 2] = g_s.z * cam.cov_scale_multiplier;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        p.g_rotations[4 * i + k] = g_q[k];
+}
+
+} // namespace dgmr
+
+using namespace dgmr;
+
+extern "C" {
+
+size_t dgmr_splat_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity)
+{
+    if (n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return 0;
+    return splat_layout(uint32_t(n_gaussians), uint32_t(width), uint32_t(height), uint32_t(pair_capacity), nullptr).bytes;
+}
+
+dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* workspace, size_t workspace_bytes,
+    dgmr_splat_views* views)
+{
+    if (!views || !workspace || n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    const uint32_t W = uint32_t(width), H = uint32_t(height);
+    const SplatLayout L = splat_layout(uint32_t(n_gaussians), W, H, uint32_t(pair_capacity), workspace);
+    if (workspace_bytes < L.bytes)
+        return DGMR_ERR_WORKSPACE;
+    const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+    const int par = tile_sort_parity(gx * gy);
+    views->rects = L.rects;
+    views->rgb = L.rgb;
+    views->rgb_sh_clamped = L.clamped;
+    views->depths = L.depths;
+    views->points_xy_image = L.xy;
+    views->conic_opacity = L.conic_opacity;
+    views->tiles_touched = reinterpret_cast<int32_t*>(L.tiles_touched);
+    views->point_offsets = reinterpret_cast<int32_t*>(L.point_offsets);
+    views->i_ranges = L.ranges;
+    views->point_list = reinterpret_cast<int32_t*>(L.bin.pair_val[par]);
+    views->point_list_tiles = L.bin.pair_tile[par];
+    views->final_transmittance = L.final_T;
+    views->n_contrib = L.n_contrib;
+    return DGMR_OK;
+}
+
+dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* workspace, size_t workspace_bytes,
+    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, DGMR_F32);
+    if (st != DGMR_OK)
+        return st;
+    if (!framebuffer || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t N = uint32_t(scene->n_gaussians), W = uint32_t(camera->width), H = uint32_t(camera->height), cap = uint32_t(pair_capacity);
+    const SplatLayout L = splat_layout(N, W, H, cap, workspace);
+    if (workspace_bytes < L.bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<float> cam = make_camera<float>(*camera);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    BinningBuffers bin = L.bin;
+    if (N > 0) {
+        SplatPre p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
+            static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.rects, L.rgb,
+            L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, bin.depth_key, bin.perm };
+        k_splat_preprocess<<<(N + 255) / 256, 256, 0, s>>>(p, cam);
+    }
+    const int par = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, bin, L.ranges, st_dev, num_sms(), s);
+    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, framebuffer, L.final_T, L.n_contrib, W, H, cam.gx,
+        cam.bg[0], cam.bg[1], cam.bg[2]);
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* camera, const float* grad_framebuffer, float* grad_sh, float* grad_weights,
+    float* grad_centroids, float* grad_scales, float* grad_rotations, void* workspace, size_t workspace_bytes, int64_t pair_capacity, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, DGMR_F32);
+    if (st != DGMR_OK)
+        return st;
+    if (!grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations || !workspace || pair_capacity < 0
+        || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t N = uint32_t(scene->n_gaussians), W = uint32_t(camera->width), H = uint32_t(camera->height), cap = uint32_t(pair_capacity);
+    const SplatLayout L = splat_layout(N, W, H, cap, workspace);
+    if (workspace_bytes < L.bytes)
+        return DGMR_ERR_WORKSPACE;
+    if (N == 0)
+        return DGMR_OK;
+    const CameraT<float> cam = make_camera<float>(*camera);
+    const int par = tile_sort_parity(cam.gx * cam.gy);
+    cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
+    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.final_T, L.n_contrib, grad_framebuffer,
+        L.grad_acc, W, H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
+        static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
+        L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations };
+    k_splat_bwd_gaussians<<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    return launch_status();
+}
+
+} // extern "C"

@@ -1,0 +1,142 @@
+"""Tile-based splat renderer: forward (the reference's dgmr::splat_forward,
+src/dgmr/splat_forward.cu) and backward (new; the reference has none), as a
+plain call and as a torch.autograd.Function.
+
+Arguments follow the vol_marcher op's conventions: float32 CUDA tensors,
+sh [N, k<=16, 3], opacity [N] or [N, 1], means [N, 3], scales [N, 3],
+rotations [N, 4] (w, x, y, z), view / full view-projection matrices in the
+transposed torch layout, background [3].
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import _native as N
+
+
+@dataclass
+class SplatFrame:
+    """Device state of one rendered frame (kept for the backward pass)."""
+    workspace: torch.Tensor
+    pair_capacity: int
+    stats: torch.Tensor  # int32[4]: n_pairs, flags, ...
+    scene: N.Scene
+    camera: N.Camera
+    n: int
+    width: int
+    height: int
+
+    def views(self) -> dict:
+        """Per-Gaussian cache and binning result as tensors (no copies)."""
+        lib = N.lib()
+        v = N.SplatViews()
+        N.check(lib.dgmr_splat_workspace_views(self.n, self.width, self.height, self.pair_capacity,
+                                               N.ptr(self.workspace), self.workspace.numel(), v), "workspace views")
+        base = self.workspace.data_ptr()
+        gx, gy = (self.width + 15) // 16, (self.height + 15) // 16
+        n, hw = self.n, self.width * self.height
+
+        def view(addr, count, dtype, shape):
+            elem = torch.tensor([], dtype=dtype).element_size()
+            off = addr - base
+            return self.workspace[off:off + count * elem].view(dtype).reshape(shape)
+
+        return dict(rects=view(v.rects, 2 * n, torch.int32, (n, 2)), rgb=view(v.rgb, 3 * n, torch.float32, (n, 3)),
+                    rgb_sh_clamped=view(v.rgb_sh_clamped, 3 * n, torch.uint8, (n, 3)),
+                    depths=view(v.depths, n, torch.float32, (n,)),
+                    points_xy_image=view(v.points_xy_image, 2 * n, torch.float32, (n, 2)),
+                    conic_opacity=view(v.conic_opacity, 4 * n, torch.float32, (n, 4)),
+                    tiles_touched=view(v.tiles_touched, n, torch.int32, (n,)),
+                    point_offsets=view(v.point_offsets, n, torch.int32, (n,)),
+                    i_ranges=view(v.i_ranges, 2 * gx * gy, torch.int32, (gx * gy, 2)),
+                    point_list=view(v.point_list, self.pair_capacity, torch.int32, (self.pair_capacity,)),
+                    point_list_tiles=view(v.point_list_tiles, self.pair_capacity, torch.int32, (self.pair_capacity,)),
+                    final_transmittance=view(v.final_transmittance, hw, torch.float32, (self.height, self.width)),
+                    n_contrib=view(v.n_contrib, hw, torch.int32, (self.height, self.width)))
+
+
+def _prepare(shs, opacity, means3D, scales, rotations):
+    ts = [shs, opacity, means3D, scales, rotations]
+    for t in ts:
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float32:
+            raise TypeError("the splat renderer takes float32 tensors")
+        if t.device.type != "cuda":
+            raise ValueError("the splat renderer runs on CUDA tensors only")
+    return [t if t.is_contiguous() else t.contiguous() for t in ts]
+
+
+def splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, background, width: int, height: int,
+                  tanfovx: float, tanfovy: float, sh_degree: int, cov_scale_multiplier: float = 1.0,
+                  pair_capacity: int | None = None, framebuffer: torch.Tensor | None = None,
+                  stream: torch.cuda.Stream | None = None) -> tuple[torch.Tensor, SplatFrame]:
+    """Render one frame.  Without ``pair_capacity`` the pair buffers are sized
+    from the frame itself (one device->host read of the pair count, like the
+    reference's .item() at splat_forward.cu:204); with it, the call is
+    asynchronous and ``frame.stats`` reports an overflow instead."""
+    shs, opacity, means3D, scales, rotations = _prepare(shs, opacity, means3D, scales, rotations)
+    lib = N.lib()
+    dev = means3D.device
+    n, W, H = int(means3D.shape[0]), int(width), int(height)
+    scene = N.make_scene(shs, opacity, means3D, scales, rotations, sh_degree)
+    cam = N.make_camera(view, proj, campos, background, W, H, tanfovx, tanfovy, cov_scale_multiplier)
+    fb = framebuffer if framebuffer is not None else torch.empty((3, H, W), dtype=torch.float32, device=dev)
+    stats = torch.zeros(4, dtype=torch.int32, device=dev)
+    sh = N.stream_handle(stream)
+    sync_size = pair_capacity is None
+    cap = int(pair_capacity) if pair_capacity is not None else max(4096, 8 * n)
+    while True:
+        ws = torch.empty(lib.dgmr_splat_workspace_size(n, W, H, cap), dtype=torch.uint8, device=dev)
+        N.check(lib.dgmr_splat_forward(scene, cam, N.ptr(fb), N.ptr(ws), ws.numel(), cap, N.ptr(stats), sh),
+                "splat forward")
+        if not sync_size:
+            break
+        n_pairs, flags = (int(v) for v in stats[:2].tolist())
+        if not (flags & N.FLAG_PAIR_OVERFLOW):
+            break
+        cap = n_pairs
+    frame = SplatFrame(ws, cap, stats, scene, cam, n, W, H)
+    return fb, frame
+
+
+def splat_backward(frame: SplatFrame, grad_framebuffer: torch.Tensor, shs, opacity, means3D, scales, rotations,
+                   stream: torch.cuda.Stream | None = None):
+    """Gradients w.r.t. (shs, opacity, means3D, scales, rotations) of a frame
+    rendered by splat_forward with the same tensors."""
+    shs, opacity, means3D, scales, rotations = _prepare(shs, opacity, means3D, scales, rotations)
+    lib = N.lib()
+    g = grad_framebuffer if grad_framebuffer.is_contiguous() else grad_framebuffer.contiguous()
+    if g.dtype != torch.float32 or tuple(g.shape) != (3, frame.height, frame.width):
+        raise ValueError("grad_framebuffer must be float32 [3, H, W]")
+    dev = means3D.device
+    n = frame.n
+    g_sh = torch.empty(shs.shape, dtype=torch.float32, device=dev)
+    g_w = torch.empty(opacity.shape, dtype=torch.float32, device=dev)
+    g_mu = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    g_s = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    g_q = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    N.check(lib.dgmr_splat_backward(frame.scene, frame.camera, N.ptr(g), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
+                                    N.ptr(g_s), N.ptr(g_q), N.ptr(frame.workspace), frame.workspace.numel(),
+                                    frame.pair_capacity, N.stream_handle(stream)), "splat backward")
+    return g_sh, g_w, g_mu, g_s, g_q
+
+
+class SplatRender(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, shs, opacity, means3D, scales, rotations, view, proj, campos, background, width: int,
+                height: int, tanfovx: float, tanfovy: float, sh_degree: int):
+        fb, frame = splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, background, width,
+                                  height, tanfovx, tanfovy, sh_degree)
+        ctx.frame = frame
+        ctx.save_for_backward(shs, opacity, means3D, scales, rotations)
+        return fb
+
+    @staticmethod
+    def backward(ctx, grad_output):
+        shs, opacity, means3D, scales, rotations = ctx.saved_tensors
+        grads = splat_backward(ctx.frame, grad_output, shs, opacity, means3D, scales, rotations)
+        return (*grads, None, None, None, None, None, None, None, None, None)
+
+
+render = SplatRender.apply

@@ -1,0 +1,46 @@
+"""Differentiable volume ray marcher -- drop-in for python_bindings/vol_marcher.py.
+
+``apply(shs, opacity, means3D, scales, rotations, world_view_transform,
+full_proj_transform, camera_center, bg_color, image_width, image_height,
+tanfovx, tanfovy, active_sh_degree) -> image [3, H, W]`` with the reference's
+argument meaning (vol_marcher.py:19-65): float32 or float64 CUDA tensors,
+matrices in the transposed (torch) layout, SH [N, k<=16, 3], opacity [N] or
+[N, 1], rotations (w, x, y, z).  Backward returns gradients for the first five
+inputs and None for the other nine.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import cpp_binding
+
+
+class VolMarcher(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
+                camera_center, bg_color, image_width: int, image_height: int, tanfovx: float, tanfovy: float,
+                active_sh_degree: int):
+        cache = cpp_binding.forward(shs, opacity, means3D, scales, rotations, world_view_transform,
+                                    full_proj_transform, camera_center, bg_color, image_width, image_height, tanfovx,
+                                    tanfovy, active_sh_degree)
+        ctx.save_for_backward(shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
+                              camera_center, bg_color, *cache)
+        ctx.frame = (int(image_width), int(image_height), float(tanfovx), float(tanfovy), int(active_sh_degree))
+        return cache[0]
+
+    @staticmethod
+    def backward(ctx, grad_output):
+        if not grad_output.is_contiguous():
+            grad_output = grad_output.contiguous()
+        saved = ctx.saved_tensors
+        shs, opacity, means3D, scales, rotations, view, proj, campos, bg = saved[:9]
+        cache = list(saved[9:])
+        W, H, tfx, tfy, deg = ctx.frame
+        g_sh, g_w, g_mu, g_s, g_q = cpp_binding.backward(shs, opacity, means3D, scales, rotations, view, proj, campos,
+                                                         bg, W, H, tfx, tfy, deg, grad_output, cache)
+        if opacity.dim() == 1:
+            g_w = g_w.reshape(-1)
+        return g_sh, g_w, g_mu, g_s, g_q, None, None, None, None, None, None, None, None, None
+
+
+apply = VolMarcher.apply

@@ -1,0 +1,176 @@
+/* C ABI of the B200 Gaussian-mixture renderer (libdgmr_b200.so).
+ *
+ * Plain structs, device pointers, sizes and a cudaStream_t.  No exception,
+ * allocation or host synchronisation happens inside these calls: the caller
+ * owns every buffer, including one workspace per frame sized by the
+ * *_workspace_size queries, and reads results whenever it synchronises.
+ *
+ * Layouts are the reference's (python_bindings/vol_marcher.cu:42-104):
+ *   centroids [N,3], sh [N,sh_stride,3] (sh_stride <= 16 coefficients),
+ *   weights [N] (opacity), scales [N,3], rotations [N,4] stored (w,x,y,z),
+ *   framebuffer [3,H,W], 4x4 matrices in glm order: element (row r, col c)
+ *   at index c*4+r -- i.e. the row-major bytes of the torch tensors the
+ *   reference's Python op receives.
+ */
+#ifndef DGMR_B200_H
+#define DGMR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dgmr_stream;
+
+typedef enum dgmr_status {
+    DGMR_OK = 0,
+    DGMR_ERR_BAD_ARG = 1, /* null pointer, negative size, sh_stride/degree out of range */
+    DGMR_ERR_WORKSPACE = 2, /* workspace smaller than the query returned */
+    DGMR_ERR_CUDA = 3, /* a launch failed; cudaGetLastError() holds the cause */
+} dgmr_status;
+
+/* Device-side frame statistics (caller-owned, 16 bytes, written by the calls
+ * that take it).  flags: bit 0 = more (tile, Gaussian) pairs than the pair
+ * capacity (pairs beyond it were dropped; re-run with a larger capacity),
+ * bit 1 = some ray march hit the large-step limit. */
+typedef struct dgmr_frame_stats {
+    uint32_t n_pairs;
+    uint32_t flags;
+    uint32_t n_visible;
+    uint32_t reserved;
+} dgmr_frame_stats;
+
+#define DGMR_FLAG_PAIR_OVERFLOW 1u
+#define DGMR_FLAG_STEP_LIMIT 2u
+
+typedef enum dgmr_dtype { DGMR_F32 = 0, DGMR_F64 = 1 } dgmr_dtype;
+
+/* The Gaussian mixture (all device pointers, element type = dtype). */
+typedef struct dgmr_scene {
+    int32_t n_gaussians;
+    int32_t sh_stride; /* coefficients stored per Gaussian, 1..16 */
+    int32_t sh_degree; /* active SH degree, 0..3 */
+    int32_t dtype; /* dgmr_dtype; the splat renderer takes DGMR_F32 only */
+    const void* centroids;
+    const void* sh;
+    const void* weights;
+    const void* scales;
+    const void* rotations;
+} dgmr_scene;
+
+/* One camera (host values). */
+typedef struct dgmr_camera {
+    int32_t width, height;
+    double view[16]; /* world -> view, glm order */
+    double proj[16]; /* full view-projection (P * V), glm order */
+    double campos[3];
+    double background[3];
+    double tan_fovx, tan_fovy;
+    double cov_scale_multiplier; /* 1.0 in the reference's Python path */
+} dgmr_camera;
+
+/* ---------------------------------------------------------------- splat */
+
+/* Replaces dgmr::splat_forward(SplatForwardData&) (src/dgmr/splat_forward.h:62,
+ * reached through dgmr::sibr_interfaces::splat, src/dgmr/sibr_interfaces.h:25).
+ * Bytes of workspace for one frame of n Gaussians at width x height with room
+ * for pair_capacity (tile, Gaussian) pairs.  The workspace also keeps what the
+ * backward pass needs, so keep it alive between forward and backward. */
+size_t dgmr_splat_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity);
+
+/* Forward splat: framebuffer [3,H,W] f32 (device).  stats may be NULL. */
+dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* workspace, size_t workspace_bytes,
+    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Views into the workspace after dgmr_splat_forward (device pointers, NULL if
+ * not available): the per-Gaussian cache and the binning result, in the
+ * reference's layouts (splat_forward.cu:108-127, :210-214, :277). */
+typedef struct dgmr_splat_views {
+    int32_t* rects; /* [N,2] */
+    float* rgb; /* [N,3] */
+    uint8_t* rgb_sh_clamped; /* [N,3] */
+    float* depths; /* [N] */
+    float* points_xy_image; /* [N,2] */
+    float* conic_opacity; /* [N,4] */
+    int32_t* tiles_touched; /* [N] */
+    int32_t* point_offsets; /* [N] inclusive scan */
+    int32_t* i_ranges; /* [tiles,2] */
+    int32_t* point_list; /* [pair_capacity] Gaussian ids sorted by (tile, depth) */
+    uint32_t* point_list_tiles; /* [pair_capacity] tile id of each point_list entry */
+    float* final_transmittance; /* [H,W] */
+    int32_t* n_contrib; /* [H,W] */
+} dgmr_splat_views;
+
+dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* workspace, size_t workspace_bytes,
+    dgmr_splat_views* views);
+
+/* Backward splat (no reference kernel; the reference only has the pieces:
+ * grad/math.h:333-527, :203-282).  grad_framebuffer [3,H,W]; grads written
+ * (not accumulated) for sh [N,sh_stride,3], weights [N], centroids [N,3],
+ * scales [N,3], rotations [N,4]. */
+dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* camera, const float* grad_framebuffer, float* grad_sh, float* grad_weights,
+    float* grad_centroids, float* grad_scales, float* grad_rotations, void* workspace, size_t workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
+
+/* ---------------------------------------------------------- vol_marcher */
+
+/* The reference's ForwardCache plus framebuffer (vol_marcher_forward.h:28-41,
+ * returned in this order by python_bindings/vol_marcher.cu:109-122).  All
+ * caller-owned device buffers; element type T = scene dtype. */
+typedef struct dgmr_vm_cache {
+    void* framebuffer; /* [3,H,W] T */
+    int32_t* rects; /* [N,2] */
+    void* rgb; /* [N,3] T */
+    uint8_t* rgb_sh_clamped; /* [N,3] bool */
+    void* depths; /* [N] T */
+    void* points_xy_image; /* [N,2] T */
+    void* inverse_filtered_cov3d; /* [N,6] T, packed 00 01 02 11 12 22 */
+    void* filtered_masses; /* [N] T */
+    int32_t* tiles_touched; /* [N] */
+    int32_t* point_offsets; /* [N] inclusive scan */
+    int32_t* i_ranges; /* [tiles,2] */
+    int32_t* b_point_list; /* [pair_capacity] */
+    void* remaining_transparency; /* [H,W] T */
+} dgmr_vm_cache;
+
+/* Workspace for forward (binning) and backward (per-Gaussian accumulators). */
+size_t dgmr_vm_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, int32_t dtype);
+
+/* Replaces the first half of dgmr::vol_marcher::forward<T>
+ * (vol_marcher_forward.cu:98-191): per-Gaussian preprocess and the scan.
+ * Afterwards point_offsets[N-1] (also stats->n_pairs) is the pair count. */
+dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, void* workspace, size_t workspace_bytes,
+    dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Second half (vol_marcher_forward.cu:197-501): binning into b_point_list and
+ * i_ranges, then the ray march into framebuffer and remaining_transparency. */
+dgmr_status dgmr_vm_forward_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace,
+    size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Replaces dgmr::vol_marcher::backward<T> (vol_marcher_backward.cu:53-386).
+ * grad_framebuffer [3,H,W] T.  Grads are written (not accumulated): sh
+ * [N,sh_stride,3] (SH coefficients beyond sh_stride read as 1.0, as the
+ * reference pads with ones, vol_marcher.cu:177), weights [N], centroids [N,3],
+ * scales [N,3], rotations [N,4]. */
+dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* cache, const void* grad_framebuffer, void* grad_sh,
+    void* grad_weights, void* grad_centroids, void* grad_scales, void* grad_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats,
+    dgmr_stream stream);
+
+/* Gradient-check mode of the marcher (the reference's compile-time
+ * DGMR_TORCH_GRAD_CHECK_CONST_SAMPLES, vol_marcher_forward.cu:343-350): with
+ * n_sections > 0 every large step uses these fixed (start, end, delta_t)
+ * sections instead of collecting them from the Gaussians.  n_sections = 0
+ * restores adaptive sampling.  Process-wide; at most 4 sections. */
+dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections);
+
+/* ---------------------------------------------------------------- misc */
+const char* dgmr_status_string(dgmr_status status);
+/* Library version, e.g. "dgmr_b200 0.1 sm_100a". */
+const char* dgmr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGMR_B200_H */
