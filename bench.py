@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Served splat renders/s at 1080p with 1M Gaussians on B200.
+
+Workload (one step = one batch of ``--batch`` render requests): a resident
+scene of 1,000,000 Gaussians drawn as the reference's configuration 0
+(centroids U[-1,1]^3, scales log-uniform [0.005, 0.05], random unit
+quaternions, opacity sigmoid(N(0,1)), RGB as SH degree 0), requests are
+random cameras on a sphere of radius 2.5-4 around it, 1920x1080, 60 degree
+vertical field of view.  Synthetic seeded data (no dataset exists for this
+path).
+
+Legs:
+  value     served renders/s, images left in HBM (RenderServer, several
+            streams, no per-request host sync)
+  e2e       the same through the public API with every image copied to
+            pinned host memory inside the timed region
+  plain     the plain per-call path: one request at a time, pair count read
+            back per call (the reference's .item()), image copied to host
+  roofline  the blend kernel re-run alone under CUDA events
+  cpu       the CPU oracle (restated reference algorithm) on one frame
+
+``--impl reference`` times the CPU restatement of the reference's path on all
+host threads instead (the reference itself cannot be built here: its
+git-fetched dependencies are absent).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "served renders/s + p50/p99 ms vs plain per-call splat, 1080p, 1M Gaussians"
+UNIT = "renders/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--batch", type=int, default=8, help="requests per step")
+    ap.add_argument("--slots", type=int, default=3, help="requests in flight")
+    ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    return {"workload": f"splat forward, {args.n} Gaussians (config-0 distribution), {args.width}x{args.height}, "
+                        f"random cameras r=2.5-4, {args.batch} requests/step",
+            "n_gaussians": args.n, "width": args.width, "height": args.height, "requests_per_step": args.batch,
+            "slots_in_flight": args.slots,
+            "l2": "working set > 126 MB L2 (~9M pairs x 32 B of binning buffers per frame)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sms, maxs, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxs.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if sms:
+            out = {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
+                   "samples": len(sms)}
+        return out
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name: str):
+    """dram bytes per launch of a kernel from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(args, cams):
+    from oracle import oracle as O
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    sc = S.make_scene(args.n, seed=0)
+    O.splat_forward(sc, cams[0], want_keys=False)  # warm
+    t = time.perf_counter()
+    frames = 0
+    for cam in cams[:2]:
+        O.splat_forward(sc, cam, want_keys=False)
+        frames += 1
+        if time.perf_counter() - t > 20:
+            break
+    dt = time.perf_counter() - t
+    return {"value": frames / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{frames} full frame(s) of the same workload (oracle splat forward, OpenMP)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from oracle import oracle as O
+    sc = S.make_scene(args.n, seed=0)
+    cams = S.random_cameras(args.warmup + args.steps, args.width, args.height, seed=1)
+    for cam in cams[:args.warmup]:
+        O.splat_forward(sc, cam, want_keys=False)
+    t = time.perf_counter()
+    for cam in cams[args.warmup:]:
+        O.splat_forward(sc, cam, want_keys=False)
+    dt = time.perf_counter() - t
+    value = args.steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload(args), requests_per_step=1,
+                           note="CPU restatement of the reference's splat path (oracle/, OpenMP); the reference "
+                                "cannot be built here (its dependencies are fetched by git at build time)"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                             "sample": f"one full frame per step, {args.steps} steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.0
+    lo, hi = math.floor(k), math.ceil(k)
+    return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from differentiable_gaussian_mixture_renderer_b200 import _native as N
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200 import splat
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene, RenderServer, Request
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = N.lib()
+    sc_np = S.make_scene(args.n, seed=0)
+    scene = GaussianScene.from_numpy(sc_np, dev)
+    n_req = (args.warmup + args.steps) * args.batch
+    cams = S.random_cameras(2 * n_req + args.plain + 4, args.width, args.height, seed=1 + 1000 * rank)
+    server = RenderServer({"scene": scene}, dev, n_slots=args.slots)
+    for cam in cams[:4]:
+        server.estimate_capacity("scene", cam)
+
+    # ---------------------------------------------------------------- value leg
+    def served_leg(cam_list, to_host: bool):
+        for i in range(args.warmup * args.batch):
+            server.submit(Request("scene", cam_list[i], to_host=to_host))
+        server.drain()
+        server.completed.clear()
+        barrier()
+        launches0 = lib.dgmr_launch_count()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        server.start_clock()
+        start.record(server.slots[0].stream)
+        t_wall = time.perf_counter()
+        for i in range(args.steps * args.batch):
+            server.submit(Request("scene", cam_list[args.warmup * args.batch + i], to_host=to_host))
+        server.drain()
+        s0 = server.slots[0].stream
+        for sl in server.slots[1:]:
+            s0.wait_stream(sl.stream)
+        end.record(s0)
+        end.synchronize()
+        wall = time.perf_counter() - t_wall
+        barrier()
+        ms = start.elapsed_time(end)
+        lat = [(r.t_done - r.t_submit) * 1e3 for r in server.completed]
+        return ms, wall, lat, lib.dgmr_launch_count() - launches0, sum(r.rerendered for r in server.completed)
+
+    with ClockSampler(local) as clk:
+        ms_value, wall_value, lat_value, launches, rerenders = served_leg(cams[:n_req], to_host=False)
+        ms_e2e, wall_e2e, lat_e2e, _, _ = served_leg(cams[n_req:2 * n_req], to_host=True)
+    ms_value = max_over_ranks(ms_value)
+    ms_e2e = max_over_ranks(ms_e2e)
+    renders = args.steps * args.batch * world
+    value = renders / (ms_value * 1e-3)
+    e2e_value = renders / (ms_e2e * 1e-3)
+
+    # ---------------------------------------------------------------- plain per-call leg
+    plain_cams = cams[2 * n_req:2 * n_req + args.plain]
+    lat_plain = []
+    for cam in cams[:args.warmup]:  # warm the allocator and the path
+        fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations,
+                                    cam.view, cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height,
+                                    cam.tan_fovx, cam.tan_fovy, scene.sh_degree)
+        fb.cpu()
+    for i, cam in enumerate(plain_cams):
+        barrier()
+        t = time.perf_counter()
+        fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations,
+                                    cam.view, cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height,
+                                    cam.tan_fovx, cam.tan_fovy, scene.sh_degree)
+        img = fb.cpu()
+        lat_plain.append((time.perf_counter() - t) * 1e3)
+    plain_rps = len(lat_plain) / (sum(lat_plain) * 1e-3) * world if lat_plain else None
+
+    # ---------------------------------------------------------------- roofline of the blend
+    cam = cams[0]
+    fb, frame = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations, cam.view,
+                                    cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
+                                    cam.tan_fovy, scene.sh_degree)
+    torch.cuda.synchronize(dev)
+    n_pairs = int(frame.stats[0].item())
+    stream = torch.cuda.current_stream(dev)
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        N.check(lib.dgmr_splat_blend(frame.camera, frame.n, N.ptr(fb), *frame.ws_args(), frame.pair_capacity,
+                                     stream.cuda_stream), "blend")
+    e0.record(stream)
+    for _ in range(reps):
+        N.check(lib.dgmr_splat_blend(frame.camera, frame.n, N.ptr(fb), *frame.ws_args(), frame.pair_capacity,
+                                     stream.cuda_stream), "blend")
+    e1.record(stream)
+    e1.synchronize()
+    blend_ms = e0.elapsed_time(e1) / reps
+    tiles = ((args.width + 15) // 16) * ((args.height + 15) // 16)
+    px = args.width * args.height
+    # per pair: list id 4 B + xy 8 B + conic/opacity 16 B + rgb 12 B; per tile: range 8 B;
+    # per pixel: colour 12 B + transmittance 4 B + contributor count 4 B
+    blend_bytes = 40 * n_pairs + 8 * tiles + 20 * px
+    peak, peak_kind = peaks()
+    achieved = blend_bytes / (blend_ms * 1e-3) / 1e9
+    traffic = profiled_traffic("splat_blend_1080p_1M.txt")
+
+    # ---------------------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, cams)
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_value / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload(args), parallelism=f"replicas x{world}"),
+            "latency_ms": {"p50": pct(lat_value, 50), "p99": pct(lat_value, 99),
+                           "note": f"submit-to-done per request with {args.slots} requests in flight"},
+            "plain_per_call": {"value": plain_rps, "unit": UNIT, "p50_ms": pct(lat_plain, 50),
+                               "p99_ms": pct(lat_plain, 99), "requests": len(lat_plain),
+                               "note": "one request at a time: preprocess, pair count read back, render, image to host"},
+            "served_over_plain": (e2e_value / plain_rps) if plain_rps else None,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": args.batch * 8 * (16 + 16 + 3 + 3 + 3 + 1),
+                    "d2h_bytes_per_step": args.batch * 3 * args.width * args.height * 4,
+                    "p50_ms": pct(lat_e2e, 50), "p99_ms": pct(lat_e2e, 99)},
+            "roofline": {"kernel": "k_splat_blend", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "ms_per_launch": blend_ms, "n_pairs": n_pairs, "algorithmic_bytes": blend_bytes,
+                         "note": "blend is FP32/SFU-bound by construction; algorithmic bytes = 40 P + 8 T + 20 px"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+            "rerenders": int(rerenders),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

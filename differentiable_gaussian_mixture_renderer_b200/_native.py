@@ -57,14 +57,21 @@ class SplatViews(C.Structure):
 
 # every symbol include/dgmr_b200.h declares, with its ctypes signature
 _SIGNATURES = {
-    "dgmr_splat_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int64]),
+    "dgmr_splat_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "dgmr_splat_pair_workspace_size": (C.c_size_t, [C.c_int32, C.c_int64]),
     "dgmr_splat_forward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_void_p, C.c_size_t,
-                                     C.c_int64, C.c_void_p, C.c_void_p]),
+                                     C.c_void_p, C.c_size_t, C.c_int64, C.c_void_p, C.c_void_p]),
+    "dgmr_splat_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p,
+                                        C.c_void_p]),
+    "dgmr_splat_render": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_void_p, C.c_size_t,
+                                    C.c_void_p, C.c_size_t, C.c_int64, C.c_void_p, C.c_void_p]),
     "dgmr_splat_workspace_views": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_void_p, C.c_size_t,
-                                             C.POINTER(SplatViews)]),
+                                             C.c_void_p, C.c_size_t, C.POINTER(SplatViews)]),
+    "dgmr_splat_blend": (C.c_int, [C.POINTER(Camera), C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                   C.c_size_t, C.c_int64, C.c_void_p]),
     "dgmr_splat_backward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int64,
-                                      C.c_void_p]),
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.c_size_t, C.c_int64, C.c_void_p]),
     "dgmr_vm_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
     "dgmr_vm_forward_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p,
                                              C.c_size_t, C.c_void_p, C.c_void_p]),
@@ -76,6 +83,7 @@ _SIGNATURES = {
     "dgmr_vm_set_const_samples": (C.c_int, [C.c_int32, C.c_void_p]),
     "dgmr_status_string": (C.c_char_p, [C.c_int]),
     "dgmr_version": (C.c_char_p, []),
+    "dgmr_launch_count": (C.c_uint64, []),
 }
 
 _lib = None
@@ -150,7 +158,8 @@ def make_scene(shs, weights, centroids, scales, rotations, sh_degree: int) -> Sc
 def _host_values(t, n: int) -> list[float]:
     if isinstance(t, torch.Tensor):
         return [float(v) for v in t.detach().reshape(-1)[:n].cpu().double().tolist()]
-    return [float(v) for v in list(t)[:n]]
+    import numpy as np
+    return [float(v) for v in np.asarray(t, dtype=np.float64).reshape(-1)[:n]]
 
 
 def make_camera(view, proj, campos, background, width: int, height: int, tan_fovx: float, tan_fovy: float,

@@ -65,7 +65,8 @@ struct BinningBuffers {
     uint32_t* n_sort; // [1] pairs to sort = min(P, cap)
 };
 
-inline void carve_binning(Carver& c, BinningBuffers& b, uint32_t N, uint32_t cap)
+// the parts sized by the Gaussian count
+inline void carve_binning_gaussians(Carver& c, BinningBuffers& b, uint32_t N)
 {
     b.depth_key = c.take<uint32_t>(N);
     b.perm = c.take<uint32_t>(N);
@@ -73,13 +74,24 @@ inline void carve_binning(Carver& c, BinningBuffers& b, uint32_t N, uint32_t cap
     b.perm_tmp = c.take<uint32_t>(N);
     b.cnt_sorted = c.take<uint32_t>(N);
     b.off_sorted = c.take<uint32_t>(N);
+    b.scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
+    b.n_sort = c.take<uint32_t>(4);
+}
+
+// the parts sized by the pair capacity (and the sort scratch)
+inline void carve_binning_pairs(Carver& c, BinningBuffers& b, uint32_t N, uint32_t cap)
+{
     for (int i = 0; i < 2; ++i) {
         b.pair_tile[i] = c.take<uint32_t>(cap);
         b.pair_val[i] = c.take<uint32_t>(cap);
     }
-    b.scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
     b.sort_tmp = c.take<char>(radix_temp_bytes(N > cap ? N : cap));
-    b.n_sort = c.take<uint32_t>(4);
+}
+
+inline void carve_binning(Carver& c, BinningBuffers& b, uint32_t N, uint32_t cap)
+{
+    carve_binning_gaussians(c, b, N);
+    carve_binning_pairs(c, b, N, cap);
 }
 
 // parity of the buffer that holds the tile-sorted pairs
@@ -157,7 +169,7 @@ static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, 
 // filled by the preprocess.
 template <class T>
 inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* tiles_touched, uint32_t* point_offsets, const int32_t* rects, const T* xy,
-    uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s)
+    uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s, bool offsets_ready = false)
 {
     const uint32_t n_tiles = gx * gy;
     cudaMemsetAsync(ranges, 0, size_t(n_tiles) * 2 * sizeof(int32_t), s);
@@ -165,19 +177,28 @@ inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* til
         cudaMemsetAsync(b.n_sort, 0, sizeof(uint32_t), s);
         return tile_sort_parity(n_tiles);
     }
-    inclusive_scan_u32(tiles_touched, point_offsets, N, b.scan_tmp, s);
-    k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
+    if (!offsets_ready) {
+        inclusive_scan_u32(tiles_touched, point_offsets, N, b.scan_tmp, s);
+        k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
+        note_launch();
+    } else {
+        k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
+        note_launch();
+    }
     const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s);
     const uint32_t* perm = dpar ? b.perm_tmp : b.perm;
     const uint32_t blocks = (N + 255) / 256;
     k_gather_counts<<<blocks, 256, 0, s>>>(perm, tiles_touched, N, b.cnt_sorted);
+    note_launch();
     inclusive_scan_u32(b.cnt_sorted, b.off_sorted, N, b.scan_tmp, s);
     k_emit_pairs<T><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, gx, gy, cap, b.pair_tile[0], b.pair_val[0]);
+    note_launch();
     const int bits = int(higher_msb(n_tiles));
     const int par = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort, 0, cap, bits, b.sort_tmp, n_sms, s);
     if (cap > 0) {
         const uint32_t want = (cap + 255) / 256, limit = uint32_t(n_sms) * 16;
         k_tile_ranges<<<want < limit ? want : limit, 256, 0, s>>>(b.pair_tile[par], b.n_sort, ranges);
+        note_launch();
     }
     return par;
 }

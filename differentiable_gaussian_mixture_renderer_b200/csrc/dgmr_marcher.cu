@@ -597,8 +597,10 @@ dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dg
         c->rgb_sh_clamped, static_cast<T*>(c->depths), static_cast<T*>(c->points_xy_image), static_cast<T*>(c->inverse_filtered_cov3d),
         static_cast<T*>(c->filtered_masses), reinterpret_cast<uint32_t*>(c->tiles_touched), aa_multiplier(cam) };
     k_vm_preprocess<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    note_launch();
     inclusive_scan_u32(reinterpret_cast<uint32_t*>(c->tiles_touched), reinterpret_cast<uint32_t*>(c->point_offsets), N, Lw.pre_scan_tmp, s);
     k_pair_count<<<1, 1, 0, s>>>(reinterpret_cast<uint32_t*>(c->point_offsets), N, 0xffffffffu, st_dev, Lw.pre_scan_tmp);
+    note_launch();
     return launch_status();
 }
 
@@ -616,8 +618,10 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     BinningBuffers bin = L.bin;
     if (N > 0)
         k_depth_keys<T><<<(N + 255) / 256, 256, 0, s>>>(static_cast<const T*>(c->depths), N, bin.depth_key, bin.perm);
+    if (N > 0)
+        note_launch();
     const int par = run_binning<T>(N, cam.gx, cam.gy, reinterpret_cast<uint32_t*>(c->tiles_touched), reinterpret_cast<uint32_t*>(c->point_offsets), c->rects,
-        static_cast<T*>(c->points_xy_image), cap, bin, c->i_ranges, st_dev, num_sms(), s);
+        static_cast<T*>(c->points_xy_image), cap, bin, c->i_ranges, st_dev, num_sms(), s, true);
     if (cap > 0)
         cudaMemcpyAsync(c->b_point_list, bin.pair_val[par], size_t(cap) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
     VmMarch<T> a {};
@@ -633,6 +637,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.stats = st_dev;
     a.cs = const_samples<T>();
     k_vm_march<T><<<cam.gx * cam.gy, 256, 0, s>>>(a, cam);
+    note_launch();
     return launch_status();
 }
 
@@ -671,6 +676,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
         c->tiles_touched, L.acc, static_cast<T*>(g_sh), static_cast<T*>(g_weights), static_cast<T*>(g_centroids), static_cast<T*>(g_scales),
         static_cast<T*>(g_rotations), aa_multiplier(cam) };
     k_vm_bwd_gaussians<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    note_launch(2);
     return launch_status();
 }
 
@@ -767,5 +773,7 @@ const char* dgmr_status_string(dgmr_status status)
 }
 
 const char* dgmr_version(void) { return "dgmr_b200 0.1 sm_100a"; }
+
+uint64_t dgmr_launch_count(void) { return launch_counter().load(); }
 
 } // extern "C"

@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "dgmr_launch_count.h"
+
 namespace dgmr {
 
 constexpr int kSortThreads = 256;
@@ -330,6 +332,7 @@ inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* 
         k_radix_hist<<<grid, kSortThreads, 0, stream>>>(ki, n_dev, n_static, capacity, shift, mask, hist, stride);
         k_radix_scan_rows<<<kSortBins, kSortThreads, 0, stream>>>(hist, n_dev, n_static, capacity, stride, dtotal);
         k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal);
+        note_launch(3);
         cur ^= 1;
     }
     return cur;
@@ -347,6 +350,7 @@ inline void inclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, vo
     k_scan_tile_sums<<<tiles, kSortThreads, 0, stream>>>(in, n, sums);
     k_scan_tile_offsets<<<1, 1024, 0, stream>>>(sums, tiles);
     k_scan_apply<<<tiles, kSortThreads, 0, stream>>>(in, n, sums, out);
+    note_launch(3);
 }
 
 } // namespace dgmr

@@ -12,6 +12,8 @@
 
 namespace dgmr {
 
+// Frame workspace: everything sized by the Gaussian count, tiles and pixels.
+// Pair workspace: the (tile, Gaussian) pair buffers and sort scratch.
 struct SplatLayout {
     int32_t* rects;
     float* rgb;
@@ -27,10 +29,11 @@ struct SplatLayout {
     float* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3)
     uint32_t* stats; // [4] used when the caller passes none
     BinningBuffers bin;
-    size_t bytes;
+    size_t bytes; // frame workspace
+    size_t pair_bytes; // pair workspace
 };
 
-inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void* base)
+inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void* base, void* pair_base)
 {
     SplatLayout L;
     Carver c;
@@ -49,8 +52,12 @@ inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap
     L.n_contrib = c.take<int32_t>(size_t(W) * H);
     L.grad_acc = c.take<float>(size_t(N) * 9);
     L.stats = c.take<uint32_t>(4);
-    carve_binning(c, L.bin, N, cap);
+    carve_binning_gaussians(c, L.bin, N);
     L.bytes = c.off;
+    Carver cp;
+    cp.base = static_cast<char*>(pair_base);
+    carve_binning_pairs(cp, L.bin, N, cap);
+    L.pair_bytes = cp.off;
     return L;
 }
 
@@ -391,23 +398,69 @@ __global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, Ca
 
 using namespace dgmr;
 
-extern "C" {
+namespace {
 
-size_t dgmr_splat_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity)
+bool bad_sizes(int32_t n, int32_t w, int32_t h, int64_t cap)
 {
-    if (n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
-        return 0;
-    return splat_layout(uint32_t(n_gaussians), uint32_t(width), uint32_t(height), uint32_t(pair_capacity), nullptr).bytes;
+    return n < 0 || w <= 0 || h <= 0 || w > 65536 || h > 65536 || cap < 0 || cap > int64_t(0x7fffffff);
 }
 
-dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* workspace, size_t workspace_bytes,
-    dgmr_splat_views* views)
+SplatPre make_pre(const dgmr_scene* scene, const SplatLayout& L)
 {
-    if (!views || !workspace || n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+    return SplatPre { uint32_t(scene->n_gaussians), static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride,
+        scene->sh_degree, static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations),
+        L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm };
+}
+
+// per-Gaussian preprocess and the inclusive scan (splat_forward.cu:133-202)
+void launch_preprocess(const dgmr_scene* scene, const CameraT<float>& cam, const SplatLayout& L, uint32_t* st_dev, cudaStream_t s)
+{
+    const uint32_t N = uint32_t(scene->n_gaussians);
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    if (N == 0)
+        return;
+    k_splat_preprocess<<<(N + 255) / 256, 256, 0, s>>>(make_pre(scene, L), cam);
+    note_launch();
+    inclusive_scan_u32(L.tiles_touched, L.point_offsets, N, L.bin.scan_tmp, s);
+}
+
+// binning (after the preprocess) and the blend
+void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb, SplatLayout& L, uint32_t cap, uint32_t* st_dev, cudaStream_t s)
+{
+    const uint32_t N = uint32_t(scene->n_gaussians);
+    const int par
+        = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
+    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, fb, L.final_T, L.n_contrib, cam.W, cam.H,
+        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    note_launch();
+}
+
+} // namespace
+
+extern "C" {
+
+size_t dgmr_splat_frame_workspace_size(int32_t n_gaussians, int32_t width, int32_t height)
+{
+    if (bad_sizes(n_gaussians, width, height, 0))
+        return 0;
+    return splat_layout(uint32_t(n_gaussians), uint32_t(width), uint32_t(height), 0, nullptr, nullptr).bytes;
+}
+
+size_t dgmr_splat_pair_workspace_size(int32_t n_gaussians, int64_t pair_capacity)
+{
+    if (bad_sizes(n_gaussians, 1, 1, pair_capacity))
+        return 0;
+    return splat_layout(uint32_t(n_gaussians), 1, 1, uint32_t(pair_capacity), nullptr, nullptr).pair_bytes;
+}
+
+dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, dgmr_splat_views* views)
+{
+    if (!views || !frame_workspace || bad_sizes(n_gaussians, width, height, pair_capacity) || (pair_capacity > 0 && !pair_workspace))
         return DGMR_ERR_BAD_ARG;
     const uint32_t W = uint32_t(width), H = uint32_t(height);
-    const SplatLayout L = splat_layout(uint32_t(n_gaussians), W, H, uint32_t(pair_capacity), workspace);
-    if (workspace_bytes < L.bytes)
+    const SplatLayout L = splat_layout(uint32_t(n_gaussians), W, H, uint32_t(pair_capacity), frame_workspace, pair_workspace);
+    if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
         return DGMR_ERR_WORKSPACE;
     const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
     const int par = tile_sort_parity(gx * gy);
@@ -420,67 +473,120 @@ dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32
     views->tiles_touched = reinterpret_cast<int32_t*>(L.tiles_touched);
     views->point_offsets = reinterpret_cast<int32_t*>(L.point_offsets);
     views->i_ranges = L.ranges;
-    views->point_list = reinterpret_cast<int32_t*>(L.bin.pair_val[par]);
-    views->point_list_tiles = L.bin.pair_tile[par];
+    views->point_list = pair_workspace ? reinterpret_cast<int32_t*>(L.bin.pair_val[par]) : nullptr;
+    views->point_list_tiles = pair_workspace ? L.bin.pair_tile[par] : nullptr;
     views->final_transmittance = L.final_T;
     views->n_contrib = L.n_contrib;
     return DGMR_OK;
 }
 
-dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* workspace, size_t workspace_bytes,
-    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+dgmr_status dgmr_splat_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, void* frame_workspace, size_t frame_workspace_bytes,
+    dgmr_frame_stats* stats, dgmr_stream stream)
 {
     dgmr_status st = check_scene(scene, camera, DGMR_F32);
     if (st != DGMR_OK)
         return st;
-    if (!framebuffer || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+    if (!frame_workspace)
         return DGMR_ERR_BAD_ARG;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const uint32_t N = uint32_t(scene->n_gaussians), W = uint32_t(camera->width), H = uint32_t(camera->height), cap = uint32_t(pair_capacity);
-    const SplatLayout L = splat_layout(N, W, H, cap, workspace);
-    if (workspace_bytes < L.bytes)
+    const SplatLayout L = splat_layout(uint32_t(scene->n_gaussians), uint32_t(camera->width), uint32_t(camera->height), 0, frame_workspace, nullptr);
+    if (frame_workspace_bytes < L.bytes)
         return DGMR_ERR_WORKSPACE;
     const CameraT<float> cam = make_camera<float>(*camera);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
-    cudaMemsetAsync(st_dev, 0, 16, s);
-    BinningBuffers bin = L.bin;
-    if (N > 0) {
-        SplatPre p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
-            static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.rects, L.rgb,
-            L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, bin.depth_key, bin.perm };
-        k_splat_preprocess<<<(N + 255) / 256, 256, 0, s>>>(p, cam);
+    launch_preprocess(scene, cam, L, st_dev, s);
+    if (scene->n_gaussians > 0) {
+        k_pair_count<<<1, 1, 0, s>>>(L.point_offsets, uint32_t(scene->n_gaussians), 0xffffffffu, st_dev, L.bin.n_sort);
+        note_launch();
     }
-    const int par = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, bin, L.ranges, st_dev, num_sms(), s);
-    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, framebuffer, L.final_T, L.n_contrib, W, H, cam.gx,
-        cam.bg[0], cam.bg[1], cam.bg[2]);
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_render(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, DGMR_F32);
+    if (st != DGMR_OK)
+        return st;
+    if (!framebuffer || !frame_workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff) || (pair_capacity > 0 && !pair_workspace))
+        return DGMR_ERR_BAD_ARG;
+    SplatLayout L = splat_layout(uint32_t(scene->n_gaussians), uint32_t(camera->width), uint32_t(camera->height), uint32_t(pair_capacity), frame_workspace,
+        pair_workspace);
+    if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<float> cam = make_camera<float>(*camera);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    launch_render(scene, cam, framebuffer, L, uint32_t(pair_capacity), st_dev, s);
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, DGMR_F32);
+    if (st != DGMR_OK)
+        return st;
+    if (!framebuffer || !frame_workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff) || (pair_capacity > 0 && !pair_workspace))
+        return DGMR_ERR_BAD_ARG;
+    SplatLayout L = splat_layout(uint32_t(scene->n_gaussians), uint32_t(camera->width), uint32_t(camera->height), uint32_t(pair_capacity), frame_workspace,
+        pair_workspace);
+    if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<float> cam = make_camera<float>(*camera);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    launch_preprocess(scene, cam, L, st_dev, s);
+    launch_render(scene, cam, framebuffer, L, uint32_t(pair_capacity), st_dev, s);
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream)
+{
+    if (!camera || !framebuffer || !frame_workspace || bad_sizes(n_gaussians, camera->width, camera->height, pair_capacity)
+        || (pair_capacity > 0 && !pair_workspace))
+        return DGMR_ERR_BAD_ARG;
+    const SplatLayout L = splat_layout(uint32_t(n_gaussians), uint32_t(camera->width), uint32_t(camera->height), uint32_t(pair_capacity), frame_workspace,
+        pair_workspace);
+    if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
+        return DGMR_ERR_WORKSPACE;
+    const CameraT<float> cam = make_camera<float>(*camera);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int par = tile_sort_parity(cam.gx * cam.gy);
+    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, framebuffer, L.final_T, L.n_contrib, cam.W,
+        cam.H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    note_launch();
     return launch_status();
 }
 
 dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* camera, const float* grad_framebuffer, float* grad_sh, float* grad_weights,
-    float* grad_centroids, float* grad_scales, float* grad_rotations, void* workspace, size_t workspace_bytes, int64_t pair_capacity, dgmr_stream stream)
+    float* grad_centroids, float* grad_scales, float* grad_rotations, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace,
+    size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream)
 {
     dgmr_status st = check_scene(scene, camera, DGMR_F32);
     if (st != DGMR_OK)
         return st;
-    if (!grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations || !workspace || pair_capacity < 0
-        || pair_capacity > int64_t(0x7fffffff))
+    if (!grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations || !frame_workspace || pair_capacity < 0
+        || pair_capacity > int64_t(0x7fffffff) || (pair_capacity > 0 && !pair_workspace))
         return DGMR_ERR_BAD_ARG;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const uint32_t N = uint32_t(scene->n_gaussians), W = uint32_t(camera->width), H = uint32_t(camera->height), cap = uint32_t(pair_capacity);
-    const SplatLayout L = splat_layout(N, W, H, cap, workspace);
-    if (workspace_bytes < L.bytes)
+    const uint32_t N = uint32_t(scene->n_gaussians);
+    const SplatLayout L = splat_layout(N, uint32_t(camera->width), uint32_t(camera->height), uint32_t(pair_capacity), frame_workspace, pair_workspace);
+    if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
         return DGMR_ERR_WORKSPACE;
     if (N == 0)
         return DGMR_OK;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(cam.gx * cam.gy);
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
     k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.final_T, L.n_contrib, grad_framebuffer,
-        L.grad_acc, W, H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+        L.grad_acc, cam.W, cam.H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
         L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations };
     k_splat_bwd_gaussians<<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    note_launch(2);
     return launch_status();
 }
 

@@ -19,7 +19,8 @@ from . import _native as N
 @dataclass
 class SplatFrame:
     """Device state of one rendered frame (kept for the backward pass)."""
-    workspace: torch.Tensor
+    frame_ws: torch.Tensor
+    pair_ws: torch.Tensor
     pair_capacity: int
     stats: torch.Tensor  # int32[4]: n_pairs, flags, ...
     scene: N.Scene
@@ -28,20 +29,24 @@ class SplatFrame:
     width: int
     height: int
 
+    def ws_args(self):
+        return (N.ptr(self.frame_ws), self.frame_ws.numel(), N.ptr(self.pair_ws), self.pair_ws.numel())
+
     def views(self) -> dict:
         """Per-Gaussian cache and binning result as tensors (no copies)."""
         lib = N.lib()
         v = N.SplatViews()
-        N.check(lib.dgmr_splat_workspace_views(self.n, self.width, self.height, self.pair_capacity,
-                                               N.ptr(self.workspace), self.workspace.numel(), v), "workspace views")
-        base = self.workspace.data_ptr()
+        N.check(lib.dgmr_splat_workspace_views(self.n, self.width, self.height, self.pair_capacity, *self.ws_args(), v),
+                "workspace views")
         gx, gy = (self.width + 15) // 16, (self.height + 15) // 16
-        n, hw = self.n, self.width * self.height
+        n, hw, cap = self.n, self.width * self.height, self.pair_capacity
 
         def view(addr, count, dtype, shape):
+            buf = self.frame_ws if self.frame_ws.data_ptr() <= addr < self.frame_ws.data_ptr() + self.frame_ws.numel() \
+                else self.pair_ws
             elem = torch.tensor([], dtype=dtype).element_size()
-            off = addr - base
-            return self.workspace[off:off + count * elem].view(dtype).reshape(shape)
+            off = addr - buf.data_ptr()
+            return buf[off:off + count * elem].view(dtype).reshape(shape)
 
         return dict(rects=view(v.rects, 2 * n, torch.int32, (n, 2)), rgb=view(v.rgb, 3 * n, torch.float32, (n, 3)),
                     rgb_sh_clamped=view(v.rgb_sh_clamped, 3 * n, torch.uint8, (n, 3)),
@@ -51,8 +56,8 @@ class SplatFrame:
                     tiles_touched=view(v.tiles_touched, n, torch.int32, (n,)),
                     point_offsets=view(v.point_offsets, n, torch.int32, (n,)),
                     i_ranges=view(v.i_ranges, 2 * gx * gy, torch.int32, (gx * gy, 2)),
-                    point_list=view(v.point_list, self.pair_capacity, torch.int32, (self.pair_capacity,)),
-                    point_list_tiles=view(v.point_list_tiles, self.pair_capacity, torch.int32, (self.pair_capacity,)),
+                    point_list=view(v.point_list, cap, torch.int32, (cap,)),
+                    point_list_tiles=view(v.point_list_tiles, cap, torch.int32, (cap,)),
                     final_transmittance=view(v.final_transmittance, hw, torch.float32, (self.height, self.width)),
                     n_contrib=view(v.n_contrib, hw, torch.int32, (self.height, self.width)))
 
@@ -71,10 +76,13 @@ def splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, 
                   tanfovx: float, tanfovy: float, sh_degree: int, cov_scale_multiplier: float = 1.0,
                   pair_capacity: int | None = None, framebuffer: torch.Tensor | None = None,
                   stream: torch.cuda.Stream | None = None) -> tuple[torch.Tensor, SplatFrame]:
-    """Render one frame.  Without ``pair_capacity`` the pair buffers are sized
-    from the frame itself (one device->host read of the pair count, like the
-    reference's .item() at splat_forward.cu:204); with it, the call is
-    asynchronous and ``frame.stats`` reports an overflow instead."""
+    """Render one frame.
+
+    Without ``pair_capacity`` the pair buffers are sized from the frame itself:
+    preprocess, one device->host read of the pair count (the reference's
+    .item() at splat_forward.cu:204), then binning and blend.  With it the call
+    is asynchronous end to end; ``frame.stats[1] & 1`` then reports a frame
+    that needed more pairs than the capacity."""
     shs, opacity, means3D, scales, rotations = _prepare(shs, opacity, means3D, scales, rotations)
     lib = N.lib()
     dev = means3D.device
@@ -84,20 +92,20 @@ def splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, 
     fb = framebuffer if framebuffer is not None else torch.empty((3, H, W), dtype=torch.float32, device=dev)
     stats = torch.zeros(4, dtype=torch.int32, device=dev)
     sh = N.stream_handle(stream)
-    sync_size = pair_capacity is None
-    cap = int(pair_capacity) if pair_capacity is not None else max(4096, 8 * n)
-    while True:
-        ws = torch.empty(lib.dgmr_splat_workspace_size(n, W, H, cap), dtype=torch.uint8, device=dev)
-        N.check(lib.dgmr_splat_forward(scene, cam, N.ptr(fb), N.ptr(ws), ws.numel(), cap, N.ptr(stats), sh),
-                "splat forward")
-        if not sync_size:
-            break
-        n_pairs, flags = (int(v) for v in stats[:2].tolist())
-        if not (flags & N.FLAG_PAIR_OVERFLOW):
-            break
-        cap = n_pairs
-    frame = SplatFrame(ws, cap, stats, scene, cam, n, W, H)
-    return fb, frame
+    frame_ws = torch.empty(lib.dgmr_splat_frame_workspace_size(n, W, H), dtype=torch.uint8, device=dev)
+    if pair_capacity is None:
+        N.check(lib.dgmr_splat_preprocess(scene, cam, N.ptr(frame_ws), frame_ws.numel(), N.ptr(stats), sh),
+                "splat preprocess")
+        cap = int(stats[0].item())
+        pair_ws = torch.empty(max(1, lib.dgmr_splat_pair_workspace_size(n, cap)), dtype=torch.uint8, device=dev)
+        N.check(lib.dgmr_splat_render(scene, cam, N.ptr(fb), N.ptr(frame_ws), frame_ws.numel(), N.ptr(pair_ws),
+                                      pair_ws.numel(), cap, N.ptr(stats), sh), "splat render")
+    else:
+        cap = int(pair_capacity)
+        pair_ws = torch.empty(max(1, lib.dgmr_splat_pair_workspace_size(n, cap)), dtype=torch.uint8, device=dev)
+        N.check(lib.dgmr_splat_forward(scene, cam, N.ptr(fb), N.ptr(frame_ws), frame_ws.numel(), N.ptr(pair_ws),
+                                       pair_ws.numel(), cap, N.ptr(stats), sh), "splat forward")
+    return fb, SplatFrame(frame_ws, pair_ws, cap, stats, scene, cam, n, W, H)
 
 
 def splat_backward(frame: SplatFrame, grad_framebuffer: torch.Tensor, shs, opacity, means3D, scales, rotations,
@@ -117,8 +125,8 @@ def splat_backward(frame: SplatFrame, grad_framebuffer: torch.Tensor, shs, opaci
     g_s = torch.empty((n, 3), dtype=torch.float32, device=dev)
     g_q = torch.empty((n, 4), dtype=torch.float32, device=dev)
     N.check(lib.dgmr_splat_backward(frame.scene, frame.camera, N.ptr(g), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
-                                    N.ptr(g_s), N.ptr(g_q), N.ptr(frame.workspace), frame.workspace.numel(),
-                                    frame.pair_capacity, N.stream_handle(stream)), "splat backward")
+                                    N.ptr(g_s), N.ptr(g_q), *frame.ws_args(), frame.pair_capacity,
+                                    N.stream_handle(stream)), "splat backward")
     return g_sh, g_w, g_mu, g_s, g_q
 
 

@@ -75,18 +75,34 @@ typedef struct dgmr_camera {
 
 /* Replaces dgmr::splat_forward(SplatForwardData&) (src/dgmr/splat_forward.h:62,
  * reached through dgmr::sibr_interfaces::splat, src/dgmr/sibr_interfaces.h:25).
- * Bytes of workspace for one frame of n Gaussians at width x height with room
- * for pair_capacity (tile, Gaussian) pairs.  The workspace also keeps what the
- * backward pass needs, so keep it alive between forward and backward. */
-size_t dgmr_splat_workspace_size(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity);
+ *
+ * Two caller-owned workspaces per frame: the frame workspace holds the
+ * per-Gaussian, per-tile and per-pixel state (sized by the Gaussian count and
+ * the resolution); the pair workspace holds the (tile, Gaussian) pairs and the
+ * sort scratch (sized by pair_capacity).  Both must stay alive between a
+ * forward and its backward. */
+size_t dgmr_splat_frame_workspace_size(int32_t n_gaussians, int32_t width, int32_t height);
+size_t dgmr_splat_pair_workspace_size(int32_t n_gaussians, int64_t pair_capacity);
 
-/* Forward splat: framebuffer [3,H,W] f32 (device).  stats may be NULL. */
-dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* workspace, size_t workspace_bytes,
-    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+/* Forward splat in one call: framebuffer [3,H,W] f32 (device).  If the frame
+ * has more pairs than pair_capacity, stats->flags gets DGMR_FLAG_PAIR_OVERFLOW
+ * (pairs beyond the capacity are dropped).  stats may be NULL. */
+dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
 
-/* Views into the workspace after dgmr_splat_forward (device pointers, NULL if
- * not available): the per-Gaussian cache and the binning result, in the
- * reference's layouts (splat_forward.cu:108-127, :210-214, :277). */
+/* The same forward in two halves, for callers that size the pair workspace
+ * from the frame itself (the reference reads the pair count back with .item(),
+ * splat_forward.cu:204): preprocess (splat_forward.cu:133-202) leaves the pair
+ * count in stats->n_pairs and in point_offsets[N-1]; render (:208-398) does
+ * the binning and the blend. */
+dgmr_status dgmr_splat_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, void* frame_workspace, size_t frame_workspace_bytes,
+    dgmr_frame_stats* stats, dgmr_stream stream);
+dgmr_status dgmr_splat_render(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Views into the workspaces after a forward (device pointers): the
+ * per-Gaussian cache and the binning result, in the reference's layouts
+ * (splat_forward.cu:108-127, :210-214, :277). */
 typedef struct dgmr_splat_views {
     int32_t* rects; /* [N,2] */
     float* rgb; /* [N,3] */
@@ -103,15 +119,22 @@ typedef struct dgmr_splat_views {
     int32_t* n_contrib; /* [H,W] */
 } dgmr_splat_views;
 
-dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* workspace, size_t workspace_bytes,
-    dgmr_splat_views* views);
+dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32_t height, int64_t pair_capacity, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, dgmr_splat_views* views);
+
+/* Re-runs only the blend stage of the last forward made in these workspaces
+ * (same camera, Gaussian count and capacity), e.g. to time the blend kernel
+ * by itself.  Splits splat_forward.cu:305-398 out of the frame. */
+dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
+    void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
 
 /* Backward splat (no reference kernel; the reference only has the pieces:
  * grad/math.h:333-527, :203-282).  grad_framebuffer [3,H,W]; grads written
  * (not accumulated) for sh [N,sh_stride,3], weights [N], centroids [N,3],
  * scales [N,3], rotations [N,4]. */
 dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* camera, const float* grad_framebuffer, float* grad_sh, float* grad_weights,
-    float* grad_centroids, float* grad_scales, float* grad_rotations, void* workspace, size_t workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
+    float* grad_centroids, float* grad_scales, float* grad_rotations, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace,
+    size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
 
 /* ---------------------------------------------------------- vol_marcher */
 
@@ -168,6 +191,8 @@ dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections
 const char* dgmr_status_string(dgmr_status status);
 /* Library version, e.g. "dgmr_b200 0.1 sm_100a". */
 const char* dgmr_version(void);
+/* Number of kernels this library has launched in this process so far. */
+uint64_t dgmr_launch_count(void);
 
 #ifdef __cplusplus
 }

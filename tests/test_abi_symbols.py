@@ -34,8 +34,9 @@ def test_library_exports_every_declared_symbol():
 
 def test_workspace_queries_without_gpu():
     lib = _native.load()
-    assert lib.dgmr_splat_workspace_size(1000, 256, 256, 5000) > 0
-    assert lib.dgmr_splat_workspace_size(-1, 256, 256, 5000) == 0
+    assert lib.dgmr_splat_frame_workspace_size(1000, 256, 256) > 0
+    assert lib.dgmr_splat_pair_workspace_size(1000, 5000) > lib.dgmr_splat_pair_workspace_size(1000, 100)
+    assert lib.dgmr_splat_frame_workspace_size(-1, 256, 256) == 0
     assert lib.dgmr_vm_workspace_size(1000, 64, 64, 10, 1) > lib.dgmr_vm_workspace_size(1000, 64, 64, 10, 0)
     assert lib.dgmr_version().decode().startswith("dgmr_b200")
     assert lib.dgmr_status_string(2).decode() == "workspace too small"
@@ -47,7 +48,7 @@ def test_bad_arguments_are_rejected_on_the_host():
     cam = _native.Camera()
     cam.width, cam.height = 16, 16
     scene.n_gaussians, scene.sh_stride, scene.sh_degree, scene.dtype = 1, 0, 0, 0
-    assert lib.dgmr_splat_forward(scene, cam, None, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+    assert lib.dgmr_splat_forward(scene, cam, None, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
     scene.sh_stride = 1
-    assert lib.dgmr_splat_forward(scene, cam, None, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+    assert lib.dgmr_splat_forward(scene, cam, None, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
     assert lib.dgmr_vm_set_const_samples(5, None) == _native.DGMR_ERR_BAD_ARG
