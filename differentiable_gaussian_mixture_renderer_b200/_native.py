@@ -12,7 +12,7 @@ import torch
 
 from . import build as _build
 
-DGMR_OK, DGMR_ERR_BAD_ARG, DGMR_ERR_WORKSPACE, DGMR_ERR_CUDA = 0, 1, 2, 3
+DGMR_OK, DGMR_ERR_BAD_ARG, DGMR_ERR_WORKSPACE, DGMR_ERR_CUDA, DGMR_ERR_STATIC_SCRATCH = 0, 1, 2, 3, 4
 DGMR_F32, DGMR_F64 = 0, 1
 FLAG_PAIR_OVERFLOW, FLAG_STEP_LIMIT = 1, 2
 
@@ -69,6 +69,8 @@ _SIGNATURES = {
                                              C.c_void_p, C.c_size_t, C.POINTER(SplatViews)]),
     "dgmr_splat_blend": (C.c_int, [C.POINTER(Camera), C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                    C.c_size_t, C.c_int64, C.c_void_p]),
+    "dgmr_splat_forward_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p]),
     "dgmr_splat_backward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_size_t, C.c_int64, C.c_void_p]),

@@ -768,6 +768,8 @@ const char* dgmr_status_string(dgmr_status status)
         return "workspace too small";
     case DGMR_ERR_CUDA:
         return "CUDA launch error";
+    case DGMR_ERR_STATIC_SCRATCH:
+        return "frame exceeds the 64 MiB static scratch of the no-allocation entry point";
     }
     return "unknown status";
 }

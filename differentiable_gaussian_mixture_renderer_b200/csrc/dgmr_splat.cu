@@ -3,6 +3,7 @@
 // include/dgmr_b200.h.
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/dgmr_b200.h"
@@ -591,3 +592,82 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Splat forward without any device allocation.
+//
+// Some callers cannot hand this library a workspace: a plugin inside a host
+// application that owns every byte of GPU memory through its own pool, or
+// code running in a per-frame callback where a cudaMalloc would synchronise
+// the whole device and stall everything else in flight.  For them the frame
+// and pair workspaces live in one fixed-size array in device memory, defined
+// below, which every GPU that loads this library keeps until the process
+// exits.  A call whose two workspaces do not fit is rejected with
+// DGMR_ERR_STATIC_SCRATCH; nothing else is allocated.
+//
+// The array is shared by every call on a device and keeps whatever the last
+// call left in it.  The forward writes everything it later reads (the frame
+// statistics and tile ranges are cleared on the stream at the start of each
+// frame), so consecutive calls are independent -- but two calls that overlap
+// on the GPU (different streams, no ordering between them) race on the array
+// and corrupt each other's frame.
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(64) << 20; // 64 MiB per device
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+void* g_static_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  Host code must
+// not pass g_static_scratch itself to a kernel: on the host that name is only
+// a stand-in for the device symbol.  Looked up once per device, on the first
+// call made with that device current.
+dgmr_status static_scratch(void** out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return DGMR_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p)
+            return DGMR_ERR_CUDA;
+        g_static_ptr[dev] = p;
+    }
+    *out = g_static_ptr[dev];
+    return DGMR_OK;
+}
+
+} // namespace
+
+extern "C" dgmr_status dgmr_splat_forward_noalloc(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, int64_t pair_capacity,
+    dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, DGMR_F32);
+    if (st != DGMR_OK)
+        return st;
+    if (!framebuffer || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    const uint32_t N = uint32_t(scene->n_gaussians), W = uint32_t(camera->width), H = uint32_t(camera->height), cap = uint32_t(pair_capacity);
+    const SplatLayout sizes = splat_layout(N, W, H, cap, nullptr, nullptr);
+    const size_t frame_bytes = align_up(sizes.bytes);
+    if (frame_bytes + sizes.pair_bytes > kStaticScratchBytes)
+        return DGMR_ERR_STATIC_SCRATCH;
+    void* base = nullptr;
+    st = static_scratch(&base);
+    if (st != DGMR_OK)
+        return st;
+    char* frame_ws = static_cast<char*>(base);
+    char* pair_ws = frame_ws + frame_bytes;
+    SplatLayout L = splat_layout(N, W, H, cap, frame_ws, pair_ws);
+    const CameraT<float> cam = make_camera<float>(*camera);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    launch_preprocess(scene, cam, L, st_dev, s);
+    launch_render(scene, cam, framebuffer, L, cap, st_dev, s);
+    return launch_status();
+}

@@ -29,6 +29,7 @@ typedef enum dgmr_status {
     DGMR_ERR_BAD_ARG = 1, /* null pointer, negative size, sh_stride/degree out of range */
     DGMR_ERR_WORKSPACE = 2, /* workspace smaller than the query returned */
     DGMR_ERR_CUDA = 3, /* a launch failed; cudaGetLastError() holds the cause */
+    DGMR_ERR_STATIC_SCRATCH = 4, /* frame too large for dgmr_splat_forward_noalloc's 64 MiB scratch */
 } dgmr_status;
 
 /* Device-side frame statistics (caller-owned, 16 bytes, written by the calls
@@ -127,6 +128,21 @@ dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32
  * by itself.  Splits splat_forward.cu:305-398 out of the frame. */
 dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
     void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
+
+/* Splat forward that allocates nothing -- no counterpart in the reference.
+ * For callers that cannot provide or allocate device memory on the render
+ * path (a plugin whose host application owns all GPU memory; a per-frame
+ * callback where cudaMalloc would synchronise the device).  Both workspaces
+ * live in one static 64 MiB device array that every GPU loading the library
+ * holds until exit; frames whose frame + pair workspaces
+ * (dgmr_splat_frame_workspace_size + dgmr_splat_pair_workspace_size) exceed
+ * it return DGMR_ERR_STATIC_SCRATCH.  The first call on each device looks up
+ * the array's device address (make that first call before any stream
+ * capture).  All calls on a device share the array: calls that overlap on the
+ * GPU race and corrupt each other; calls ordered on one stream are fine.
+ * Results equal dgmr_splat_forward's; the workspace views are not available. */
+dgmr_status dgmr_splat_forward_noalloc(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, int64_t pair_capacity,
+    dgmr_frame_stats* stats, dgmr_stream stream);
 
 /* Backward splat (no reference kernel; the reference only has the pieces:
  * grad/math.h:333-527, :203-282).  grad_framebuffer [3,H,W]; grads written
