@@ -315,9 +315,9 @@ def run_ours(args):
     blend_ms = e0.elapsed_time(e1) / reps
     tiles = ((args.width + 15) // 16) * ((args.height + 15) // 16)
     px = args.width * args.height
-    # per pair: list id 4 B + xy 8 B + conic/opacity 16 B + rgb 12 B; per tile: range 8 B;
+    # per pair: list id 4 B + 32-byte splat record + rgb 12 B; per tile: range 8 B;
     # per pixel: colour 12 B + transmittance 4 B + contributor count 4 B
-    blend_bytes = 40 * n_pairs + 8 * tiles + 20 * px
+    blend_bytes = 48 * n_pairs + 8 * tiles + 20 * px
     peak, peak_kind = peaks()
     achieved = blend_bytes / (blend_ms * 1e-3) / 1e9
     traffic = profiled_traffic("splat_blend_1080p_1M.txt")
@@ -347,7 +347,7 @@ def run_ours(args):
             "roofline": {"kernel": "k_splat_blend", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "ms_per_launch": blend_ms, "n_pairs": n_pairs, "algorithmic_bytes": blend_bytes,
-                         "note": "blend is FP32/SFU-bound by construction; algorithmic bytes = 40 P + 8 T + 20 px"},
+                         "note": "blend is FP32-bound by construction; algorithmic bytes = 48 P + 8 T + 20 px"},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),

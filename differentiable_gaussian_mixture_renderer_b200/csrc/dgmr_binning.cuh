@@ -110,45 +110,112 @@ static __global__ void k_pair_count(const uint32_t* __restrict__ point_offsets, 
     *n_sort = P < cap ? P : cap;
 }
 
-static __global__ void k_gather_counts(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tiles_touched, uint32_t N, uint32_t* __restrict__ cnt_sorted)
+static __global__ void k_gather_counts(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tiles_touched, uint32_t N, uint32_t* __restrict__ cnt_sorted,
+    uint32_t* __restrict__ stats)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < N)
-        cnt_sorted[j] = tiles_touched[perm[j]];
+    if (j < N) {
+        const uint32_t g = perm[j];
+        if (g < N) {
+            cnt_sorted[j] = tiles_touched[g];
+        } else {
+            cnt_sorted[j] = 0;
+            flag_bounds(stats, 0x21u);
+        }
+    }
 }
 
 // Pairs in depth order: for the j-th Gaussian by depth, one entry per tile
-// its rectangle touches (util.h:42-52 applied to the cached rect + centroid).
+// its rectangle touches, row-major (util.h:42-52 applied to the cached rect
+// and centroid).  The 32 Gaussians of a warp own one contiguous output range
+// (their offsets come from an inclusive scan in the same order), so the warp
+// writes that range together: in each round lane l takes slot base + l and
+// finds its owner -- the first lane whose inclusive end exceeds the slot -- by
+// a five-step binary search over the lanes' ends, done with shuffles.
 template <class T>
-static __global__ void k_emit_pairs(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ cnt_sorted, const uint32_t* __restrict__ off_sorted,
-    const int32_t* __restrict__ rects, const T* __restrict__ xy, uint32_t N, unsigned gx, unsigned gy, uint32_t cap, uint32_t* __restrict__ pair_tile,
-    uint32_t* __restrict__ pair_val)
+static __global__ void __launch_bounds__(256) k_emit_pairs(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ cnt_sorted,
+    const uint32_t* __restrict__ off_sorted, const int32_t* __restrict__ rects, const T* __restrict__ xy, uint32_t N, unsigned gx, unsigned gy, uint32_t cap,
+    uint32_t* __restrict__ pair_tile, uint32_t* __restrict__ pair_val, uint32_t* __restrict__ stats)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N)
+    const int lane = threadIdx.x & 31;
+    if (__all_sync(0xffffffffu, j >= N))
         return;
-    const uint32_t c = cnt_sorted[j];
-    if (c == 0)
-        return;
-    const uint32_t g = perm[j];
-    uint32_t off = off_sorted[j] - c;
-    const TileRect r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], gx, gy);
-    for (unsigned y = r.y0; y < r.y1; ++y)
-        for (unsigned x = r.x0; x < r.x1; ++x) {
-            if (off < cap) {
-                pair_tile[off] = y * gx + x;
-                pair_val[off] = g;
+    uint32_t c = 0, end = 0, g = 0;
+    TileRect r = { 0, 0, 0, 0 };
+    if (j < N) {
+        c = cnt_sorted[j];
+        end = off_sorted[j];
+        if (c > 0) {
+            g = perm[j];
+            if (g < N) {
+                r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], gx, gy);
+                if ((r.x1 - r.x0) * (r.y1 - r.y0) != c) {
+                    flag_bounds(stats, 0x22u);
+                    r = { 0, 0, 0, 0 };
+                }
+            } else {
+                flag_bounds(stats, 0x23u);
+                g = 0;
             }
-            ++off;
         }
+    }
+    const uint32_t start = end - c;
+    // inclusive ends, non-decreasing across the warp; lanes past N sort last
+    const uint32_t key = j < N ? end : 0xffffffffu;
+    const uint32_t lo = __shfl_sync(0xffffffffu, start, 0);
+    uint32_t hi = j < N ? end : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    const uint32_t rw = r.x1 - r.x0;
+    for (uint32_t base = lo; base < hi; base += 32) {
+        const uint32_t pos = base + lane;
+        // first lane with end > pos (that lane's count is > 0 whenever pos < hi)
+        int a = 0, b = 31;
+#pragma unroll
+        for (int it = 0; it < 5; ++it) {
+            const int mid = (a + b) >> 1;
+            const uint32_t m = __shfl_sync(0xffffffffu, key, mid);
+            if (m > pos)
+                b = mid;
+            else
+                a = mid + 1;
+        }
+        const int src = a;
+        const uint32_t s_start = __shfl_sync(0xffffffffu, start, src);
+        const uint32_t s_c = __shfl_sync(0xffffffffu, c, src);
+        const uint32_t s_g = __shfl_sync(0xffffffffu, g, src);
+        const uint32_t s_x0 = __shfl_sync(0xffffffffu, r.x0, src);
+        const uint32_t s_y0 = __shfl_sync(0xffffffffu, r.y0, src);
+        const uint32_t s_w = __shfl_sync(0xffffffffu, rw, src);
+        if (pos < hi && pos < cap) {
+            const uint32_t k = pos - s_start;
+            const uint32_t t = (s_w && k < s_c) ? (s_y0 + k / s_w) * gx + s_x0 + k % s_w : 0xffffffffu;
+            if (t < gx * gy) {
+                pair_tile[pos] = t;
+                pair_val[pos] = s_g;
+            } else {
+                pair_tile[pos] = 0;
+                pair_val[pos] = 0;
+                flag_bounds(stats, 0x24u);
+            }
+        }
+    }
 }
 
 // splat_forward.cu:281-302 on the tile-sorted list (ranges zeroed beforehand)
-static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, const uint32_t* __restrict__ n_dev, int32_t* __restrict__ ranges)
+static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, const uint32_t* __restrict__ n_dev, int32_t* __restrict__ ranges, uint32_t n_tiles,
+    uint32_t* __restrict__ stats)
 {
     const uint32_t n = *n_dev;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         const uint32_t cur = tiles_sorted[idx];
+        const uint32_t prev_t = idx ? tiles_sorted[idx - 1] : 0u;
+        if (cur >= n_tiles || prev_t >= n_tiles) {
+            flag_bounds(stats, 0x25u);
+            continue;
+        }
         if (idx == 0)
             ranges[2 * cur] = 0;
         else {
@@ -185,19 +252,19 @@ inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* til
         k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
         note_launch();
     }
-    const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s);
+    const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s, stats);
     const uint32_t* perm = dpar ? b.perm_tmp : b.perm;
     const uint32_t blocks = (N + 255) / 256;
-    k_gather_counts<<<blocks, 256, 0, s>>>(perm, tiles_touched, N, b.cnt_sorted);
+    k_gather_counts<<<blocks, 256, 0, s>>>(perm, tiles_touched, N, b.cnt_sorted, stats);
     note_launch();
     inclusive_scan_u32(b.cnt_sorted, b.off_sorted, N, b.scan_tmp, s);
-    k_emit_pairs<T><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, gx, gy, cap, b.pair_tile[0], b.pair_val[0]);
+    k_emit_pairs<T><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, gx, gy, cap, b.pair_tile[0], b.pair_val[0], stats);
     note_launch();
     const int bits = int(higher_msb(n_tiles));
-    const int par = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort, 0, cap, bits, b.sort_tmp, n_sms, s);
+    const int par = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort, 0, cap, bits, b.sort_tmp, n_sms, s, stats);
     if (cap > 0) {
         const uint32_t want = (cap + 255) / 256, limit = uint32_t(n_sms) * 16;
-        k_tile_ranges<<<want < limit ? want : limit, 256, 0, s>>>(b.pair_tile[par], b.n_sort, ranges);
+        k_tile_ranges<<<want < limit ? want : limit, 256, 0, s>>>(b.pair_tile[par], b.n_sort, ranges, n_tiles, stats);
         note_launch();
     }
     return par;

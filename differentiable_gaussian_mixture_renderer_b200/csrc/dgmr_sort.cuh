@@ -21,6 +21,17 @@ constexpr int kSortItemsPerThread = 8;
 constexpr int kSortTile = kSortThreads * kSortItemsPerThread; // 2048 items per tile
 constexpr int kSortBins = 256; // 8-bit digits
 
+// Guards on data-dependent indices: a violated guard skips the access, sets
+// bit 2 of the frame flags and records the first site's code in stats[3].
+constexpr uint32_t kFlagBounds = 4u;
+__device__ __forceinline__ void flag_bounds(uint32_t* stats, uint32_t site)
+{
+    if (stats) {
+        atomicOr(&stats[1], kFlagBounds);
+        atomicCAS(&stats[3], 0u, site);
+    }
+}
+
 __device__ __forceinline__ uint32_t dev_count(const uint32_t* n_dev, uint32_t n_static, uint32_t capacity)
 {
     const uint32_t n = n_dev ? *n_dev : n_static;
@@ -155,14 +166,12 @@ static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, const uin
             (&h[0][0])[i] = 0;
         __syncthreads();
         const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+        // per-warp histograms keep shared-memory atomic contention inside one warp
+#pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
             const uint32_t idx = base + r * 32 + lane;
-            const bool valid = idx < n;
-            const uint32_t d = valid ? ((keys[idx] >> shift) & mask) : 0xffffffffu;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            if (valid && lane == __ffs(peers) - 1)
-                h[warp][d] += __popc(peers);
-            __syncwarp();
+            if (idx < n)
+                atomicAdd(&h[warp][(keys[idx] >> shift) & mask], 1u);
         }
         __syncthreads();
         uint32_t t = 0;
@@ -222,7 +231,7 @@ static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint
 // its items in order with __match_any_sync, so equal digits keep input order.
 static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask, const uint32_t* __restrict__ hist,
-    uint32_t tile_stride, const uint32_t* __restrict__ digit_total)
+    uint32_t tile_stride, const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ stats)
 {
     __shared__ uint32_t wcount[kSortWarps][kSortBins];
     __shared__ uint32_t gbase[kSortBins];
@@ -293,8 +302,12 @@ static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, con
             if (idx < n) {
                 const uint32_t d = (k[r] >> shift) & mask;
                 const uint32_t pos = gbase[d] + wcount[warp][d] + rank[r];
-                keys_out[pos] = k[r];
-                vals_out[pos] = v[r];
+                if (pos < n) {
+                    keys_out[pos] = k[r];
+                    vals_out[pos] = v[r];
+                } else {
+                    flag_bounds(stats, 0x11u);
+                }
             }
         }
         __syncthreads();
@@ -312,7 +325,7 @@ inline size_t radix_temp_bytes(uint32_t capacity)
 // between (k0, v0) and (k1, v1); returns 0 if the result is in k0/v0, 1 if in
 // k1/v1.  n comes from *n_dev (device) when non-null, else n_static.
 inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int end_bit,
-    void* temp, int n_sms, cudaStream_t stream)
+    void* temp, int n_sms, cudaStream_t stream, uint32_t* stats = nullptr)
 {
     const uint32_t tiles = (capacity + kSortTile - 1) / kSortTile;
     if (tiles == 0)
@@ -331,7 +344,7 @@ inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* 
         uint32_t* vo = cur ? v0 : v1;
         k_radix_hist<<<grid, kSortThreads, 0, stream>>>(ki, n_dev, n_static, capacity, shift, mask, hist, stride);
         k_radix_scan_rows<<<kSortBins, kSortThreads, 0, stream>>>(hist, n_dev, n_static, capacity, stride, dtotal);
-        k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal);
+        k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal, stats);
         note_launch(3);
         cur ^= 1;
     }

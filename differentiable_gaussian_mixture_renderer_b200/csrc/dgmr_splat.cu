@@ -28,6 +28,7 @@ struct SplatLayout {
     float* final_T;
     int32_t* n_contrib;
     float* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3)
+    float4* blend_rec; // [N,2]: (x, y, a, c), (2b, opacity, q_cut, 0) -- the blend's 32-byte record
     uint32_t* stats; // [4] used when the caller passes none
     BinningBuffers bin;
     size_t bytes; // frame workspace
@@ -52,6 +53,7 @@ inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap
     L.final_T = c.take<float>(size_t(W) * H);
     L.n_contrib = c.take<int32_t>(size_t(W) * H);
     L.grad_acc = c.take<float>(size_t(N) * 9);
+    L.blend_rec = c.take<float4>(size_t(N) * 2);
     L.stats = c.take<uint32_t>(4);
     carve_binning_gaussians(c, L.bin, N);
     L.bytes = c.off;
@@ -79,6 +81,7 @@ struct SplatPre {
     uint32_t* tiles_touched;
     uint32_t* depth_key;
     uint32_t* perm;
+    float4* blend_rec;
 };
 
 // splat_forward.cu:137-180
@@ -101,6 +104,8 @@ __global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<fl
         p.clamped[3 * i + c] = 0;
     }
     reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    p.blend_rec[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    p.blend_rec[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
     const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
     if (view_z(cam.view, mu) < 0.2f)
         return;
@@ -136,80 +141,140 @@ __global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<fl
         p.clamped[3 * i + c] = mask[c];
     const S2<float> con = inverse2(g.cov);
     reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(con.v[0], con.v[1], con.v[2], g.weight);
+    // q_cut: any pixel with d'Qd > q_cut has opacity * exp(-d'Qd/2) < exp(-1e-3) / 255, i.e. alpha < 1/255
+    // with a margin far above the rounding of the exponential, so the blend may skip it without changing
+    // a single result
+    const float q_cut = 2.f * (dgmr_fm::log_f(255.f * g.weight) + 1e-3f);
+    p.blend_rec[2 * i] = make_float4(g.centroid.x, g.centroid.y, con.v[0], con.v[2]);
+    p.blend_rec[2 * i + 1] = make_float4(2.f * con.v[1], g.weight, q_cut, 0.f);
 }
 
-// (pixel, splat) evaluation of splat_forward.cu:365-370
-__device__ __forceinline__ float splat_gauss(float4 co, float2 xy, float px, float py, float* dx_o, float* dy_o)
+// d'Qd of one (pixel, splat) pair (splat_forward.cu:365), evaluated as
+// dx * (a dx + 2b dy) + (c dy) dy with two fused multiply-adds; r0 = (x, y, a, c), b2 = 2b
+__device__ __forceinline__ float splat_q(float4 r0, float b2, float px, float py, float* dx_o, float* dy_o)
 {
-    const float dx = px - xy.x;
-    const float dy = py - xy.y;
-    const float q = ((co.x * dx) * dx + (co.z * dy) * dy) + ((2.f * co.y) * dx) * dy;
+    const float dx = px - r0.x;
+    const float dy = py - r0.y;
     *dx_o = dx;
     *dy_o = dy;
-    return dgmr_fm::exp_f(-0.5f * q);
+    return __fmaf_rn(__fmaf_rn(r0.z, dx, b2 * dy), dx, (r0.w * dy) * dy);
 }
 
-// One 16x16 tile per block, one pixel per thread; batches of 256 splats staged
-// in shared memory; the block stops when every pixel is saturated.
-__global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float* __restrict__ xy,
-    const float* __restrict__ conic_opacity, const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib,
-    unsigned W, unsigned H, unsigned gx, float bg0, float bg1, float bg2)
+__device__ __forceinline__ float splat_gauss(float4 co, float2 xy, float px, float py, float* dx_o, float* dy_o)
 {
-    __shared__ float2 s_xy[256];
-    __shared__ float4 s_co[256];
-    __shared__ float s_rgb[3][256];
+    const float4 r0 = make_float4(xy.x, xy.y, co.x, co.z);
+    return dgmr_fm::exp_f(-0.5f * splat_q(r0, 2.f * co.y, px, py, dx_o, dy_o));
+}
+
+// Per-pixel blend step shared by both pixels a thread owns
+// (splat_forward.cu:365-384).
+struct PixelState {
+    float T, c0, c1, c2;
+    int32_t last;
+    bool done;
+};
+
+__device__ __forceinline__ void blend_step(PixelState& ps, float q, float qcut, float opacity, float r, float g, float b, int32_t idx)
+{
+    if (ps.done || q > qcut)
+        return;
+    const float alpha = min_f(0.99f, opacity * dgmr_fm::exp_f(-0.5f * q));
+    if (alpha < 1.0f / 255.0f)
+        return;
+    const float test_T = ps.T * (1.f - alpha);
+    if (test_T < 0.0001f) {
+        ps.done = true;
+        return;
+    }
+    const float w = alpha * ps.T;
+    ps.c0 = __fmaf_rn(r, w, ps.c0);
+    ps.c1 = __fmaf_rn(g, w, ps.c1);
+    ps.c2 = __fmaf_rn(b, w, ps.c2);
+    ps.T = test_T;
+    ps.last = idx;
+}
+
+// One 16x16 tile per block of 128 threads, two pixels per thread (rows y and
+// y + 8); batches of 256 splats are staged in shared memory as 32-byte records
+// and evaluated by both pixels.  Pairs beyond a splat's q_cut skip the
+// exponential; the block stops when every pixel is saturated.
+__global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
+    const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib, unsigned W, unsigned H, unsigned gx,
+    float bg0, float bg1, float bg2, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats)
+{
+    constexpr int kBatch = 256;
+    __shared__ float4 s_r0[kBatch];
+    __shared__ float4 s_r1[kBatch];
+    __shared__ float s_rgb[3][kBatch];
     const unsigned tile = blockIdx.x;
     const unsigned tx = tile % gx, ty = tile / gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
-    const bool inside = px < W && py < H;
-    bool done = !inside;
-    const int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
-    float Tr = 1.f, C0 = 0.f, C1 = 0.f, C2 = 0.f;
-    int32_t last = 0;
-    const float fpx = float(px), fpy = float(py);
-    for (int32_t base = b; base < e; base += 256) {
-        if (__syncthreads_count(done) == 256)
+    const unsigned px = tx * kTile + (threadIdx.x & 15u);
+    const unsigned py0 = ty * kTile + (threadIdx.x >> 4), py1 = py0 + 8;
+    PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py0 < H) };
+    PixelState p1 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py1 < H) };
+    const bool in0 = !p0.done, in1 = !p1.done;
+    int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
+    if (b < 0 || e < b || uint32_t(e) > cap) {
+        if (threadIdx.x == 0)
+            flag_bounds(stats, 0x31u);
+        b = e = 0;
+    }
+    const float fpx = float(px), fpy0 = float(py0), fpy1 = float(py1);
+    for (int32_t base = b; base < e; base += kBatch) {
+        if (__syncthreads_count(p0.done && p1.done) == int(blockDim.x))
             break;
-        const int32_t k = base + int32_t(threadIdx.x);
-        if (k < e) {
-            const uint32_t id = list[k];
-            s_xy[threadIdx.x] = reinterpret_cast<const float2*>(xy)[id];
-            s_co[threadIdx.x] = reinterpret_cast<const float4*>(conic_opacity)[id];
-            s_rgb[0][threadIdx.x] = rgb[3 * id];
-            s_rgb[1][threadIdx.x] = rgb[3 * id + 1];
-            s_rgb[2][threadIdx.x] = rgb[3 * id + 2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int slot = int(threadIdx.x) + h * 128;
+            const int32_t k = base + slot;
+            if (k < e) {
+                uint32_t id = list[k];
+                if (id >= N) {
+                    flag_bounds(stats, 0x32u);
+                    id = 0;
+                }
+                s_r0[slot] = rec[2 * size_t(id)];
+                s_r1[slot] = rec[2 * size_t(id) + 1];
+                s_rgb[0][slot] = rgb[3 * size_t(id)];
+                s_rgb[1][slot] = rgb[3 * size_t(id) + 1];
+                s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
+            }
         }
         __syncthreads();
-        if (done)
+        if (p0.done && p1.done)
             continue;
-        const int n = min(256, e - base);
+        const int n = min(kBatch, e - base);
         for (int j = 0; j < n; ++j) {
+            const float4 r0 = s_r0[j];
+            const float4 r1 = s_r1[j];
+            const int32_t idx = base + j - b + 1;
             float dx, dy;
-            const float4 co = s_co[j];
-            const float g = splat_gauss(co, s_xy[j], fpx, fpy, &dx, &dy);
-            const float alpha = min_f(0.99f, co.w * g);
-            if (alpha < 1.0f / 255.0f)
+            const float q0 = splat_q(r0, r1.x, fpx, fpy0, &dx, &dy);
+            const float q1 = splat_q(r0, r1.x, fpx, fpy1, &dx, &dy);
+            if ((p0.done || q0 > r1.z) && (p1.done || q1 > r1.z))
                 continue;
-            const float test_T = Tr * (1.f - alpha);
-            if (test_T < 0.0001f) {
-                done = true;
-                break;
-            }
-            C0 = C0 + (s_rgb[0][j] * alpha) * Tr;
-            C1 = C1 + (s_rgb[1][j] * alpha) * Tr;
-            C2 = C2 + (s_rgb[2][j] * alpha) * Tr;
-            Tr = test_T;
-            last = base + j - b + 1;
+            const float cr = s_rgb[0][j], cg = s_rgb[1][j], cb = s_rgb[2][j];
+            blend_step(p0, q0, r1.z, r1.y, cr, cg, cb, idx);
+            blend_step(p1, q1, r1.z, r1.y, cr, cg, cb, idx);
         }
     }
-    if (!inside)
-        return;
-    const size_t pix = size_t(py) * W + px;
-    fb[pix] = C0 + Tr * bg0;
-    fb[size_t(W) * H + pix] = C1 + Tr * bg1;
-    fb[2 * size_t(W) * H + pix] = C2 + Tr * bg2;
-    final_T[pix] = Tr;
-    n_contrib[pix] = last;
+    const size_t plane = size_t(W) * H;
+    if (in0) {
+        const size_t pix = size_t(py0) * W + px;
+        fb[pix] = p0.c0 + p0.T * bg0;
+        fb[plane + pix] = p0.c1 + p0.T * bg1;
+        fb[2 * plane + pix] = p0.c2 + p0.T * bg2;
+        final_T[pix] = p0.T;
+        n_contrib[pix] = p0.last;
+    }
+    if (in1) {
+        const size_t pix = size_t(py1) * W + px;
+        fb[pix] = p1.c0 + p1.T * bg0;
+        fb[plane + pix] = p1.c1 + p1.T * bg1;
+        fb[2 * plane + pix] = p1.c2 + p1.T * bg2;
+        final_T[pix] = p1.T;
+        n_contrib[pix] = p1.last;
+    }
 }
 
 __device__ __forceinline__ float warp_sum(float v)
@@ -410,7 +475,7 @@ SplatPre make_pre(const dgmr_scene* scene, const SplatLayout& L)
 {
     return SplatPre { uint32_t(scene->n_gaussians), static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride,
         scene->sh_degree, static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations),
-        L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm };
+        L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm, L.blend_rec };
 }
 
 // per-Gaussian preprocess and the inclusive scan (splat_forward.cu:133-202)
@@ -431,8 +496,8 @@ void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb
     const uint32_t N = uint32_t(scene->n_gaussians);
     const int par
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
-    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, fb, L.final_T, L.n_contrib, cam.W, cam.H,
-        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, fb, L.final_T, L.n_contrib, cam.W, cam.H, cam.gx,
+        cam.bg[0], cam.bg[1], cam.bg[2], N, cap, st_dev);
     note_launch();
 }
 
@@ -555,8 +620,8 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
     const CameraT<float> cam = make_camera<float>(*camera);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int par = tile_sort_parity(cam.gx * cam.gy);
-    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, framebuffer, L.final_T, L.n_contrib, cam.W,
-        cam.H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, framebuffer, L.final_T, L.n_contrib, cam.W, cam.H,
+        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2], uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats);
     note_launch();
     return launch_status();
 }

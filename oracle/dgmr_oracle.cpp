@@ -237,13 +237,15 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
     }
 }
 
-// alpha of one (pixel, splat) pair, splat_forward.cu:365-370
+// alpha of one (pixel, splat) pair, splat_forward.cu:365-370.  The quadratic
+// form d'Qd is evaluated as dx * (a dx + 2b dy) + (c dy) dy with two fused
+// multiply-adds, in this order (the device blend uses the same sequence).
 template <class T>
 inline T splat_alpha(const T* co, const T* xy, T px, T py, T* g_out = nullptr, T* dx_out = nullptr, T* dy_out = nullptr)
 {
     const T dx = px - xy[0];
     const T dy = py - xy[1];
-    const T q = ((co[0] * dx) * dx + (co[2] * dy) * dy) + ((T(2) * co[1]) * dx) * dy;
+    const T q = std::fma(std::fma(co[0], dx, (T(2) * co[1]) * dy), dx, (co[2] * dy) * dy);
     const T g = dgmr_fm::exp_f(T(-0.5f) * q);
     if (g_out) {
         *g_out = g;
@@ -280,9 +282,11 @@ void splat_blend(const SceneIn<T>& s, const T* rgb, const T* xy, const T* conic_
                     const T test_T = Tr * (T(1) - alpha);
                     if (test_T < T(0.0001f))
                         break;
-                    C.x = C.x + (rgb[3 * id] * alpha) * Tr;
-                    C.y = C.y + (rgb[3 * id + 1] * alpha) * Tr;
-                    C.z = C.z + (rgb[3 * id + 2] * alpha) * Tr;
+                    // C += rgb * alpha * T, as one product and three fused multiply-adds
+                    const T wgt = alpha * Tr;
+                    C.x = std::fma(rgb[3 * id], wgt, C.x);
+                    C.y = std::fma(rgb[3 * id + 1], wgt, C.y);
+                    C.z = std::fma(rgb[3 * id + 2], wgt, C.z);
                     Tr = test_T;
                     last = k - b + 1;
                 }
