@@ -194,18 +194,53 @@ __device__ __forceinline__ void blend_step(PixelState& ps, float q, float qcut, 
     ps.last = idx;
 }
 
+// Minimum of d'Qd over the tile's pixel rectangle [x0,x1] x [y0,y1] for a
+// splat at (cx, cy) with conic (a, b, c): 0 if the centre is inside, else the
+// minimum over the four edges (each a clamped 1-D quadratic).  Returns 0 (keep)
+// for a conic that is not positive definite.  Only used to drop splats with a
+// wide margin, so approximate division is fine here.
+__device__ __forceinline__ float rect_min_q(float cx, float cy, float a, float b, float c, float x0, float x1, float y0, float y1)
+{
+    if (!(a > 0.f && c > 0.f && a * c - b * b > 0.f))
+        return 0.f;
+    if (cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1)
+        return 0.f;
+    const auto q = [&](float dx, float dy) { return a * dx * dx + 2.f * b * dx * dy + c * dy * dy; };
+    float m = 3.0e38f;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float dx = (e == 0 ? x0 : x1) - cx;
+        const float dy = fminf(fmaxf(cy - __fdividef(b * dx, c), y0), y1) - cy;
+        m = fminf(m, q(dx, dy));
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float dy = (e == 0 ? y0 : y1) - cy;
+        const float dx = fminf(fmaxf(cx - __fdividef(b * dy, a), x0), x1) - cx;
+        m = fminf(m, q(dx, dy));
+    }
+    return m;
+}
+
 // One 16x16 tile per block of 128 threads, two pixels per thread (rows y and
-// y + 8); batches of 256 splats are staged in shared memory as 32-byte records
-// and evaluated by both pixels.  Pairs beyond a splat's q_cut skip the
-// exponential; the block stops when every pixel is saturated.
+// y + 8).  Each batch of up to 256 list entries is loaded two per thread;
+// splats whose cutoff ellipse cannot reach the tile are dropped (an exact
+// rectangle minimum with a margin, so no pixel that could pass its own cutoff
+// test loses a splat); the rest are compacted in list order into shared memory
+// as 32-byte records and evaluated by both pixels.  The block stops when every
+// pixel is saturated.
 __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
     const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib, unsigned W, unsigned H, unsigned gx,
     float bg0, float bg1, float bg2, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats)
 {
-    constexpr int kBatch = 256;
+    constexpr int kThreads = 128;
+    constexpr int kPer = 2; // list entries loaded per thread per batch
+    constexpr int kBatch = kThreads * kPer;
+    constexpr int kWarps = kThreads / 32;
     __shared__ float4 s_r0[kBatch];
-    __shared__ float4 s_r1[kBatch];
+    __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
     __shared__ float s_rgb[3][kBatch];
+    __shared__ int s_warp_tot[kWarps];
     const unsigned tile = blockIdx.x;
     const unsigned tx = tile % gx, ty = tile / gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u);
@@ -219,44 +254,83 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
             flag_bounds(stats, 0x31u);
         b = e = 0;
     }
+    const float fx0 = float(tx * kTile), fx1 = fx0 + 15.f, fy0 = float(ty * kTile), fy1 = fy0 + 15.f;
     const float fpx = float(px), fpy0 = float(py0), fpy1 = float(py1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int32_t base = b; base < e; base += kBatch) {
-        if (__syncthreads_count(p0.done && p1.done) == int(blockDim.x))
+        const bool all_done = p0.done && p1.done;
+        if (__syncthreads_count(all_done) == kThreads)
             break;
+        float4 r0[kPer], r1[kPer];
+        uint32_t id[kPer];
+        int keep = 0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int slot = int(threadIdx.x) + h * 128;
-            const int32_t k = base + slot;
+        for (int h = 0; h < kPer; ++h) {
+            const int32_t k = base + int(threadIdx.x) * kPer + h;
+            id[h] = 0xffffffffu;
             if (k < e) {
-                uint32_t id = list[k];
-                if (id >= N) {
+                uint32_t g = list[k];
+                if (g >= N) {
                     flag_bounds(stats, 0x32u);
-                    id = 0;
+                    g = 0;
                 }
-                s_r0[slot] = rec[2 * size_t(id)];
-                s_r1[slot] = rec[2 * size_t(id) + 1];
-                s_rgb[0][slot] = rgb[3 * size_t(id)];
-                s_rgb[1][slot] = rgb[3 * size_t(id) + 1];
-                s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
+                r0[h] = rec[2 * size_t(g)];
+                r1[h] = rec[2 * size_t(g) + 1];
+                const float qmin = rect_min_q(r0[h].x, r0[h].y, r0[h].z, 0.5f * r1[h].x, r0[h].w, fx0, fx1, fy0, fy1);
+                if (!(qmin > r1[h].z * 1.001f + 0.01f)) {
+                    id[h] = g;
+                    r1[h].w = __int_as_float(k - b + 1);
+                    ++keep;
+                }
+            }
+        }
+        // order-preserving compaction: exclusive scan of the per-thread counts
+        int x = keep;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            s_warp_tot[warp] = x;
+        __syncthreads();
+        int slot = x - keep;
+        int n = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const int t = s_warp_tot[w];
+            slot += (w < warp) ? t : 0;
+            n += t;
+        }
+#pragma unroll
+        for (int h = 0; h < kPer; ++h) {
+            if (id[h] != 0xffffffffu) {
+                s_r0[slot] = r0[h];
+                s_r1[slot] = r1[h];
+                s_rgb[0][slot] = rgb[3 * size_t(id[h])];
+                s_rgb[1][slot] = rgb[3 * size_t(id[h]) + 1];
+                s_rgb[2][slot] = rgb[3 * size_t(id[h]) + 2];
+                ++slot;
             }
         }
         __syncthreads();
-        if (p0.done && p1.done)
-            continue;
-        const int n = min(kBatch, e - base);
-        for (int j = 0; j < n; ++j) {
-            const float4 r0 = s_r0[j];
-            const float4 r1 = s_r1[j];
-            const int32_t idx = base + j - b + 1;
-            float dx, dy;
-            const float q0 = splat_q(r0, r1.x, fpx, fpy0, &dx, &dy);
-            const float q1 = splat_q(r0, r1.x, fpx, fpy1, &dx, &dy);
-            if ((p0.done || q0 > r1.z) && (p1.done || q1 > r1.z))
-                continue;
-            const float cr = s_rgb[0][j], cg = s_rgb[1][j], cb = s_rgb[2][j];
-            blend_step(p0, q0, r1.z, r1.y, cr, cg, cb, idx);
-            blend_step(p1, q1, r1.z, r1.y, cr, cg, cb, idx);
+        if (!all_done) {
+            for (int j = 0; j < n; ++j) {
+                const float4 a0 = s_r0[j];
+                const float4 a1 = s_r1[j];
+                float dx, dy;
+                const float q0 = splat_q(a0, a1.x, fpx, fpy0, &dx, &dy);
+                const float q1 = splat_q(a0, a1.x, fpx, fpy1, &dx, &dy);
+                if ((p0.done || q0 > a1.z) && (p1.done || q1 > a1.z))
+                    continue;
+                const float cr = s_rgb[0][j], cg = s_rgb[1][j], cb = s_rgb[2][j];
+                const int32_t idx = __float_as_int(a1.w);
+                blend_step(p0, q0, a1.z, a1.y, cr, cg, cb, idx);
+                blend_step(p1, q1, a1.z, a1.y, cr, cg, cb, idx);
+            }
         }
+        __syncthreads();
     }
     const size_t plane = size_t(W) * H;
     if (in0) {
