@@ -229,22 +229,27 @@ static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint
 
 // Stable scatter: warp w of a tile owns a contiguous 256-item slice and ranks
 // its items in order with __match_any_sync, so equal digits keep input order.
-static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
-    uint32_t* __restrict__ vals_out, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask, const uint32_t* __restrict__ hist,
-    uint32_t tile_stride, const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ stats)
+// The tile is first rearranged in shared memory into digit order, then written
+// out so that consecutive threads store consecutive addresses of each digit's
+// run (coalesced), instead of every lane storing into a different bucket.
+static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask,
+    const uint32_t* __restrict__ hist, uint32_t tile_stride, const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ stats)
 {
     __shared__ uint32_t wcount[kSortWarps][kSortBins];
-    __shared__ uint32_t gbase[kSortBins];
+    __shared__ uint32_t gbase[kSortBins]; // global start of this tile's run of each digit
+    __shared__ uint32_t lbase[kSortBins]; // start of each digit's run inside the tile
     __shared__ uint32_t dbase[kSortBins];
     __shared__ uint32_t warp_tot[kSortWarps];
+    __shared__ uint32_t s_key[kSortTile];
+    __shared__ uint32_t s_val[kSortTile];
     const uint32_t n = dev_count(n_dev, n_static, capacity);
     const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
 
-    // digit bases: exclusive scan of the 256 digit totals
-    {
-        const uint32_t v = digit_total[threadIdx.x];
+    // block-wide exclusive scan of one value per thread (256 threads)
+    const auto block_excl_scan = [&](uint32_t v) -> uint32_t {
         uint32_t x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -259,15 +264,19 @@ static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, con
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w)
             wex += (w < warp) ? warp_tot[w] : 0;
-        dbase[threadIdx.x] = wex + x - v;
         __syncthreads();
-    }
+        return wex + x - v;
+    };
+
+    dbase[threadIdx.x] = block_excl_scan(digit_total[threadIdx.x]);
+    __syncthreads();
 
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         for (int i = threadIdx.x; i < kSortWarps * kSortBins; i += kSortThreads)
             (&wcount[0][0])[i] = 0;
         __syncthreads();
-        const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
+        const uint32_t tile_base = tile * kSortTile;
+        const uint32_t base = tile_base + warp * (kSortTile / kSortWarps);
         uint32_t k[kSortItemsPerThread], v[kSortItemsPerThread], rank[kSortItemsPerThread];
 #pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
@@ -284,30 +293,42 @@ static __global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in, con
             __syncwarp();
         }
         __syncthreads();
+        // per digit: prefix over warps (in place) and the tile's count of that digit
+        uint32_t count = 0;
         {
             const uint32_t d = threadIdx.x;
-            uint32_t run = 0;
 #pragma unroll
             for (int w = 0; w < kSortWarps; ++w) {
                 const uint32_t t = wcount[w][d];
-                wcount[w][d] = run;
-                run += t;
+                wcount[w][d] = count;
+                count += t;
             }
             gbase[d] = dbase[d] + hist[d * tile_stride + tile];
         }
+        lbase[threadIdx.x] = block_excl_scan(count);
         __syncthreads();
+        // digit-ordered staging in shared memory
 #pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
             const uint32_t idx = base + r * 32 + lane;
             if (idx < n) {
                 const uint32_t d = (k[r] >> shift) & mask;
-                const uint32_t pos = gbase[d] + wcount[warp][d] + rank[r];
-                if (pos < n) {
-                    keys_out[pos] = k[r];
-                    vals_out[pos] = v[r];
-                } else {
-                    flag_bounds(stats, 0x11u);
-                }
+                const uint32_t lpos = lbase[d] + wcount[warp][d] + rank[r];
+                s_key[lpos] = k[r];
+                s_val[lpos] = v[r];
+            }
+        }
+        __syncthreads();
+        const uint32_t in_tile = (n - tile_base) < uint32_t(kSortTile) ? (n - tile_base) : uint32_t(kSortTile);
+        for (uint32_t i = threadIdx.x; i < in_tile; i += kSortThreads) {
+            const uint32_t key = s_key[i];
+            const uint32_t d = (key >> shift) & mask;
+            const uint32_t pos = gbase[d] + (i - lbase[d]);
+            if (pos < n) {
+                keys_out[pos] = key;
+                vals_out[pos] = s_val[i];
+            } else {
+                flag_bounds(stats, 0x11u);
             }
         }
         __syncthreads();
