@@ -230,6 +230,36 @@ static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, 
     }
 }
 
+// Launch order for the per-tile kernels: tiles bucketed by floor(log2(list
+// length + 1)), longest first, so the heaviest tiles start at the head of the
+// grid instead of stretching its tail.  One block; order inside a bucket is
+// arbitrary (it only affects scheduling, never results).
+static __global__ void __launch_bounds__(1024) k_tile_order(const int32_t* __restrict__ ranges, uint32_t n_tiles, uint32_t* __restrict__ order)
+{
+    __shared__ uint32_t count[33];
+    __shared__ uint32_t cursor[33];
+    if (threadIdx.x < 33)
+        count[threadIdx.x] = 0;
+    __syncthreads();
+    const auto bucket = [&](uint32_t t) {
+        const int32_t len = ranges[2 * t + 1] - ranges[2 * t];
+        return 32u - uint32_t(32 - __clz(len > 0 ? len : 0)); // 32 - bit length: long lists -> small bucket
+    };
+    for (uint32_t t = threadIdx.x; t < n_tiles; t += blockDim.x)
+        atomicAdd(&count[bucket(t)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int b = 0; b < 33; ++b) {
+            cursor[b] = run;
+            run += count[b];
+        }
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < n_tiles; t += blockDim.x)
+        order[atomicAdd(&cursor[bucket(t)], 1u)] = t;
+}
+
 // Full binning: point_offsets (inclusive scan, reference order), depth sort,
 // emission, tile sort and ranges.  Returns the buffer index holding the
 // sorted (tile, Gaussian) pairs.  Requires b.perm = iota and b.depth_key

@@ -356,8 +356,13 @@ inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* 
     uint32_t* dtotal = hist + size_t(kSortBins) * stride;
     const uint32_t grid = tiles < uint32_t(n_sms * 8) ? tiles : uint32_t(n_sms * 8);
     int cur = 0;
-    for (int shift = 0; shift < end_bit; shift += 8) {
-        const int bits = (end_bit - shift) < 8 ? (end_bit - shift) : 8;
+    // fewest 8-bit-or-narrower passes, with the bits spread evenly over them
+    // (e.g. 13 tile bits -> 7 + 6): fewer buckets per pass keep the runs each
+    // tile writes per digit longer
+    const int n_pass = (end_bit + 7) / 8;
+    const int width = n_pass ? (end_bit + n_pass - 1) / n_pass : 8;
+    for (int shift = 0; shift < end_bit; shift += width) {
+        const int bits = (end_bit - shift) < width ? (end_bit - shift) : width;
         const uint32_t mask = (1u << bits) - 1u;
         uint32_t* ki = cur ? k1 : k0;
         uint32_t* vi = cur ? v1 : v0;

@@ -29,6 +29,7 @@ struct SplatLayout {
     int32_t* n_contrib;
     float* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3)
     float4* blend_rec; // [N,2]: (x, y, a, c), (2b, opacity, q_cut, 0) -- the blend's 32-byte record
+    uint32_t* tile_order; // [tiles] launch order of the per-tile kernels, heaviest first
     uint32_t* stats; // [4] used when the caller passes none
     BinningBuffers bin;
     size_t bytes; // frame workspace
@@ -54,6 +55,7 @@ inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap
     L.n_contrib = c.take<int32_t>(size_t(W) * H);
     L.grad_acc = c.take<float>(size_t(N) * 9);
     L.blend_rec = c.take<float4>(size_t(N) * 2);
+    L.tile_order = c.take<uint32_t>(size_t(gx) * gy);
     L.stats = c.take<uint32_t>(4);
     carve_binning_gaussians(c, L.bin, N);
     L.bytes = c.off;
@@ -231,7 +233,7 @@ __device__ __forceinline__ float rect_min_q(float cx, float cy, float a, float b
 // pixel is saturated.
 __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
     const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib, unsigned W, unsigned H, unsigned gx,
-    float bg0, float bg1, float bg2, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats)
+    float bg0, float bg1, float bg2, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, const uint32_t* __restrict__ tile_order)
 {
     constexpr int kThreads = 128;
     constexpr int kPer = 2; // list entries loaded per thread per batch
@@ -241,7 +243,7 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
     __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
     __shared__ float s_rgb[3][kBatch];
     __shared__ int s_warp_tot[kWarps];
-    const unsigned tile = blockIdx.x;
+    const unsigned tile = tile_order ? tile_order[blockIdx.x] : blockIdx.x;
     const unsigned tx = tile % gx, ty = tile / gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u);
     const unsigned py0 = ty * kTile + (threadIdx.x >> 4), py1 = py0 + 8;
@@ -570,9 +572,10 @@ void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb
     const uint32_t N = uint32_t(scene->n_gaussians);
     const int par
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
+    k_tile_order<<<1, 1024, 0, s>>>(L.ranges, cam.gx * cam.gy, L.tile_order);
     k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, fb, L.final_T, L.n_contrib, cam.W, cam.H, cam.gx,
-        cam.bg[0], cam.bg[1], cam.bg[2], N, cap, st_dev);
-    note_launch();
+        cam.bg[0], cam.bg[1], cam.bg[2], N, cap, st_dev, L.tile_order);
+    note_launch(2);
 }
 
 } // namespace
@@ -695,7 +698,7 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int par = tile_sort_parity(cam.gx * cam.gy);
     k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, framebuffer, L.final_T, L.n_contrib, cam.W, cam.H,
-        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2], uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats);
+        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2], uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats, L.tile_order);
     note_launch();
     return launch_status();
 }
