@@ -17,7 +17,8 @@
 //    field.
 //  * log: x = m*2^e with m in [sqrt(1/2), sqrt(2)); log(m) = 2*atanh(s),
 //    s = (m-1)/(m+1), by its odd power series to s^11 (|s| < 0.172).
-//  * erf: Abramowitz & Stegun, Handbook of Mathematical Functions, eq. 7.1.26
+//  * erf: for |x| < 1 the Maclaurin series (Abramowitz & Stegun, Handbook
+//    of Mathematical Functions, eq. 7.1.5) to x^23; above, eq. 7.1.26
 //    (Hastings' approximation, |error| <= 1.5e-7), saturated to +-1 for
 //    |x| >= 3.92 where the true erf already rounds to 1 in float.
 // Double-precision overloads forward to the platform's correctly-rounding-ish
@@ -201,7 +202,25 @@ DGMR_HD float erf_f(float x)
         return x;
     const float ax = x < 0.0f ? -x : x;
     float y;
-    if (ax >= 3.92f) {
+    if (ax < 1.0f) {
+        // Maclaurin series (A&S 7.1.5): erf(x) = 2/sqrt(pi) sum (-1)^n x^(2n+1) / (n! (2n+1)),
+        // through n = 11 (truncation < 2e-9 at |x| = 1); avoids the cancellation of
+        // 7.1.26 for small arguments
+        const float z = ax * ax;
+        float p = -1.22905553017179263e-09f; // -2/sqrt(pi) / 918086400
+        p = fma_f(p, z, 1.48071928158792176e-08f); // 2/sqrt(pi) / 76204800
+        p = fma_f(p, z, -1.63658446912349245e-07f); // -2/sqrt(pi) / 6894720
+        p = fma_f(p, z, 1.64621143658892463e-06f); // 2/sqrt(pi) / 685440
+        p = fma_f(p, z, -1.49256503584062504e-05f); // -2/sqrt(pi) / 75600
+        p = fma_f(p, z, 1.20553329817896636e-04f); // 2/sqrt(pi) / 9360
+        p = fma_f(p, z, -8.54832702345085225e-04f); // -2/sqrt(pi) / 1320
+        p = fma_f(p, z, 5.22397762544218793e-03f); // 2/sqrt(pi) / 216
+        p = fma_f(p, z, -2.68661706451312522e-02f); // -2/sqrt(pi) / 42
+        p = fma_f(p, z, 1.12837916709551261e-01f); // 2/sqrt(pi) / 10
+        p = fma_f(p, z, -3.76126389031837538e-01f); // -2/sqrt(pi) / 3
+        p = fma_f(p, z, 1.12837916709551256e+00f); // 2/sqrt(pi) / 1
+        y = ax * p;
+    } else if (ax >= 3.92f) {
         y = 1.0f;
     } else {
         // Abramowitz & Stegun 7.1.26

@@ -1,0 +1,164 @@
+// Capacity-bounded set of sample sections of the volume marcher and the walk
+// that turns it into sample positions (host and device code).
+//
+// Semantics follow src/dgmr/marching_steps.h:35-220 (DensityArray, sample).
+// A section {start, end, delta_t} asks for samples at most delta_t apart
+// inside [start, end).  Inserting a section that overlaps existing ones splits
+// them and keeps the smaller delta_t on the overlap; when the set is full,
+// sections that no longer fit are dropped and the set's end is pulled in.
+// Which sections survive that truncation is part of the rendered result and
+// is pinned by the reference's known-answer tests, so the insertion steps are
+// kept one to one.
+#pragma once
+
+#include "dgmr_fmath.h"
+
+#if defined(__CUDACC__)
+#define DGMR_HD_NOINLINE __host__ __device__ __noinline__
+#else
+#define DGMR_HD_NOINLINE
+#endif
+
+namespace dgmr {
+
+using dgmr_fm::max_f;
+using dgmr_fm::min_f;
+
+template <class T>
+struct Section {
+    T start, end, delta_t;
+};
+
+template <unsigned MAX, class T>
+struct SectionSet {
+    unsigned n;
+    T lo, hi;
+    Section<T> e[MAX];
+
+    DGMR_HD void reset(T start)
+    {
+        n = 0;
+        lo = start;
+        hi = T(1) / T(0);
+    }
+
+    DGMR_HD static void combine(const Section<T>& a, const Section<T>& b, Section<T> out[3])
+    {
+        if (a.start < b.start)
+            out[0] = { a.start, min_f(a.end, b.start), a.delta_t };
+        else
+            out[0] = { b.start, min_f(b.end, a.start), b.delta_t };
+        if (b.end < a.end)
+            out[2] = { b.end, a.end, a.delta_t };
+        else
+            out[2] = { a.end, b.end, b.delta_t };
+        out[1] = { out[0].end, out[2].start, min_f(a.delta_t, b.delta_t) };
+    }
+
+    DGMR_HD_NOINLINE void put(Section<T> s)
+    {
+        if (s.end <= lo)
+            return;
+        if (s.start >= hi)
+            return;
+        s.start = max_f(lo, s.start);
+        s.end = min_f(hi, s.end);
+        unsigned first = n;
+        for (unsigned i = 0; i < n; ++i)
+            if (e[i].end > s.start) {
+                first = i;
+                break;
+            }
+        if (first >= n) {
+            if (first < MAX)
+                e[n++] = s;
+            else
+                hi = s.start;
+            return;
+        }
+        unsigned last = n;
+        for (unsigned i = first; i < n; ++i)
+            if (e[i].end > s.end) {
+                last = i;
+                break;
+            }
+        if (last < n && e[last].start < s.end)
+            ++last;
+        Section<T> ring[MAX];
+        unsigned r_read = 0, r_write = 0;
+        unsigned i_read = first, i_write = first;
+        unsigned grown = 0;
+        while (i_read < last + grown && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            if (r_read >= r_write)
+                break;
+            const Section<T> head = ring[r_read % MAX];
+            if (head.end <= s.start) {
+                e[i_write++] = ring[(r_read++) % MAX];
+                continue;
+            }
+            if (head.start >= s.end)
+                break;
+            Section<T> p[3];
+            combine(ring[(r_read++) % MAX], s, p);
+            if (p[0].delta_t == p[1].delta_t) {
+                p[1].start = p[0].start;
+                p[0].end = p[0].start;
+            }
+            s = p[2];
+            if (p[0].end - p[0].start <= T(0)) {
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                e[i_write++] = p[1];
+            } else {
+                e[i_write++] = p[0];
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                ++grown;
+                ring[(--r_read) % MAX] = p[1];
+            }
+        }
+        if (s.end - s.start > T(0) && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            e[i_write++] = s;
+        }
+        while (r_write - r_read && i_write < MAX) {
+            if (i_read < n)
+                ring[(r_write++) % MAX] = e[i_read++];
+            e[i_write++] = ring[(r_read++) % MAX];
+        }
+        n = i_write + n - i_read;
+        if (n == MAX)
+            hi = min_f(hi, e[n - 1].end);
+    }
+};
+
+// marching_steps.h:202-220: NS monotone sample positions (all zero for an empty set)
+template <unsigned NS, unsigned MAX, class T>
+DGMR_HD void sample_positions_n(const SectionSet<MAX, T>& d, T* out)
+{
+    if (d.n == 0) {
+        for (unsigned i = 0; i < NS; ++i)
+            out[i] = T(0);
+        return;
+    }
+    out[0] = d.e[0].start;
+    unsigned cur = 0;
+    T prev = out[0];
+    for (unsigned i = 1; i < NS; ++i) {
+        const T v = min_f(d.e[cur].end, prev + d.e[cur].delta_t);
+        out[i] = v;
+        prev = v;
+        if (cur < d.n - 1 && v == d.e[cur].end)
+            ++cur;
+    }
+}
+
+
+} // namespace dgmr

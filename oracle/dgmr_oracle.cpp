@@ -17,6 +17,7 @@
 //                       blend at splat_forward.cu:362-384 (alpha = min(0.99, .)).
 // Built with -ffp-contract=off so float results match the device kernels.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -1263,71 +1264,145 @@ DEF_VM(float, f32)
 DEF_VM(double, f64)
 
 // ------------------------------------------------- known-answer test hooks
-// DensityArray<4 or 16, T>: apply `n_ops` puts (start,end,delta_t triples) and
-// report the final sections (capacity 16), size and end.
-#define DEF_DA(T, SUFFIX)                                                                                                               \
-    int orc_density_array_##SUFFIX(int capacity, T start, const T* ops, int n_ops, T* out_sections, T* out_end)                         \
-    {                                                                                                                                    \
-        if (capacity == 4) {                                                                                                             \
-            DensityArray<4, T> a(start);                                                                                                 \
-            for (int i = 0; i < n_ops; ++i)                                                                                              \
-                a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });                                                                   \
-            for (unsigned i = 0; i < a.size(); ++i) {                                                                                    \
-                out_sections[3 * i] = a[i].start;                                                                                        \
-                out_sections[3 * i + 1] = a[i].end;                                                                                      \
-                out_sections[3 * i + 2] = a[i].delta_t;                                                                                  \
-            }                                                                                                                            \
-            *out_end = a.end();                                                                                                          \
-            return int(a.size());                                                                                                        \
-        }                                                                                                                                \
-        if (capacity == 16) {                                                                                                            \
-            DensityArray<16, T> a(start);                                                                                                \
-            for (int i = 0; i < n_ops; ++i)                                                                                              \
-                a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });                                                                   \
-            for (unsigned i = 0; i < a.size(); ++i) {                                                                                    \
-                out_sections[3 * i] = a[i].start;                                                                                        \
-                out_sections[3 * i + 1] = a[i].end;                                                                                      \
-                out_sections[3 * i + 2] = a[i].delta_t;                                                                                  \
-            }                                                                                                                            \
-            *out_end = a.end();                                                                                                          \
-            return int(a.size());                                                                                                        \
-        }                                                                                                                                \
-        return -1;                                                                                                                       \
-    }                                                                                                                                    \
-    void orc_density_combine_##SUFFIX(const T* a, const T* b, T* out9)                                                                   \
-    {                                                                                                                                    \
-        Section<T> p[3];                                                                                                                 \
-        DensityArray<4, T>::combine({ a[0], a[1], a[2] }, { b[0], b[1], b[2] }, p);                                                      \
-        for (int i = 0; i < 3; ++i) {                                                                                                    \
-            out9[3 * i] = p[i].start;                                                                                                    \
-            out9[3 * i + 1] = p[i].end;                                                                                                  \
-            out9[3 * i + 2] = p[i].delta_t;                                                                                              \
-        }                                                                                                                                \
-    }                                                                                                                                    \
-    /* sample<n_samples> over a DensityArray<cap> built from the puts */                                                                 \
-    void orc_density_sample_##SUFFIX(int capacity, T start, const T* ops, int n_ops, int n_samples, T* out)                             \
-    {                                                                                                                                    \
-        if (capacity == 4) {                                                                                                             \
-            DensityArray<4, T> a(start);                                                                                                 \
-            for (int i = 0; i < n_ops; ++i)                                                                                              \
-                a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });                                                                   \
-            if (n_samples == 16)                                                                                                         \
-                sample<16>(a, out);                                                                                                      \
-            else if (n_samples == 128)                                                                                                   \
-                sample<128>(a, out);                                                                                                     \
-        } else {                                                                                                                         \
-            DensityArray<16, T> a(start);                                                                                                \
-            for (int i = 0; i < n_ops; ++i)                                                                                              \
-                a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });                                                                   \
-            if (n_samples == 16)                                                                                                         \
-                sample<16>(a, out);                                                                                                      \
-            else if (n_samples == 128)                                                                                                   \
-                sample<128>(a, out);                                                                                                     \
-        }                                                                                                                                \
-    }
+} // extern "C"
 
-DEF_DA(float, f32)
-DEF_DA(double, f64)
+namespace {
+template <unsigned CAP, class T>
+int da_puts(T start, const T* ops, int n_ops, T* out_sections, T* out_end)
+{
+    DensityArray<CAP, T> a(start);
+    for (int i = 0; i < n_ops; ++i)
+        a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });
+    for (unsigned i = 0; i < a.size(); ++i) {
+        out_sections[3 * i] = a[i].start;
+        out_sections[3 * i + 1] = a[i].end;
+        out_sections[3 * i + 2] = a[i].delta_t;
+    }
+    *out_end = a.end();
+    return int(a.size());
+}
+
+template <class T>
+int da_dispatch(int cap, T start, const T* ops, int n_ops, T* out, T* end)
+{
+    switch (cap) {
+    case 4:
+        return da_puts<4, T>(start, ops, n_ops, out, end);
+    case 8:
+        return da_puts<8, T>(start, ops, n_ops, out, end);
+    case 16:
+        return da_puts<16, T>(start, ops, n_ops, out, end);
+    }
+    return -1;
+}
+
+template <unsigned CAP, class T>
+void da_sample(T start, const T* ops, int n_ops, int n_samples, T* out)
+{
+    DensityArray<CAP, T> a(start);
+    for (int i = 0; i < n_ops; ++i)
+        a.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });
+    if (n_samples == 16)
+        sample<16>(a, out);
+    else if (n_samples == 128)
+        sample<128>(a, out);
+}
+
+// unittests/marching_steps.cpp:939-1002: std::srand(0), iters x puts random
+// puts into a DensityArray<8>, validity after every put and the stored delta_t
+// at `probes` random points against the true minimum.  Returns #failures.
+template <class T>
+int da_randomised(int iters, int puts, int probes)
+{
+    std::srand(0);
+    const auto r = []() { return T(std::rand()) / T(RAND_MAX); };
+    int failures = 0;
+    for (int i = 0; i < iters; ++i) {
+        const T smallest = r();
+        DensityArray<8, T> arr(smallest);
+        std::vector<Section<T>> entries;
+        for (int j = 0; j < puts; ++j) {
+            const T start = r() * 10.0f;
+            const T end = start + r();
+            entries.push_back({ start, end, r() });
+            arr.put(entries.back());
+            if (arr.size()) {
+                failures += !(arr[0].start >= smallest);
+                failures += !(arr[0].start < arr[0].end);
+            }
+            for (unsigned k = 1; k < arr.size(); ++k) {
+                failures += !(arr[k - 1].start != arr[k].start || arr[k - 1].end != arr[k].end || arr[k - 1].delta_t != arr[k].delta_t);
+                failures += !(arr[k].start < arr[k].end);
+                failures += !(arr[k - 1].end <= arr[k].start);
+            }
+            if (arr.size() == 0)
+                continue;
+            for (int l = 0; l < probes; ++l) {
+                const T t = r() * (arr[arr.size() - 1].end - smallest - 0.00001f) + smallest;
+                T real = T(1) / T(0);
+                for (const auto& e : entries)
+                    if (e.start <= t && t < e.end)
+                        real = min_f(real, e.delta_t);
+                T comp = T(1) / T(0);
+                for (unsigned k = 0; k < arr.size(); ++k)
+                    if (arr[k].start <= t && t < arr[k].end) {
+                        comp = arr[k].delta_t;
+                        break;
+                    }
+                failures += !(real == comp);
+            }
+        }
+    }
+    return failures;
+}
+} // namespace
+
+extern "C" {
+
+int orc_density_array_f32(int capacity, float start, const float* ops, int n_ops, float* out_sections, float* out_end)
+{
+    return da_dispatch<float>(capacity, start, ops, n_ops, out_sections, out_end);
+}
+int orc_density_array_f64(int capacity, double start, const double* ops, int n_ops, double* out_sections, double* out_end)
+{
+    return da_dispatch<double>(capacity, start, ops, n_ops, out_sections, out_end);
+}
+void orc_density_combine_f32(const float* a, const float* b, float* out9)
+{
+    Section<float> p[3];
+    DensityArray<4, float>::combine({ a[0], a[1], a[2] }, { b[0], b[1], b[2] }, p);
+    for (int i = 0; i < 3; ++i) {
+        out9[3 * i] = p[i].start;
+        out9[3 * i + 1] = p[i].end;
+        out9[3 * i + 2] = p[i].delta_t;
+    }
+}
+void orc_density_combine_f64(const double* a, const double* b, double* out9)
+{
+    Section<double> p[3];
+    DensityArray<4, double>::combine({ a[0], a[1], a[2] }, { b[0], b[1], b[2] }, p);
+    for (int i = 0; i < 3; ++i) {
+        out9[3 * i] = p[i].start;
+        out9[3 * i + 1] = p[i].end;
+        out9[3 * i + 2] = p[i].delta_t;
+    }
+}
+void orc_density_sample_f32(int capacity, float start, const float* ops, int n_ops, int n_samples, float* out)
+{
+    if (capacity == 4)
+        da_sample<4, float>(start, ops, n_ops, n_samples, out);
+    else
+        da_sample<16, float>(start, ops, n_ops, n_samples, out);
+}
+void orc_density_sample_f64(int capacity, double start, const double* ops, int n_ops, int n_samples, double* out)
+{
+    if (capacity == 4)
+        da_sample<4, double>(start, ops, n_ops, n_samples, out);
+    else
+        da_sample<16, double>(start, ops, n_ops, n_samples, out);
+}
+int orc_density_randomised_f32(int iters, int puts, int probes) { return da_randomised<float>(iters, puts, probes); }
+int orc_density_randomised_f64(int iters, int puts, int probes) { return da_randomised<double>(iters, puts, probes); }
 
 // elementary functions, for error-bound tests against libm
 void orc_fmath_f32(int which, const float* x, float* y, int n)

@@ -81,6 +81,10 @@ def _declare(L):
         f = getattr(L, f"orc_density_sample_{sfx}")
         f.restype = None
         f.argtypes = [C.c_int, C.c_float if sfx == "f32" else C.c_double, fp, C.c_int, C.c_int, fp]
+    for sfx in ("f32", "f64"):
+        f = getattr(L, f"orc_density_randomised_{sfx}")
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_int]
     L.orc_set_const_samples.restype = None
     L.orc_set_const_samples.argtypes = [C.c_int, _f64p]
     L.orc_fmath_f32.restype = None
@@ -267,3 +271,9 @@ def set_const_samples(sections) -> None:
     if arr.size == 0:
         arr = np.zeros(3)
     lib().orc_set_const_samples(len(sections), arr)
+
+
+def density_randomised(iters=1000, puts=100, probes=50, dtype=np.float32) -> int:
+    """The reference's srand(0) randomised DensityArray test; returns #failed checks."""
+    sfx = "f32" if dtype == np.float32 else "f64"
+    return int(getattr(lib(), f"orc_density_randomised_{sfx}")(iters, puts, probes))

@@ -1,0 +1,202 @@
+// TEST INFRASTRUCTURE: exposes the product's host/device headers
+// (differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_sections.h and
+// dgmr_volume_fit.h) through a C ABI so the reference's known-answer tests
+// can run them on the CPU, the way the reference's own unit tests run its
+// __host__ __device__ math on the host.
+#include <cstdlib>
+#include <vector>
+
+#include "../../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_sections.h"
+#include "../../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_volume_fit.h"
+
+namespace {
+
+template <unsigned CAP, class T>
+int run_puts(T start, const T* ops, int n_ops, T* out_sections, T* out_end)
+{
+    dgmr::SectionSet<CAP, T> s;
+    s.reset(start);
+    for (int i = 0; i < n_ops; ++i)
+        s.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });
+    for (unsigned i = 0; i < s.n; ++i) {
+        out_sections[3 * i] = s.e[i].start;
+        out_sections[3 * i + 1] = s.e[i].end;
+        out_sections[3 * i + 2] = s.e[i].delta_t;
+    }
+    *out_end = s.hi;
+    return int(s.n);
+}
+
+template <class T>
+int puts_dispatch(int cap, T start, const T* ops, int n_ops, T* out, T* end)
+{
+    switch (cap) {
+    case 4:
+        return run_puts<4, T>(start, ops, n_ops, out, end);
+    case 8:
+        return run_puts<8, T>(start, ops, n_ops, out, end);
+    case 16:
+        return run_puts<16, T>(start, ops, n_ops, out, end);
+    }
+    return -1;
+}
+
+template <unsigned CAP, class T>
+void run_sample(T start, const T* ops, int n_ops, T* out)
+{
+    dgmr::SectionSet<CAP, T> s;
+    s.reset(start);
+    for (int i = 0; i < n_ops; ++i)
+        s.put({ ops[3 * i], ops[3 * i + 1], ops[3 * i + 2] });
+    dgmr::sample_positions_n<16>(s, out);
+}
+
+// unittests/marching_steps.cpp:939-1002 on a SectionSet<8, T>: std::srand(0),
+// 1000 x 100 random puts, validity after each put and the stored delta_t at 50
+// random points against the true minimum.  Returns the number of failed checks.
+template <class T>
+int randomised(int iters, int puts, int probes)
+{
+    std::srand(0);
+    const auto r = []() { return T(std::rand()) / T(RAND_MAX); };
+    int failures = 0;
+    for (int i = 0; i < iters; ++i) {
+        const T smallest = r();
+        dgmr::SectionSet<8, T> arr;
+        arr.reset(smallest);
+        std::vector<dgmr::Section<T>> entries;
+        for (int j = 0; j < puts; ++j) {
+            const T start = r() * 10.0f;
+            const T end = start + r();
+            entries.push_back({ start, end, r() });
+            arr.put(entries.back());
+            if (arr.n) {
+                failures += !(arr.e[0].start >= smallest);
+                failures += !(arr.e[0].start < arr.e[0].end);
+            }
+            for (unsigned k = 1; k < arr.n; ++k) {
+                const auto& a = arr.e[k - 1];
+                const auto& b = arr.e[k];
+                failures += !(a.start != b.start || a.end != b.end || a.delta_t != b.delta_t);
+                failures += !(b.start < b.end);
+                failures += !(a.end <= b.start);
+            }
+            if (arr.n == 0)
+                continue;
+            for (int l = 0; l < probes; ++l) {
+                const T t = r() * (arr.e[arr.n - 1].end - smallest - 0.00001f) + smallest;
+                T real = T(1) / T(0);
+                for (const auto& e : entries)
+                    if (e.start <= t && t < e.end)
+                        real = dgmr_fm::min_f(real, e.delta_t);
+                T comp = T(1) / T(0);
+                for (unsigned k = 0; k < arr.n; ++k)
+                    if (arr.e[k].start <= t && t < arr.e[k].end) {
+                        comp = arr.e[k].delta_t;
+                        break;
+                    }
+                failures += !(real == comp);
+            }
+        }
+    }
+    return failures;
+}
+
+} // namespace
+
+extern "C" {
+
+int kat_density_array_f32(int cap, float start, const float* ops, int n_ops, float* out, float* end) { return puts_dispatch<float>(cap, start, ops, n_ops, out, end); }
+int kat_density_array_f64(int cap, double start, const double* ops, int n_ops, double* out, double* end) { return puts_dispatch<double>(cap, start, ops, n_ops, out, end); }
+
+void kat_density_combine_f32(const float* a, const float* b, float* out9)
+{
+    dgmr::Section<float> p[3];
+    dgmr::SectionSet<4, float>::combine({ a[0], a[1], a[2] }, { b[0], b[1], b[2] }, p);
+    for (int i = 0; i < 3; ++i) {
+        out9[3 * i] = p[i].start;
+        out9[3 * i + 1] = p[i].end;
+        out9[3 * i + 2] = p[i].delta_t;
+    }
+}
+void kat_density_combine_f64(const double* a, const double* b, double* out9)
+{
+    dgmr::Section<double> p[3];
+    dgmr::SectionSet<4, double>::combine({ a[0], a[1], a[2] }, { b[0], b[1], b[2] }, p);
+    for (int i = 0; i < 3; ++i) {
+        out9[3 * i] = p[i].start;
+        out9[3 * i + 1] = p[i].end;
+        out9[3 * i + 2] = p[i].delta_t;
+    }
+}
+
+void kat_density_sample16_f32(float start, const float* ops, int n_ops, float* out) { run_sample<4, float>(start, ops, n_ops, out); }
+
+int kat_density_randomised_f32(int iters, int puts, int probes) { return randomised<float>(iters, puts, probes); }
+int kat_density_randomised_f64(int iters, int puts, int probes) { return randomised<double>(iters, puts, probes); }
+
+// FunctionGroup packed as d0[4] k0[4] t1[4] t2[4] k2[4] t_right (21 doubles)
+static dgmr::FunctionGroup<double> unpack(const double* p)
+{
+    dgmr::FunctionGroup<double> f;
+    for (int i = 0; i < 4; ++i) {
+        f.d0[i] = p[i];
+        f.k0[i] = p[4 + i];
+        f.t1[i] = p[8 + i];
+        f.t2[i] = p[12 + i];
+        f.k2[i] = p[16 + i];
+    }
+    f.t_right = p[20];
+    return f;
+}
+static void pack(const dgmr::FunctionGroup<double>& f, double* p)
+{
+    for (int i = 0; i < 4; ++i) {
+        p[i] = f.d0[i];
+        p[4 + i] = f.k0[i];
+        p[8 + i] = f.t1[i];
+        p[12 + i] = f.t2[i];
+        p[16 + i] = f.k2[i];
+    }
+    p[20] = f.t_right;
+}
+
+void kat_pl_sample(const double* packed, double t, double* out4)
+{
+    const auto f = unpack(packed);
+    for (int i = 0; i < 4; ++i)
+        out4[i] = f.sample(i, t);
+}
+int kat_pl_valid(const double* packed) { return unpack(packed).valid() ? 1 : 0; }
+void kat_pl_create(const double* mpl, const double* mt, const double* el, const double* er, double t_right, double* packed_out)
+{
+    pack(dgmr::create_approximation<double>(mpl, mt, el, er, t_right), packed_out);
+}
+void kat_pl_volume_integrate(const double* packed, int n, int steps, double* out3)
+{
+    std::vector<dgmr::FunctionGroup<double>> g;
+    for (int i = 0; i < n; ++i)
+        g.push_back(unpack(packed + 21 * i));
+    dgmr::volume_integrate<double>(g.data(), unsigned(n), unsigned(steps), out3);
+}
+
+// RasterBinSizer<4>: adds (mass, centre, sd) triples; reports is_full after
+// every add, then finalises and reports is_full and begin/end of each bin.
+void kat_rbs4(float sigma, float transmission_threshold, const float* adds, int n, int* full_after_add, int* full_after_finalise, float* begin4,
+    float* end4)
+{
+    dgmr::RasterBinSizer<4> s;
+    s.init(sigma, transmission_threshold);
+    for (int i = 0; i < n; ++i) {
+        s.add_gaussian(adds[3 * i], adds[3 * i + 1], adds[3 * i + 2]);
+        full_after_add[i] = s.is_full() ? 1 : 0;
+    }
+    s.finalise();
+    *full_after_finalise = s.is_full() ? 1 : 0;
+    for (unsigned i = 0; i < 4; ++i) {
+        begin4[i] = s.begin_of(i);
+        end4[i] = s.end_of(i);
+    }
+}
+
+} // extern "C"

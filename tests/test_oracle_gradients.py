@@ -1,0 +1,73 @@
+"""Finite-difference checks of the oracle's adjoints (float64, CPU).
+
+The reference checks every adjoint of its device math by central differences
+(unittests/grad_math.cu, unittests/grad_inria_splatter_render.cu); here the
+whole pipelines are checked the same way: a random upstream image gradient G,
+loss = sum(render * G), 25 random parameters per input tensor, eps 1e-6.
+The volume marcher runs with fixed sample sections (the reference's
+DGMR_TORCH_GRAD_CHECK_CONST_SAMPLES mode), because adaptive sampling makes the
+forward piecewise constant in the sample positions.
+"""
+import numpy as np
+import pytest
+
+from differentiable_gaussian_mixture_renderer_b200 import scene as S
+from oracle import oracle as O
+
+TOL = 1e-3
+
+
+def as_f64(sc):
+    for k in ("centroids", "sh", "weights", "scales", "rotations"):
+        setattr(sc, k, getattr(sc, k).astype(np.float64))
+    return sc
+
+
+def fd_check(sc, grads, loss, rng, per_tensor=25, eps=1e-6):
+    bad = []
+    for name in ("centroids", "scales", "rotations", "weights", "sh"):
+        flat = getattr(sc, name).reshape(-1)
+        ga = grads[name].reshape(-1)
+        for i in rng.choice(flat.size, size=min(per_tensor, flat.size), replace=False):
+            o = flat[i]
+            flat[i] = o + eps
+            lp = loss()
+            flat[i] = o - eps
+            lm = loss()
+            flat[i] = o
+            fd = (lp - lm) / (2 * eps)
+            err = abs(fd - ga[i]) / max(1e-4, abs(fd), abs(ga[i]))
+            if err > TOL:
+                bad.append((name, int(i), fd, float(ga[i]), err))
+    return bad
+
+
+def test_splat_backward_matches_finite_differences():
+    sc = as_f64(S.make_scene(60, seed=3, sh_degree=3, scale_range=(0.05, 0.3)))
+    cam = S.make_camera(48, 40, eye=(0.3, -0.2, -3.0), dtype=np.float64)
+    rng = np.random.default_rng(2)
+    G = rng.normal(size=(3, 40, 48))
+    bg = np.array([0.1, 0.2, 0.3])
+    _, g = O.splat_render_f64(sc, cam, grad_fb=G, bg=bg)
+    loss = lambda: float((O.splat_render_f64(sc, cam, bg=bg) * G).sum())
+    bad = fd_check(sc, g, loss, rng)
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("seed", [5, 9])
+def test_vol_marcher_backward_matches_finite_differences(seed):
+    sc = as_f64(S.make_scene(40, seed=seed, sh_degree=2, scale_range=(0.05, 0.25), extent=0.6))
+    cam = S.make_camera(24, 20, eye=(0.2, -0.1, -3.0), dtype=np.float64)
+    O.set_const_samples([(2.0, 3.0, 1.0 / 31), (3.0, 4.0, 1.0 / 31)])
+    try:
+        rng = np.random.default_rng(seed)
+        G = rng.normal(size=(3, 20, 24))
+        bg = np.array([0.1, 0.2, 0.3])
+        c = O.vm_forward(sc, cam, bg=bg, dtype=np.float64)
+        assert c["remaining_transparency"].min() < 0.9  # the scene does occlude
+        g = O.vm_backward(sc, cam, c, G, bg=bg, dtype=np.float64)
+        loss = lambda: float((O.vm_forward(sc, cam, bg=bg, dtype=np.float64)["fb"] * G).sum())
+        bad = fd_check(sc, g, loss, rng)
+        assert not bad, bad
+    finally:
+        O.set_const_samples([])
