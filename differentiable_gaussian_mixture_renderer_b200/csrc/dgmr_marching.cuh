@@ -50,6 +50,50 @@ __device__ __forceinline__ bool gaussian_on_ray(const Gauss1d<T>& g, T mass, T* 
     return true;
 }
 
+// Range of bins a 1-D Gaussian can put mass into.  cdf_inv_SD computes
+// z = ((x - c) inv_sd) / sqrt(2) and 0.5 (1 + erf(z)); for float, erf_f is
+// exactly -1 / +1 once |z| >= 3.92, so a bin whose two borders both lie at
+// z <= -3.92 (or both at z >= 3.92) has a CDF difference of exactly zero and is
+// skipped by the mass test anyway.  For double the cut is |z| >= 5, where the
+// tail mass (< 1e-12) times the largest accepted mass on the ray (1000) stays
+// far below the 1e-5 per-bin threshold.  The borders are non-decreasing, so
+// both ends are found by binary search; the loops below then visit exactly
+// the bins that could pass the test, in the same order, with the same values.
+template <class T>
+__device__ __forceinline__ T tail_z();
+template <>
+__device__ __forceinline__ float tail_z<float>() { return 3.92f; }
+template <>
+__device__ __forceinline__ double tail_z<double>() { return 5.0; }
+
+template <class T>
+__device__ __forceinline__ T border_z(T x, T c, T inv_sd) { return ((x - c) * inv_sd) * T(0.70710678118654752440); }
+
+// first index i in [0, n) with z(borders[i]) > lim (strict) or >= lim, else n
+template <class T, bool STRICT>
+__device__ __forceinline__ int first_border(const T* borders, int n, T c, T inv_sd, T lim)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const T z = border_z(borders[mid], c, inv_sd);
+        if (STRICT ? (z > lim) : (z >= lim))
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
+}
+
+template <class T>
+__device__ __forceinline__ void live_bins(const T* borders, T c, T inv_sd, int* k_first, int* k_last)
+{
+    const int i0 = first_border<T, true>(borders, int(kSmallSteps), c, inv_sd, -tail_z<T>());
+    const int j1 = first_border<T, false>(borders, int(kSmallSteps), c, inv_sd, tail_z<T>());
+    *k_first = i0 > 0 ? i0 - 1 : 0;
+    *k_last = j1 - 1 < int(kBins) - 1 ? j1 - 1 : int(kBins) - 1;
+}
+
 // math.h:430-468
 template <class T>
 __device__ __forceinline__ void sample_gaussian(const Gauss1d<T>& g, T mass, V3<T> rgb, const T* borders, Bin<T>* bins)
@@ -62,8 +106,10 @@ __device__ __forceinline__ void sample_gaussian(const Gauss1d<T>& g, T mass, V3<
     const T mib = mor * (cdf_inv_SD(centre, inv_sd, borders[kBins]) - cdf_inv_SD(centre, inv_sd, borders[0]));
     if (mib < T(0.0001f))
         return;
-    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[0]);
-    for (unsigned k = 0; k < kBins; ++k) {
+    int k0, k1;
+    live_bins(borders, centre, inv_sd, &k0, &k1);
+    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[k0]);
+    for (int k = k0; k <= k1; ++k) {
         const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
         const T m = max_f(T(0), (cdf_end - cdf_start) * mor);
         cdf_start = cdf_end;
@@ -139,8 +185,10 @@ __device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V
         return;
     T g_centre = 0, g_inv_sd = 0, g_mor = 0;
     V3<T> grgb = { 0, 0, 0 };
-    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[0]);
-    for (unsigned k = 0; k < kBins; ++k) {
+    int k0, k1;
+    live_bins(borders, centre, inv_sd, &k0, &k1);
+    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[k0]);
+    for (int k = k0; k <= k1; ++k) {
         const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
         const T delta = cdf_end - cdf_start;
         const T m = max_f(T(0), delta * mor);
