@@ -208,14 +208,22 @@ struct VmMarch {
     ConstSamplesT<T> cs;
 };
 
+// A march block covers kMarchRows pixel rows of one 16x16 tile (kMarchParts
+// blocks per tile).  Small blocks let the blocks of a heavy tile spread over
+// several SMs and retire independently; every block reads the tile's whole
+// Gaussian list in batches of kMarchThreads.
+constexpr unsigned kMarchThreads = 64;
+constexpr unsigned kMarchRows = kMarchThreads / kTile;
+constexpr unsigned kMarchParts = kTile / kMarchRows;
+
 template <class T>
 struct MarchShared {
-    uint32_t id[256];
-    T mu[3][256];
-    T Q[6][256];
-    T mass[256];
-    T rgb[3][256];
-    T depth[256];
+    uint32_t id[kMarchThreads];
+    T mu[3][kMarchThreads];
+    T Q[6][kMarchThreads];
+    T mass[kMarchThreads];
+    T rgb[3][kMarchThreads];
+    T depth[kMarchThreads];
 };
 
 template <class T>
@@ -256,14 +264,14 @@ __device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec
         return;
     }
     bool done1 = done;
-    for (int32_t base = b; base < e; base += 256) {
-        if (__syncthreads_count(done1) == 256)
+    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
+        if (__syncthreads_count(done1) == int(kMarchThreads))
             break;
         load_batch(sh, a, base + int32_t(threadIdx.x), e);
         __syncthreads();
         if (done1)
             continue;
-        const int n = min(256, e - base);
+        const int n = min(int(kMarchThreads), e - base);
         for (int j = 0; j < n; ++j) {
             const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
             const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
@@ -292,14 +300,14 @@ template <class T>
 __device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done, V3<T> o,
     V3<T> d)
 {
-    for (int32_t base = b; base < e; base += 256) {
-        if (__syncthreads_count(done) == 256)
+    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
+        if (__syncthreads_count(done) == int(kMarchThreads))
             break;
         load_batch(sh, a, base + int32_t(threadIdx.x), e);
         __syncthreads();
         if (done)
             continue;
-        const int n = min(256, e - base);
+        const int n = min(int(kMarchThreads), e - base);
         for (int j = 0; j < n; ++j) {
             const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
             const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
@@ -309,12 +317,12 @@ __device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchS
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_vm_march(VmMarch<T> a, CameraT<T> cam)
+__global__ void __launch_bounds__(kMarchThreads) k_vm_march(VmMarch<T> a, CameraT<T> cam)
 {
     __shared__ MarchShared<T> sh;
-    const unsigned tile = blockIdx.x;
+    const unsigned tile = blockIdx.x / kMarchParts, part = blockIdx.x % kMarchParts;
     const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + part * kMarchRows + (threadIdx.x >> 4);
     const bool inside = px < cam.W && py < cam.H;
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(256) k_vm_march(VmMarch<T> a, CameraT<T> cam)
     T borders[kSmallSteps];
     Bin<T> bins[kBins];
     for (unsigned step = 0;; ++step) {
-        if (__syncthreads_count(done) == 256)
+        if (__syncthreads_count(done) == int(kMarchThreads))
             break;
         if (step >= kMaxLargeSteps) {
             if (!done)
@@ -369,12 +377,12 @@ __device__ __forceinline__ T warp_sum_t(T v)
 // the reference are replaced by a warp-level shuffle sum and one atomic per
 // value per warp.
 template <class T>
-__global__ void __launch_bounds__(256) k_vm_march_bwd(VmMarch<T> a, CameraT<T> cam)
+__global__ void __launch_bounds__(kMarchThreads) k_vm_march_bwd(VmMarch<T> a, CameraT<T> cam)
 {
     __shared__ MarchShared<T> sh;
-    const unsigned tile = blockIdx.x;
+    const unsigned tile = blockIdx.x / kMarchParts, part = blockIdx.x % kMarchParts;
     const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + part * kMarchRows + (threadIdx.x >> 4);
     const bool inside = px < cam.W && py < cam.H;
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
@@ -399,7 +407,7 @@ __global__ void __launch_bounds__(256) k_vm_march_bwd(VmMarch<T> a, CameraT<T> c
     Bin<T> bins[kBins];
     Bin<T> gbins[kBins];
     for (unsigned step = 0;; ++step) {
-        if (__syncthreads_count(done) == 256)
+        if (__syncthreads_count(done) == int(kMarchThreads))
             break;
         if (step >= kMaxLargeSteps) {
             if (!done)
@@ -415,12 +423,12 @@ __global__ void __launch_bounds__(256) k_vm_march_bwd(VmMarch<T> a, CameraT<T> c
         if (!done)
             grad_integrate_bins(colour, tr, final_T, bins, gc, gt, gbins);
         // pass 3: adjoint of the bin masses, per Gaussian
-        for (int32_t base = b; base < e; base += 256) {
-            if (__syncthreads_count(done) == 256)
+        for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
+            if (__syncthreads_count(done) == int(kMarchThreads))
                 break;
             load_batch(sh, a, base + int32_t(threadIdx.x), e);
             __syncthreads();
-            const int n = min(256, e - base);
+            const int n = min(int(kMarchThreads), e - base);
             for (int j = 0; j < n; ++j) {
                 T v[10];
                 V3<T> gmu = { T(0), T(0), T(0) };
@@ -636,7 +644,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.remaining_T = static_cast<T*>(c->remaining_transparency);
     a.stats = st_dev;
     a.cs = const_samples<T>();
-    k_vm_march<T><<<cam.gx * cam.gy, 256, 0, s>>>(a, cam);
+    k_vm_march<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
     note_launch();
     return launch_status();
 }
@@ -670,7 +678,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     a.g_centroids = static_cast<T*>(g_centroids);
     a.stats = st_dev;
     a.cs = const_samples<T>();
-    k_vm_march_bwd<T><<<cam.gx * cam.gy, 256, 0, s>>>(a, cam);
+    k_vm_march_bwd<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
     VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
         c->tiles_touched, L.acc, static_cast<T*>(g_sh), static_cast<T*>(g_weights), static_cast<T*>(g_centroids), static_cast<T*>(g_scales),
