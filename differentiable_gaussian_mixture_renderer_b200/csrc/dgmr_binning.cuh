@@ -2,7 +2,7 @@
 //
 // The reference emits one 64-bit key (tile << 32 | float bits of depth) per
 // (tile, Gaussian) pair and radix-sorts all pairs over 32 + msb(tiles) bits
-// (splat_forward.cu:222-274).  The sorted order it produces is the order of
+// (splat_forward.cu:159-211).  The sorted order it produces is the order of
 // (tile, depth bits, Gaussian index).  Here the same order is reached with
 // far less traffic: the N Gaussians are stably sorted once by their 32-bit
 // depth bits (N << pairs), pairs are emitted in that depth order, and a
@@ -204,7 +204,7 @@ static __global__ void __launch_bounds__(256) k_emit_pairs(const uint32_t* __res
     }
 }
 
-// splat_forward.cu:281-302 on the tile-sorted list (ranges zeroed beforehand)
+// splat_forward.cu:218-239 on the tile-sorted list (ranges zeroed beforehand)
 static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, const uint32_t* __restrict__ n_dev, int32_t* __restrict__ ranges, uint32_t n_tiles,
     uint32_t* __restrict__ stats)
 {

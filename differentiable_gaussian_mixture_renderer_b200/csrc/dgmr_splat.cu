@@ -1,4 +1,4 @@
-// Tile-based EWA splat renderer: forward (src/dgmr/splat_forward.cu:93-401)
+// Tile-based EWA splat renderer: forward (src/dgmr/splat_forward.cu:30-338)
 // and a reverse-order backward (no reference kernel), behind the C ABI of
 // include/dgmr_b200.h.
 #include <cstdint>
@@ -86,7 +86,7 @@ struct SplatPre {
     float4* blend_rec;
 };
 
-// splat_forward.cu:137-180
+// splat_forward.cu:70-118
 __global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<float> cam)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<fl
     p.blend_rec[2 * i + 1] = make_float4(2.f * con.v[1], g.weight, q_cut, 0.f);
 }
 
-// d'Qd of one (pixel, splat) pair (splat_forward.cu:365), evaluated as
+// d'Qd of one (pixel, splat) pair (splat_forward.cu:302), evaluated as
 // dx * (a dx + 2b dy) + (c dy) dy with two fused multiply-adds; r0 = (x, y, a, c), b2 = 2b
 __device__ __forceinline__ float splat_q(float4 r0, float b2, float px, float py, float* dx_o, float* dy_o)
 {
@@ -169,7 +169,7 @@ __device__ __forceinline__ float splat_gauss(float4 co, float2 xy, float px, flo
 }
 
 // Per-pixel blend step shared by both pixels a thread owns
-// (splat_forward.cu:365-384).
+// (splat_forward.cu:299-321).
 struct PixelState {
     float T, c0, c1, c2;
     int32_t last;
@@ -554,7 +554,7 @@ SplatPre make_pre(const dgmr_scene* scene, const SplatLayout& L)
         L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm, L.blend_rec };
 }
 
-// per-Gaussian preprocess and the inclusive scan (splat_forward.cu:133-202)
+// per-Gaussian preprocess and the inclusive scan (splat_forward.cu:70-139)
 void launch_preprocess(const dgmr_scene* scene, const CameraT<float>& cam, const SplatLayout& L, uint32_t* st_dev, cudaStream_t s)
 {
     const uint32_t N = uint32_t(scene->n_gaussians);

@@ -93,8 +93,8 @@ dgmr_status dgmr_splat_forward(const dgmr_scene* scene, const dgmr_camera* camer
 
 /* The same forward in two halves, for callers that size the pair workspace
  * from the frame itself (the reference reads the pair count back with .item(),
- * splat_forward.cu:204): preprocess (splat_forward.cu:133-202) leaves the pair
- * count in stats->n_pairs and in point_offsets[N-1]; render (:208-398) does
+ * splat_forward.cu:141): preprocess (splat_forward.cu:70-139) leaves the pair
+ * count in stats->n_pairs and in point_offsets[N-1]; render (:145-335) does
  * the binning and the blend. */
 dgmr_status dgmr_splat_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, void* frame_workspace, size_t frame_workspace_bytes,
     dgmr_frame_stats* stats, dgmr_stream stream);
@@ -103,7 +103,7 @@ dgmr_status dgmr_splat_render(const dgmr_scene* scene, const dgmr_camera* camera
 
 /* Views into the workspaces after a forward (device pointers): the
  * per-Gaussian cache and the binning result, in the reference's layouts
- * (splat_forward.cu:108-127, :210-214, :277). */
+ * (splat_forward.cu:96-107, :159-191, :218-239). */
 typedef struct dgmr_splat_views {
     int32_t* rects; /* [N,2] */
     float* rgb; /* [N,3] */
@@ -125,7 +125,7 @@ dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32
 
 /* Re-runs only the blend stage of the last forward made in these workspaces
  * (same camera, Gaussian count and capacity), e.g. to time the blend kernel
- * by itself.  Splits splat_forward.cu:305-398 out of the frame. */
+ * by itself.  Splits splat_forward.cu:242-335 out of the frame. */
 dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, float* framebuffer, void* frame_workspace, size_t frame_workspace_bytes,
     void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
 

@@ -5,16 +5,16 @@
 // The product never links or calls this library.
 //
 // Restates, on the CPU and in plain loops:
-//   splat forward       src/dgmr/splat_forward.cu:93-401 (preprocess :137-180,
-//                       scan :187-202, duplicateWithKeys :222-254, stable radix
-//                       sort over bits [0, 32+msb) :256-274, identifyTileRanges
-//                       :281-302, blend :312-397)
+//   splat forward       src/dgmr/splat_forward.cu:30-338 (preprocess :70-118,
+//                       scan :120-143, duplicateWithKeys :145-191, stable radix
+//                       sort over bits [0, 32+msb) :193-211, identifyTileRanges
+//                       :213-240, blend :242-335)
 //   vol_marcher forward src/dgmr/vol_marcher_forward.cu:42-503
 //   vol_marcher backward src/dgmr/vol_marcher_backward.cu:53-386
 //   splat backward      no reference kernel; assembled from the projection
 //                       adjoint grad/math.h:333-527, the SH adjoint
 //                       grad/math.h:203-282 and a reverse-order adjoint of the
-//                       blend at splat_forward.cu:362-384 (alpha = min(0.99, .)).
+//                       blend at splat_forward.cu:299-321 (alpha = min(0.99, .)).
 // Built with -ffp-contract=off so float results match the device kernels.
 #include <algorithm>
 #include <cstdlib>
@@ -202,7 +202,7 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
         for (int c = 0; c < 4; ++c)
             conic_opacity[4 * i + c] = T(0);
         const V3<T> mu = load3(s.centroids, size_t(i));
-        if (mat4_mul_point(s.view, mu).z < T(0.2)) // splat_forward.cu:149
+        if (mat4_mul_point(s.view, mu).z < T(0.2)) // splat_forward.cu:86
             continue;
         const T w = s.weights[i];
         const V3<T> sc = mul(load3(s.scales, size_t(i)), s.cov_scale_multiplier);
@@ -238,7 +238,7 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
     }
 }
 
-// alpha of one (pixel, splat) pair, splat_forward.cu:365-370.  The quadratic
+// alpha of one (pixel, splat) pair, splat_forward.cu:302-309.  The quadratic
 // form d'Qd is evaluated as dx * (a dx + 2b dy) + (c dy) dy with two fused
 // multiply-adds, in this order (the device blend uses the same sequence).
 template <class T>
