@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--gaussians", type=int, default=1_000_000)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--batch", type=int, default=8, help="requests per step")
@@ -62,9 +62,9 @@ def parse():
 
 
 def workload(args):
-    return {"workload": f"splat forward, {args.n} Gaussians (config-0 distribution), {args.width}x{args.height}, "
+    return {"workload": f"splat forward, {args.gaussians} Gaussians (config-0 distribution), {args.width}x{args.height}, "
                         f"random cameras r=2.5-4, {args.batch} requests/step",
-            "n_gaussians": args.n, "width": args.width, "height": args.height, "requests_per_step": args.batch,
+            "n_gaussians": args.gaussians, "width": args.width, "height": args.height, "requests_per_step": args.batch,
             "slots_in_flight": args.slots,
             "l2": "working set > 126 MB L2 (~9M pairs x 32 B of binning buffers per frame)"}
 
@@ -149,7 +149,7 @@ def profiled_traffic(name: str):
 def cpu_baseline(args, cams):
     from oracle import oracle as O
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
-    sc = S.make_scene(args.n, seed=0)
+    sc = S.make_scene(args.gaussians, seed=0)
     O.splat_forward(sc, cams[0], want_keys=False)  # warm
     t = time.perf_counter()
     frames = 0
@@ -169,7 +169,7 @@ def run_reference(args):
         return 0
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
     from oracle import oracle as O
-    sc = S.make_scene(args.n, seed=0)
+    sc = S.make_scene(args.gaussians, seed=0)
     cams = S.random_cameras(args.warmup + args.steps, args.width, args.height, seed=1)
     for cam in cams[:args.warmup]:
         O.splat_forward(sc, cam, want_keys=False)
@@ -200,6 +200,15 @@ def pct(xs, q):
     return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
 
 
+def replica_totals(ms_local: float, units_local: int, world: int, reduce_max, reduce_sum):
+    """Whole-job numbers of N independent replicas: the slowest rank's device
+    time and the units all ranks processed.  reduce_max / reduce_sum combine a
+    float over the ranks (identity for one rank)."""
+    ms = reduce_max(float(ms_local)) if world > 1 else float(ms_local)
+    units = reduce_sum(float(units_local)) if world > 1 else float(units_local)
+    return ms, units, units / (ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -223,15 +232,18 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def over_ranks(op):
+        def reduce(x: float) -> float:
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=op)
+            return float(t.item())
+        return reduce
+
+    max_over_ranks = over_ranks(dist.ReduceOp.MAX) if world > 1 else (lambda x: x)
+    sum_over_ranks = over_ranks(dist.ReduceOp.SUM) if world > 1 else (lambda x: x)
 
     lib = N.lib()
-    sc_np = S.make_scene(args.n, seed=0)
+    sc_np = S.make_scene(args.gaussians, seed=0)
     scene = GaussianScene.from_numpy(sc_np, dev)
     n_req = (args.warmup + args.steps) * args.batch
     cams = S.random_cameras(2 * n_req + args.plain + 4, args.width, args.height, seed=1 + 1000 * rank)
@@ -269,11 +281,9 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms_value, wall_value, lat_value, launches, rerenders = served_leg(cams[:n_req], to_host=False)
         ms_e2e, wall_e2e, lat_e2e, _, _ = served_leg(cams[n_req:2 * n_req], to_host=True)
-    ms_value = max_over_ranks(ms_value)
-    ms_e2e = max_over_ranks(ms_e2e)
-    renders = args.steps * args.batch * world
-    value = renders / (ms_value * 1e-3)
-    e2e_value = renders / (ms_e2e * 1e-3)
+    local_renders = args.steps * args.batch
+    ms_value, _, value = replica_totals(ms_value, local_renders, world, max_over_ranks, sum_over_ranks)
+    ms_e2e, _, e2e_value = replica_totals(ms_e2e, local_renders, world, max_over_ranks, sum_over_ranks)
 
     # ---------------------------------------------------------------- plain per-call leg
     plain_cams = cams[2 * n_req:2 * n_req + args.plain]
@@ -324,7 +334,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     achieved = blend_bytes / (blend_ms * 1e-3) / 1e9
     # the committed ncu capture is of this frame at the default workload only
-    default_workload = (args.n, args.width, args.height) == (1_000_000, 1920, 1080)
+    default_workload = (args.gaussians, args.width, args.height) == (1_000_000, 1920, 1080)
     traffic = profiled_traffic("splat_blend_1080p_1M.txt") if default_workload else None
 
     # ---------------------------------------------------------------- CPU baseline
