@@ -55,6 +55,19 @@ class SplatViews(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in _SPLAT_VIEW_FIELDS]
 
 
+BATCH_MAX_VIEWS, BATCH_MAX_SCENES = 64, 16
+
+
+class BatchView(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("reserved", C.c_int32), ("camera", Camera), ("framebuffer", C.c_void_p),
+                ("grad_framebuffer", C.c_void_p)]
+
+
+class SceneGrads(C.Structure):
+    _fields_ = [("sh", C.c_void_p), ("weights", C.c_void_p), ("centroids", C.c_void_p), ("scales", C.c_void_p),
+                ("rotations", C.c_void_p)]
+
+
 # every symbol include/dgmr_b200.h declares, with its ctypes signature
 _SIGNATURES = {
     "dgmr_splat_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
@@ -74,6 +87,15 @@ _SIGNATURES = {
     "dgmr_splat_backward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_size_t, C.c_int64, C.c_void_p]),
+    "dgmr_splat_batch_workspace_size": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
+                                                  C.c_int64, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "dgmr_splat_batch_preprocess": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
+                                              C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "dgmr_splat_batch_forward": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32, C.c_void_p,
+                                           C.c_size_t, C.c_void_p, C.c_size_t, C.c_int64, C.c_void_p, C.c_void_p]),
+    "dgmr_splat_batch_backward": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
+                                            C.POINTER(SceneGrads), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                            C.c_int64, C.c_void_p]),
     "dgmr_vm_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
     "dgmr_vm_forward_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p,
                                              C.c_size_t, C.c_void_p, C.c_void_p]),

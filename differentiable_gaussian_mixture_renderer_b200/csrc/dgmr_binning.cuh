@@ -125,6 +125,18 @@ static __global__ void k_gather_counts(const uint32_t* __restrict__ perm, const 
     }
 }
 
+// Tile grid of the frame a Gaussian slot belongs to: its size and the offset
+// of its first tile in the (possibly multi-frame) tile numbering.
+struct TileGrid {
+    unsigned gx, gy, off;
+};
+
+// One frame: every slot uses the same grid.
+struct SingleGrid {
+    unsigned gx, gy;
+    __device__ __forceinline__ TileGrid grid(uint32_t) const { return TileGrid { gx, gy, 0u }; }
+};
+
 // Pairs in depth order: for the j-th Gaussian by depth, one entry per tile
 // its rectangle touches, row-major (util.h:42-52 applied to the cached rect
 // and centroid).  The 32 Gaussians of a warp own one contiguous output range
@@ -132,10 +144,10 @@ static __global__ void k_gather_counts(const uint32_t* __restrict__ perm, const 
 // writes that range together: in each round lane l takes slot base + l and
 // finds its owner -- the first lane whose inclusive end exceeds the slot -- by
 // a five-step binary search over the lanes' ends, done with shuffles.
-template <class T>
+template <class T, class Grids>
 static __global__ void __launch_bounds__(256) k_emit_pairs(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ cnt_sorted,
-    const uint32_t* __restrict__ off_sorted, const int32_t* __restrict__ rects, const T* __restrict__ xy, uint32_t N, unsigned gx, unsigned gy, uint32_t cap,
-    uint32_t* __restrict__ pair_tile, uint32_t* __restrict__ pair_val, uint32_t* __restrict__ stats)
+    const uint32_t* __restrict__ off_sorted, const int32_t* __restrict__ rects, const T* __restrict__ xy, uint32_t N, uint32_t cap,
+    uint32_t* __restrict__ pair_tile, uint32_t* __restrict__ pair_val, uint32_t* __restrict__ stats, const __grid_constant__ Grids grids)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -143,13 +155,15 @@ static __global__ void __launch_bounds__(256) k_emit_pairs(const uint32_t* __res
         return;
     uint32_t c = 0, end = 0, g = 0;
     TileRect r = { 0, 0, 0, 0 };
+    TileGrid tg = { 0u, 0u, 0u };
     if (j < N) {
         c = cnt_sorted[j];
         end = off_sorted[j];
         if (c > 0) {
             g = perm[j];
             if (g < N) {
-                r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], gx, gy);
+                tg = grids.grid(g);
+                r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], tg.gx, tg.gy);
                 if ((r.x1 - r.x0) * (r.y1 - r.y0) != c) {
                     flag_bounds(stats, 0x22u);
                     r = { 0, 0, 0, 0 };
@@ -189,11 +203,14 @@ static __global__ void __launch_bounds__(256) k_emit_pairs(const uint32_t* __res
         const uint32_t s_x0 = __shfl_sync(0xffffffffu, r.x0, src);
         const uint32_t s_y0 = __shfl_sync(0xffffffffu, r.y0, src);
         const uint32_t s_w = __shfl_sync(0xffffffffu, rw, src);
+        const uint32_t s_gx = __shfl_sync(0xffffffffu, tg.gx, src);
+        const uint32_t s_n = __shfl_sync(0xffffffffu, tg.gx * tg.gy, src);
+        const uint32_t s_off = __shfl_sync(0xffffffffu, tg.off, src);
         if (pos < hi && pos < cap) {
             const uint32_t k = pos - s_start;
-            const uint32_t t = (s_w && k < s_c) ? (s_y0 + k / s_w) * gx + s_x0 + k % s_w : 0xffffffffu;
-            if (t < gx * gy) {
-                pair_tile[pos] = t;
+            const uint32_t t = (s_w && k < s_c) ? (s_y0 + k / s_w) * s_gx + s_x0 + k % s_w : 0xffffffffu;
+            if (t < s_n) {
+                pair_tile[pos] = s_off + t;
                 pair_val[pos] = s_g;
             } else {
                 pair_tile[pos] = 0;
@@ -264,11 +281,10 @@ static __global__ void __launch_bounds__(1024) k_tile_order(const int32_t* __res
 // emission, tile sort and ranges.  Returns the buffer index holding the
 // sorted (tile, Gaussian) pairs.  Requires b.perm = iota and b.depth_key
 // filled by the preprocess.
-template <class T>
-inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* tiles_touched, uint32_t* point_offsets, const int32_t* rects, const T* xy,
-    uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s, bool offsets_ready = false)
+template <class T, class Grids>
+inline int run_binning_grids(uint32_t N, uint32_t n_tiles, const Grids& grids, const uint32_t* tiles_touched, uint32_t* point_offsets, const int32_t* rects,
+    const T* xy, uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s, bool offsets_ready)
 {
-    const uint32_t n_tiles = gx * gy;
     cudaMemsetAsync(ranges, 0, size_t(n_tiles) * 2 * sizeof(int32_t), s);
     if (N == 0) {
         cudaMemsetAsync(b.n_sort, 0, sizeof(uint32_t), s);
@@ -288,7 +304,7 @@ inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* til
     k_gather_counts<<<blocks, 256, 0, s>>>(perm, tiles_touched, N, b.cnt_sorted, stats);
     note_launch();
     inclusive_scan_u32(b.cnt_sorted, b.off_sorted, N, b.scan_tmp, s);
-    k_emit_pairs<T><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, gx, gy, cap, b.pair_tile[0], b.pair_val[0], stats);
+    k_emit_pairs<T, Grids><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rects, xy, N, cap, b.pair_tile[0], b.pair_val[0], stats, grids);
     note_launch();
     const int bits = int(higher_msb(n_tiles));
     const int par = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort, 0, cap, bits, b.sort_tmp, n_sms, s, stats);
@@ -298,6 +314,13 @@ inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* til
         note_launch();
     }
     return par;
+}
+
+template <class T>
+inline int run_binning(uint32_t N, unsigned gx, unsigned gy, const uint32_t* tiles_touched, uint32_t* point_offsets, const int32_t* rects, const T* xy,
+    uint32_t cap, BinningBuffers& b, int32_t* ranges, uint32_t* stats, int n_sms, cudaStream_t s, bool offsets_ready = false)
+{
+    return run_binning_grids<T>(N, gx * gy, SingleGrid { gx, gy }, tiles_touched, point_offsets, rects, xy, cap, b, ranges, stats, n_sms, s, offsets_ready);
 }
 
 } // namespace dgmr

@@ -393,21 +393,29 @@ __device__ __forceinline__ V3<T> sh_to_colour(const T* sh, uint32_t i, int strid
 // reference's cat + slice) and returns d/ddirection.
 template <class T>
 __device__ __forceinline__ V3<T> grad_sh_to_colour(const T* sh, uint32_t i, int stride, int deg, V3<T> dir, V3<T> g_in, const uint8_t* mask, T pad,
-    T* g_sh_out)
+    T* g_sh_out, bool accumulate = false)
 {
     const V3<T> g = { mask[0] ? g_in.x : T(0), mask[1] ? g_in.y : T(0), mask[2] ? g_in.z : T(0) };
     const auto put = [&](int j, T basis) {
         if (j < stride) {
             T* p = g_sh_out + (size_t(i) * stride + j) * 3;
-            p[0] = g.x * basis;
-            p[1] = g.y * basis;
-            p[2] = g.z * basis;
+            if (accumulate) {
+                p[0] += g.x * basis;
+                p[1] += g.y * basis;
+                p[2] += g.z * basis;
+            } else {
+                p[0] = g.x * basis;
+                p[1] = g.y * basis;
+                p[2] = g.z * basis;
+            }
         }
     };
     const auto S = [&](int j) { return sh_load(sh, i, stride, j, pad); };
-    for (int j = 0; j < stride; ++j) {
-        T* p = g_sh_out + (size_t(i) * stride + j) * 3;
-        p[0] = p[1] = p[2] = T(0);
+    if (!accumulate) {
+        for (int j = 0; j < stride; ++j) {
+            T* p = g_sh_out + (size_t(i) * stride + j) * 3;
+            p[0] = p[1] = p[2] = T(0);
+        }
     }
     V3<T> dx = { 0, 0, 0 }, dy = { 0, 0, 0 }, dz = { 0, 0, 0 };
     const T x = dir.x, y = dir.y, z = dir.z;

@@ -36,12 +36,12 @@ struct SplatLayout {
     size_t pair_bytes; // pair workspace
 };
 
-inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void* base, void* pair_base)
+// N Gaussians (or view-Gaussians of a batch), n_tiles tiles and n_px pixels
+inline SplatLayout splat_layout_n(uint32_t N, uint32_t n_tiles, size_t n_px, uint32_t cap, void* base, void* pair_base)
 {
     SplatLayout L;
     Carver c;
     c.base = static_cast<char*>(base);
-    const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
     L.rects = c.take<int32_t>(size_t(N) * 2);
     L.rgb = c.take<float>(size_t(N) * 3);
     L.clamped = c.take<uint8_t>(size_t(N) * 3);
@@ -50,12 +50,12 @@ inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap
     L.conic_opacity = c.take<float>(size_t(N) * 4);
     L.tiles_touched = c.take<uint32_t>(N);
     L.point_offsets = c.take<uint32_t>(N);
-    L.ranges = c.take<int32_t>(size_t(gx) * gy * 2);
-    L.final_T = c.take<float>(size_t(W) * H);
-    L.n_contrib = c.take<int32_t>(size_t(W) * H);
+    L.ranges = c.take<int32_t>(size_t(n_tiles) * 2);
+    L.final_T = c.take<float>(n_px);
+    L.n_contrib = c.take<int32_t>(n_px);
     L.grad_acc = c.take<float>(size_t(N) * 9);
     L.blend_rec = c.take<float4>(size_t(N) * 2);
-    L.tile_order = c.take<uint32_t>(size_t(gx) * gy);
+    L.tile_order = c.take<uint32_t>(n_tiles);
     L.stats = c.take<uint32_t>(4);
     carve_binning_gaussians(c, L.bin, N);
     L.bytes = c.off;
@@ -64,6 +64,12 @@ inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap
     carve_binning_pairs(cp, L.bin, N, cap);
     L.pair_bytes = cp.off;
     return L;
+}
+
+inline SplatLayout splat_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void* base, void* pair_base)
+{
+    const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+    return splat_layout_n(N, gx * gy, size_t(W) * H, cap, base, pair_base);
 }
 
 struct SplatPre {
@@ -86,28 +92,26 @@ struct SplatPre {
     float4* blend_rec;
 };
 
-// splat_forward.cu:70-118
-__global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<float> cam)
+// splat_forward.cu:70-118 for Gaussian i of the scene, written to output
+// slot o (o = i for one frame; o = the view's offset + i in a batch)
+__device__ __forceinline__ void preprocess_one(const SplatPre& p, const CameraT<float>& cam, uint32_t i, uint32_t o)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.N)
-        return;
-    p.tiles_touched[i] = 0;
-    p.perm[i] = i;
-    p.depth_key[i] = 0;
-    p.rects[2 * i] = 0;
-    p.rects[2 * i + 1] = 0;
-    p.xy[2 * i] = 0.f;
-    p.xy[2 * i + 1] = 0.f;
-    p.depths[i] = 0.f;
+    p.tiles_touched[o] = 0;
+    p.perm[o] = o;
+    p.depth_key[o] = 0;
+    p.rects[2 * o] = 0;
+    p.rects[2 * o + 1] = 0;
+    p.xy[2 * o] = 0.f;
+    p.xy[2 * o + 1] = 0.f;
+    p.depths[o] = 0.f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        p.rgb[3 * i + c] = 0.f;
-        p.clamped[3 * i + c] = 0;
+        p.rgb[3 * o + c] = 0.f;
+        p.clamped[3 * o + c] = 0;
     }
-    reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    p.blend_rec[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    p.blend_rec[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    reinterpret_cast<float4*>(p.conic_opacity)[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+    p.blend_rec[2 * o] = make_float4(0.f, 0.f, 0.f, 0.f);
+    p.blend_rec[2 * o + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
     const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
     if (view_z(cam.view, mu) < 0.2f)
         return;
@@ -118,37 +122,44 @@ __global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<fl
     const Gaussian2d<float> g = splat_project<Formulation::Ots>(w, mu, sc, R, cam, 0.3f);
     const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
     const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
-    p.rects[2 * i] = ex;
-    p.rects[2 * i + 1] = ey;
+    p.rects[2 * o] = ex;
+    p.rects[2 * o + 1] = ey;
     const TileRect r = get_rect(g.centroid.x, g.centroid.y, ex, ey, cam.gx, cam.gy);
     const unsigned touched = (r.x1 - r.x0) * (r.y1 - r.y0);
     if (touched == 0)
         return;
-    p.tiles_touched[i] = touched;
-    p.xy[2 * i] = g.centroid.x;
-    p.xy[2 * i + 1] = g.centroid.y;
+    p.tiles_touched[o] = touched;
+    p.xy[2 * o] = g.centroid.x;
+    p.xy[2 * o + 1] = g.centroid.y;
     const V3<float> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const float depth = len3(sub3(campos, mu));
-    p.depths[i] = depth;
-    p.depth_key[i] = __float_as_uint(depth);
+    p.depths[o] = depth;
+    p.depth_key[o] = __float_as_uint(depth);
     const V3<float> v = sub3(mu, campos);
     const V3<float> dir = mul3(v, 1.f / dgmr_fm::sqrt_f(dot3(v, v)));
     uint8_t mask[3];
     const V3<float> col = sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, mask);
-    p.rgb[3 * i] = col.x;
-    p.rgb[3 * i + 1] = col.y;
-    p.rgb[3 * i + 2] = col.z;
+    p.rgb[3 * o] = col.x;
+    p.rgb[3 * o + 1] = col.y;
+    p.rgb[3 * o + 2] = col.z;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        p.clamped[3 * i + c] = mask[c];
+        p.clamped[3 * o + c] = mask[c];
     const S2<float> con = inverse2(g.cov);
-    reinterpret_cast<float4*>(p.conic_opacity)[i] = make_float4(con.v[0], con.v[1], con.v[2], g.weight);
+    reinterpret_cast<float4*>(p.conic_opacity)[o] = make_float4(con.v[0], con.v[1], con.v[2], g.weight);
     // q_cut: any pixel with d'Qd > q_cut has opacity * exp(-d'Qd/2) < exp(-1e-3) / 255, i.e. alpha < 1/255
     // with a margin far above the rounding of the exponential, so the blend may skip it without changing
     // a single result
     const float q_cut = 2.f * (dgmr_fm::log_f(255.f * g.weight) + 1e-3f);
-    p.blend_rec[2 * i] = make_float4(g.centroid.x, g.centroid.y, con.v[0], con.v[2]);
-    p.blend_rec[2 * i + 1] = make_float4(2.f * con.v[1], g.weight, q_cut, 0.f);
+    p.blend_rec[2 * o] = make_float4(g.centroid.x, g.centroid.y, con.v[0], con.v[2]);
+    p.blend_rec[2 * o + 1] = make_float4(2.f * con.v[1], g.weight, q_cut, 0.f);
+}
+
+__global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<float> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.N)
+        preprocess_one(p, cam, i, i);
 }
 
 // d'Qd of one (pixel, splat) pair (splat_forward.cu:302), evaluated as
@@ -231,9 +242,33 @@ __device__ __forceinline__ float rect_min_q(float cx, float cy, float a, float b
 // test loses a splat); the rest are compacted in list order into shared memory
 // as 32-byte records and evaluated by both pixels.  The block stops when every
 // pixel is saturated.
+// Where one tile's pixels live: the frame it belongs to and the tile's index
+// inside that frame's grid.  final_T / n_contrib / grad_fb point at the
+// frame's own planes.
+struct FrameRef {
+    unsigned W, H, gx, tile;
+    float bg0, bg1, bg2;
+    float* fb;
+    float* final_T;
+    int32_t* n_contrib;
+    const float* grad_fb;
+};
+
+// A single frame: every tile is one of its tiles.
+struct SingleFrame {
+    unsigned W, H, gx;
+    float bg0, bg1, bg2;
+    float* fb;
+    float* final_T;
+    int32_t* n_contrib;
+    const float* grad_fb;
+    __device__ __forceinline__ FrameRef frame(uint32_t tile) const { return FrameRef { W, H, gx, tile, bg0, bg1, bg2, fb, final_T, n_contrib, grad_fb }; }
+};
+
+template <class Frames>
 __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
-    const float* __restrict__ rgb, float* __restrict__ fb, float* __restrict__ final_T, int32_t* __restrict__ n_contrib, unsigned W, unsigned H, unsigned gx,
-    float bg0, float bg1, float bg2, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, const uint32_t* __restrict__ tile_order)
+    const float* __restrict__ rgb, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, const uint32_t* __restrict__ tile_order,
+    const __grid_constant__ Frames frames)
 {
     constexpr int kThreads = 128;
     constexpr int kPer = 2; // list entries loaded per thread per batch
@@ -244,7 +279,9 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
     __shared__ float s_rgb[3][kBatch];
     __shared__ int s_warp_tot[kWarps];
     const unsigned tile = tile_order ? tile_order[blockIdx.x] : blockIdx.x;
-    const unsigned tx = tile % gx, ty = tile / gx;
+    const FrameRef f = frames.frame(tile);
+    const unsigned W = f.W, H = f.H;
+    const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u);
     const unsigned py0 = ty * kTile + (threadIdx.x >> 4), py1 = py0 + 8;
     PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py0 < H) };
@@ -337,19 +374,19 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
     const size_t plane = size_t(W) * H;
     if (in0) {
         const size_t pix = size_t(py0) * W + px;
-        fb[pix] = p0.c0 + p0.T * bg0;
-        fb[plane + pix] = p0.c1 + p0.T * bg1;
-        fb[2 * plane + pix] = p0.c2 + p0.T * bg2;
-        final_T[pix] = p0.T;
-        n_contrib[pix] = p0.last;
+        f.fb[pix] = p0.c0 + p0.T * f.bg0;
+        f.fb[plane + pix] = p0.c1 + p0.T * f.bg1;
+        f.fb[2 * plane + pix] = p0.c2 + p0.T * f.bg2;
+        f.final_T[pix] = p0.T;
+        f.n_contrib[pix] = p0.last;
     }
     if (in1) {
         const size_t pix = size_t(py1) * W + px;
-        fb[pix] = p1.c0 + p1.T * bg0;
-        fb[plane + pix] = p1.c1 + p1.T * bg1;
-        fb[2 * plane + pix] = p1.c2 + p1.T * bg2;
-        final_T[pix] = p1.T;
-        n_contrib[pix] = p1.last;
+        f.fb[pix] = p1.c0 + p1.T * f.bg0;
+        f.fb[plane + pix] = p1.c1 + p1.T * f.bg1;
+        f.fb[2 * plane + pix] = p1.c2 + p1.T * f.bg2;
+        f.final_T[pix] = p1.T;
+        f.n_contrib[pix] = p1.last;
     }
 }
 
@@ -364,10 +401,10 @@ __device__ __forceinline__ float warp_sum(float v)
 // Reverse-order blend adjoint: each pixel walks its contributors back to
 // front, recovering T_i = T_{i+1} / (1 - alpha_i); per-splat gradients are
 // summed over the warp with shuffles before one atomic per value.
+template <class Frames>
 __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
-    const float* __restrict__ xy, const float* __restrict__ conic_opacity, const float* __restrict__ rgb, const float* __restrict__ final_T,
-    const int32_t* __restrict__ n_contrib, const float* __restrict__ grad_fb, float* __restrict__ acc, unsigned W, unsigned H, unsigned gx, float bg0, float bg1,
-    float bg2)
+    const float* __restrict__ xy, const float* __restrict__ conic_opacity, const float* __restrict__ rgb, float* __restrict__ acc,
+    const __grid_constant__ Frames frames)
 {
     __shared__ float2 s_xy[256];
     __shared__ float4 s_co[256];
@@ -375,12 +412,14 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
     __shared__ uint32_t s_id[256];
     __shared__ int s_max;
     const unsigned tile = blockIdx.x;
-    const unsigned tx = tile % gx, ty = tile / gx;
+    const FrameRef f = frames.frame(tile);
+    const unsigned W = f.W, H = f.H;
+    const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
     const bool inside = px < W && py < H;
     const int32_t b = ranges[2 * tile];
     const size_t pix = size_t(py) * W + px;
-    const int32_t my_n = inside ? n_contrib[pix] : 0;
+    const int32_t my_n = inside ? f.n_contrib[pix] : 0;
     if (threadIdx.x == 0)
         s_max = 0;
     __syncthreads();
@@ -389,12 +428,12 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
     const int32_t max_n = s_max;
     float g0 = 0.f, g1 = 0.f, g2 = 0.f, Tf = 1.f;
     if (inside) {
-        g0 = grad_fb[pix];
-        g1 = grad_fb[size_t(W) * H + pix];
-        g2 = grad_fb[2 * size_t(W) * H + pix];
-        Tf = final_T[pix];
+        g0 = f.grad_fb[pix];
+        g1 = f.grad_fb[size_t(W) * H + pix];
+        g2 = f.grad_fb[2 * size_t(W) * H + pix];
+        Tf = f.final_T[pix];
     }
-    const float bg_dot = (bg0 * g0 + bg1 * g1) + bg2 * g2;
+    const float bg_dot = (f.bg0 * g0 + f.bg1 * g1) + f.bg2 * g2;
     float Tr = Tf;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f; // accumulated colour behind the current splat
     const float fpx = float(px), fpy = float(py);
@@ -479,12 +518,8 @@ struct SplatBwdGauss {
     float* g_rotations;
 };
 
-// per-Gaussian chain rule: conic -> 2-D covariance -> projection adjoint, SH
-__global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, CameraT<float> cam)
+__device__ __forceinline__ void zero_gaussian_grads(const SplatBwdGauss& p, uint32_t i)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.N)
-        return;
     for (int k = 0; k < p.sh_stride * 3; ++k)
         p.g_sh[size_t(i) * p.sh_stride * 3 + k] = 0.f;
     p.g_weights[i] = 0.f;
@@ -496,9 +531,16 @@ __global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, Ca
 #pragma unroll
     for (int k = 0; k < 4; ++k)
         p.g_rotations[4 * i + k] = 0.f;
-    if (p.tiles_touched[i] == 0)
+}
+
+// per-Gaussian chain rule: conic -> 2-D covariance -> projection adjoint, SH.
+// Gaussian i of the scene, per-view state at slot o; the result is added to
+// the (zeroed) gradient rows of i, so several views of one scene sum up.
+__device__ __forceinline__ void bwd_gaussian_one(const SplatBwdGauss& p, const CameraT<float>& cam, uint32_t i, uint32_t o)
+{
+    if (p.tiles_touched[o] == 0)
         return;
-    const float* a = p.acc + size_t(i) * 9;
+    const float* a = p.acc + size_t(o) * 9;
     const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
     const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
     const float* q = p.rotations + 4 * size_t(i);
@@ -521,19 +563,29 @@ __global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, Ca
     const V3<float> v = sub3(mu, campos);
     const float vl = dgmr_fm::sqrt_f(dot3(v, v));
     const V3<float> dir = mul3(v, 1.f / vl);
-    const V3<float> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<float> { a[6], a[7], a[8] }, p.clamped + 3 * size_t(i), 0.f, p.g_sh);
+    const V3<float> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<float> { a[6], a[7], a[8] }, p.clamped + 3 * size_t(o), 0.f, p.g_sh,
+        true);
     const float gd = dot3(g_dir, dir);
     g_mu = add3(g_mu, mul3(sub3(g_dir, mul3(dir, gd)), 1.f / vl));
-    p.g_weights[i] = g_weight;
-    p.g_centroids[3 * i] = g_mu.x;
-    p.g_centroids[3 * i + 1] = g_mu.y;
-    p.g_centroids[3 * i + 2] = g_mu.z;
-    p.g_scales[3 * i] = g_s.x * cam.cov_scale_multiplier;
-    p.g_scales[3 * i + 1] = g_s.y * cam.cov_scale_multiplier;
-    p.g_scales[3 * i + 2] = g_s.z * cam.cov_scale_multiplier;
+    p.g_weights[i] += g_weight;
+    p.g_centroids[3 * i] += g_mu.x;
+    p.g_centroids[3 * i + 1] += g_mu.y;
+    p.g_centroids[3 * i + 2] += g_mu.z;
+    p.g_scales[3 * i] += g_s.x * cam.cov_scale_multiplier;
+    p.g_scales[3 * i + 1] += g_s.y * cam.cov_scale_multiplier;
+    p.g_scales[3 * i + 2] += g_s.z * cam.cov_scale_multiplier;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-        p.g_rotations[4 * i + k] = g_q[k];
+        p.g_rotations[4 * i + k] += g_q[k];
+}
+
+__global__ void __launch_bounds__(128) k_splat_bwd_gaussians(SplatBwdGauss p, CameraT<float> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N)
+        return;
+    zero_gaussian_grads(p, i);
+    bwd_gaussian_one(p, cam, i, i);
 }
 
 } // namespace dgmr
@@ -552,6 +604,11 @@ SplatPre make_pre(const dgmr_scene* scene, const SplatLayout& L)
     return SplatPre { uint32_t(scene->n_gaussians), static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride,
         scene->sh_degree, static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations),
         L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm, L.blend_rec };
+}
+
+SingleFrame single_frame(const CameraT<float>& cam, float* fb, const SplatLayout& L, const float* grad_fb = nullptr)
+{
+    return SingleFrame { cam.W, cam.H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2], fb, L.final_T, L.n_contrib, grad_fb };
 }
 
 // per-Gaussian preprocess and the inclusive scan (splat_forward.cu:70-139)
@@ -573,8 +630,7 @@ void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb
     const int par
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
     k_tile_order<<<1, 1024, 0, s>>>(L.ranges, cam.gx * cam.gy, L.tile_order);
-    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, fb, L.final_T, L.n_contrib, cam.W, cam.H, cam.gx,
-        cam.bg[0], cam.bg[1], cam.bg[2], N, cap, st_dev, L.tile_order);
+    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, N, cap, st_dev, L.tile_order, single_frame(cam, fb, L));
     note_launch(2);
 }
 
@@ -697,8 +753,8 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
     const CameraT<float> cam = make_camera<float>(*camera);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int par = tile_sort_parity(cam.gx * cam.gy);
-    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, framebuffer, L.final_T, L.n_contrib, cam.W, cam.H,
-        cam.gx, cam.bg[0], cam.bg[1], cam.bg[2], uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats, L.tile_order);
+    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
+        L.tile_order, single_frame(cam, framebuffer, L));
     note_launch();
     return launch_status();
 }
@@ -723,12 +779,368 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(cam.gx * cam.gy);
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
-    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.final_T, L.n_contrib, grad_framebuffer,
-        L.grad_acc, cam.W, cam.H, cam.gx, cam.bg[0], cam.bg[1], cam.bg[2]);
+    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc,
+        single_frame(cam, nullptr, L, grad_framebuffer));
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
         L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations };
     k_splat_bwd_gaussians<<<(N + 127) / 128, 128, 0, s>>>(p, cam);
+    note_launch(2);
+    return launch_status();
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched multi-view rendering.
+//
+// Many views -- cameras of one or several resident scenes, each at its own
+// resolution -- go through ONE launch sequence: one preprocess over every
+// (view, Gaussian) slot, one depth sort, one pair emission, one tile sort and
+// one blend over the tiles of all views, ordered heaviest-first across views.
+// Slots of view v are [g_off[v], g_off[v+1]); its tiles are numbered from
+// tile_off[v].  The stable depth sort over all slots keeps every view's
+// Gaussians in their own (depth, index) order and a global tile holds pairs
+// of one view only, so each view's point list, ranges and image are the same,
+// bit for bit, as when it is rendered alone.  The view table travels as a
+// __grid_constant__ kernel parameter (no host copy, nothing to keep alive,
+// capturable in a CUDA graph).
+
+namespace dgmr {
+
+constexpr int kMaxBatchViews = DGMR_BATCH_MAX_VIEWS;
+constexpr int kMaxBatchScenes = DGMR_BATCH_MAX_SCENES;
+
+struct BatchScene {
+    const float* centroids;
+    const float* sh;
+    const float* weights;
+    const float* scales;
+    const float* rotations;
+    uint32_t n;
+    int sh_stride, sh_degree;
+    uint32_t view_begin, view_end; // range in BatchTable::view_by_scene
+    float* g_sh;
+    float* g_weights;
+    float* g_centroids;
+    float* g_scales;
+    float* g_rotations;
+};
+
+struct BatchView {
+    CameraT<float> cam;
+    float* fb;
+    const float* grad_fb;
+    uint32_t scene, g_off, tile_off;
+    size_t px_off;
+};
+
+struct BatchTable {
+    uint32_t n_views, n_scenes, G, n_tiles;
+    uint32_t g_off[kMaxBatchViews + 1];
+    uint32_t tile_off[kMaxBatchViews + 1];
+    uint32_t scene_off[kMaxBatchScenes + 1];
+    uint8_t view_by_scene[kMaxBatchViews];
+    float* final_T;
+    int32_t* n_contrib;
+    BatchScene scenes[kMaxBatchScenes];
+    BatchView views[kMaxBatchViews];
+
+    // largest v with off[v] <= x (views that own nothing are skipped over)
+    __device__ __forceinline__ static uint32_t owner(const uint32_t* off, uint32_t n, uint32_t x)
+    {
+        uint32_t lo = 0, hi = n;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (off[mid] <= x)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        return lo;
+    }
+    __device__ __forceinline__ TileGrid grid(uint32_t g) const
+    {
+        const uint32_t v = owner(g_off, n_views, g);
+        return TileGrid { views[v].cam.gx, views[v].cam.gy, tile_off[v] };
+    }
+    __device__ __forceinline__ FrameRef frame(uint32_t t) const
+    {
+        const uint32_t v = owner(tile_off, n_views, t);
+        const BatchView& bv = views[v];
+        return FrameRef { bv.cam.W, bv.cam.H, bv.cam.gx, t - tile_off[v], bv.cam.bg[0], bv.cam.bg[1], bv.cam.bg[2], bv.fb, final_T + bv.px_off,
+            n_contrib + bv.px_off, bv.grad_fb };
+    }
+};
+static_assert(sizeof(BatchTable) < 32000, "the view table must fit in the kernel parameter space");
+
+__global__ void __launch_bounds__(256) k_batch_preprocess(SplatPre out, const __grid_constant__ BatchTable tab)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= tab.G)
+        return;
+    const uint32_t v = BatchTable::owner(tab.g_off, tab.n_views, g);
+    const BatchView& bv = tab.views[v];
+    const BatchScene& sc = tab.scenes[bv.scene];
+    SplatPre p = out;
+    p.N = sc.n;
+    p.centroids = sc.centroids;
+    p.sh = sc.sh;
+    p.sh_stride = sc.sh_stride;
+    p.sh_degree = sc.sh_degree;
+    p.weights = sc.weights;
+    p.scales = sc.scales;
+    p.rotations = sc.rotations;
+    preprocess_one(p, bv.cam, g - tab.g_off[v], g);
+}
+
+// per scene Gaussian: zero its gradient rows, then add the chain rule of
+// every view of its scene, in view order (deterministic, no atomics)
+__global__ void __launch_bounds__(128) k_batch_bwd_gaussians(SplatBwdGauss state, const __grid_constant__ BatchTable tab)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= tab.scene_off[tab.n_scenes])
+        return;
+    const uint32_t s = BatchTable::owner(tab.scene_off, tab.n_scenes, k);
+    const BatchScene& sc = tab.scenes[s];
+    const uint32_t i = k - tab.scene_off[s];
+    SplatBwdGauss p = state;
+    p.N = sc.n;
+    p.centroids = sc.centroids;
+    p.sh = sc.sh;
+    p.sh_stride = sc.sh_stride;
+    p.sh_degree = sc.sh_degree;
+    p.weights = sc.weights;
+    p.scales = sc.scales;
+    p.rotations = sc.rotations;
+    p.g_sh = sc.g_sh;
+    p.g_weights = sc.g_weights;
+    p.g_centroids = sc.g_centroids;
+    p.g_scales = sc.g_scales;
+    p.g_rotations = sc.g_rotations;
+    zero_gaussian_grads(p, i);
+    for (uint32_t q = sc.view_begin; q < sc.view_end; ++q) {
+        const uint32_t v = tab.view_by_scene[q];
+        bwd_gaussian_one(p, tab.views[v].cam, i, tab.g_off[v] + i);
+    }
+}
+
+} // namespace dgmr
+
+namespace {
+
+struct BatchPlan {
+    BatchTable tab;
+    SplatLayout L;
+    size_t px_total;
+};
+
+// Validates the batch and builds its table and workspace layout.  grads may be
+// null (forward).  Bases may be null (size query).
+dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, const dgmr_scene_grads* grads,
+    int64_t pair_capacity, void* frame_ws, void* pair_ws, BatchPlan& plan)
+{
+    if (!scenes || !views || n_scenes <= 0 || n_views <= 0 || n_scenes > kMaxBatchScenes || n_views > kMaxBatchViews || pair_capacity < 0
+        || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    BatchTable& t = plan.tab;
+    std::memset(&t, 0, sizeof(t));
+    t.n_views = uint32_t(n_views);
+    t.n_scenes = uint32_t(n_scenes);
+    uint64_t G = 0, T = 0, px = 0, gs = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        const dgmr_scene& sc = scenes[s];
+        if (sc.dtype != DGMR_F32 || sc.n_gaussians < 0 || sc.sh_stride < 1 || sc.sh_stride > 16 || sc.sh_degree < 0 || sc.sh_degree > 3)
+            return DGMR_ERR_BAD_ARG;
+        if (sc.n_gaussians > 0 && (!sc.centroids || !sc.sh || !sc.weights || !sc.scales || !sc.rotations))
+            return DGMR_ERR_BAD_ARG;
+        BatchScene& b = t.scenes[s];
+        b.centroids = static_cast<const float*>(sc.centroids);
+        b.sh = static_cast<const float*>(sc.sh);
+        b.weights = static_cast<const float*>(sc.weights);
+        b.scales = static_cast<const float*>(sc.scales);
+        b.rotations = static_cast<const float*>(sc.rotations);
+        b.n = uint32_t(sc.n_gaussians);
+        b.sh_stride = sc.sh_stride;
+        b.sh_degree = sc.sh_degree;
+        if (grads) {
+            const dgmr_scene_grads& g = grads[s];
+            if (sc.n_gaussians > 0 && (!g.sh || !g.weights || !g.centroids || !g.scales || !g.rotations))
+                return DGMR_ERR_BAD_ARG;
+            b.g_sh = g.sh;
+            b.g_weights = g.weights;
+            b.g_centroids = g.centroids;
+            b.g_scales = g.scales;
+            b.g_rotations = g.rotations;
+        }
+        t.scene_off[s] = uint32_t(gs);
+        gs += uint64_t(sc.n_gaussians);
+    }
+    t.scene_off[n_scenes] = uint32_t(gs);
+    // views grouped by scene, each group in view order
+    uint32_t q = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        t.scenes[s].view_begin = q;
+        for (int v = 0; v < n_views; ++v)
+            if (views[v].scene == s)
+                t.view_by_scene[q++] = uint8_t(v);
+        t.scenes[s].view_end = q;
+    }
+    for (int v = 0; v < n_views; ++v) {
+        const dgmr_batch_view& bv = views[v];
+        if (bv.scene < 0 || bv.scene >= n_scenes)
+            return DGMR_ERR_BAD_ARG;
+        const dgmr_camera& c = bv.camera;
+        if (c.width <= 0 || c.height <= 0 || c.width > 65536 || c.height > 65536)
+            return DGMR_ERR_BAD_ARG;
+        BatchView& w = t.views[v];
+        w.cam = make_camera<float>(c);
+        w.fb = bv.framebuffer;
+        w.grad_fb = bv.grad_framebuffer;
+        w.scene = uint32_t(bv.scene);
+        w.g_off = uint32_t(G);
+        w.tile_off = uint32_t(T);
+        w.px_off = size_t(px);
+        t.g_off[v] = uint32_t(G);
+        t.tile_off[v] = uint32_t(T);
+        G += uint64_t(scenes[bv.scene].n_gaussians);
+        T += uint64_t(w.cam.gx) * w.cam.gy;
+        px += uint64_t(c.width) * uint64_t(c.height);
+    }
+    t.g_off[n_views] = uint32_t(G);
+    t.tile_off[n_views] = uint32_t(T);
+    if (G > 0x7fffffffull || T > (1ull << 30) || gs > 0x7fffffffull)
+        return DGMR_ERR_BAD_ARG;
+    t.G = uint32_t(G);
+    t.n_tiles = uint32_t(T);
+    plan.px_total = size_t(px);
+    plan.L = splat_layout_n(t.G, t.n_tiles, plan.px_total, uint32_t(pair_capacity), frame_ws, pair_ws);
+    t.final_T = plan.L.final_T;
+    t.n_contrib = plan.L.n_contrib;
+    return DGMR_OK;
+}
+
+SplatPre batch_pre(const SplatLayout& L, uint32_t G)
+{
+    return SplatPre { G, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched,
+        L.bin.depth_key, L.bin.perm, L.blend_rec };
+}
+
+// need_pairs = false for the preprocess alone, which touches no pair buffer
+dgmr_status batch_check_ws(const BatchPlan& plan, void* frame_ws, size_t frame_bytes, void* pair_ws, size_t pair_bytes, int64_t pair_capacity,
+    bool need_pairs = true)
+{
+    if (!frame_ws || (need_pairs && pair_capacity > 0 && !pair_ws))
+        return DGMR_ERR_BAD_ARG;
+    if (frame_bytes < plan.L.bytes || (need_pairs && pair_bytes < plan.L.pair_bytes))
+        return DGMR_ERR_WORKSPACE;
+    return DGMR_OK;
+}
+
+void batch_preprocess(const BatchPlan& plan, uint32_t* st_dev, cudaStream_t s)
+{
+    const SplatLayout& L = plan.L;
+    const uint32_t G = plan.tab.G;
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    if (G == 0)
+        return;
+    k_batch_preprocess<<<(G + 255) / 256, 256, 0, s>>>(batch_pre(L, G), plan.tab);
+    note_launch();
+    inclusive_scan_u32(L.tiles_touched, L.point_offsets, G, L.bin.scan_tmp, s);
+}
+
+} // namespace
+
+extern "C" {
+
+dgmr_status dgmr_splat_batch_workspace_size(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, int64_t pair_capacity,
+    size_t* frame_workspace_bytes, size_t* pair_workspace_bytes)
+{
+    if (!frame_workspace_bytes || !pair_workspace_bytes)
+        return DGMR_ERR_BAD_ARG;
+    static thread_local BatchPlan plan;
+    const dgmr_status st = make_batch(scenes, n_scenes, views, n_views, nullptr, pair_capacity, nullptr, nullptr, plan);
+    if (st != DGMR_OK)
+        return st;
+    *frame_workspace_bytes = plan.L.bytes;
+    *pair_workspace_bytes = plan.L.pair_bytes;
+    return DGMR_OK;
+}
+
+dgmr_status dgmr_splat_batch_preprocess(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    static thread_local BatchPlan plan;
+    dgmr_status st = make_batch(scenes, n_scenes, views, n_views, nullptr, 0, frame_workspace, nullptr, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = batch_check_ws(plan, frame_workspace, frame_workspace_bytes, nullptr, 0, 0, false);
+    if (st != DGMR_OK)
+        return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : plan.L.stats;
+    batch_preprocess(plan, st_dev, s);
+    if (plan.tab.G > 0) {
+        k_pair_count<<<1, 1, 0, s>>>(plan.L.point_offsets, plan.tab.G, 0xffffffffu, st_dev, plan.L.bin.n_sort);
+        note_launch();
+    }
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    static thread_local BatchPlan plan;
+    dgmr_status st = make_batch(scenes, n_scenes, views, n_views, nullptr, pair_capacity, frame_workspace, pair_workspace, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = batch_check_ws(plan, frame_workspace, frame_workspace_bytes, pair_workspace, pair_workspace_bytes, pair_capacity);
+    if (st != DGMR_OK)
+        return st;
+    for (int v = 0; v < n_views; ++v)
+        if (!views[v].framebuffer)
+            return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    SplatLayout& L = plan.L;
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    const uint32_t G = plan.tab.G, cap = uint32_t(pair_capacity);
+    batch_preprocess(plan, st_dev, s);
+    const int par = run_binning_grids<float>(G, plan.tab.n_tiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev,
+        num_sms(), s, true);
+    k_tile_order<<<1, 1024, 0, s>>>(L.ranges, plan.tab.n_tiles, L.tile_order);
+    k_splat_blend<<<plan.tab.n_tiles, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab);
+    note_launch(2);
+    return launch_status();
+}
+
+dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
+    const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
+    int64_t pair_capacity, dgmr_stream stream)
+{
+    if (!grads)
+        return DGMR_ERR_BAD_ARG;
+    static thread_local BatchPlan plan;
+    dgmr_status st = make_batch(scenes, n_scenes, views, n_views, grads, pair_capacity, frame_workspace, pair_workspace, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = batch_check_ws(plan, frame_workspace, frame_workspace_bytes, pair_workspace, pair_workspace_bytes, pair_capacity);
+    if (st != DGMR_OK)
+        return st;
+    for (int v = 0; v < n_views; ++v)
+        if (!views[v].grad_framebuffer)
+            return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const SplatLayout& L = plan.L;
+    const uint32_t G = plan.tab.G;
+    const uint32_t n_scene_gaussians = plan.tab.scene_off[n_scenes];
+    if (n_scene_gaussians == 0)
+        return DGMR_OK;
+    const int par = tile_sort_parity(plan.tab.n_tiles);
+    cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
+    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc, plan.tab);
+    SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
+        nullptr };
+    k_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);
     note_launch(2);
     return launch_status();
 }

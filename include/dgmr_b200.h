@@ -152,6 +152,53 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     float* grad_centroids, float* grad_scales, float* grad_rotations, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace,
     size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_stream stream);
 
+/* ------------------------------------------------------- batched splat */
+
+/* Many views of one or several scenes rendered by ONE launch sequence (no
+ * reference counterpart: the reference renders one view per call,
+ * splat_forward.cu:30-338).  Each view's image, point list and tile ranges are
+ * bit-identical to a dgmr_splat_forward of that view alone.  All views share one
+ * frame workspace and one pair workspace (pair_capacity = pairs of all views
+ * together), sized by dgmr_splat_batch_workspace_size.  No allocation, no host
+ * synchronisation: the calls can be captured in a CUDA graph. */
+#define DGMR_BATCH_MAX_VIEWS 64
+#define DGMR_BATCH_MAX_SCENES 16
+
+typedef struct dgmr_batch_view {
+    int32_t scene; /* index into the scenes array */
+    int32_t reserved;
+    dgmr_camera camera;
+    float* framebuffer; /* [3,H,W] device, written by the forward */
+    const float* grad_framebuffer; /* [3,H,W] device, read by the backward */
+} dgmr_batch_view;
+
+typedef struct dgmr_scene_grads { /* device outputs of the batched backward, per scene */
+    float* sh; /* [N,sh_stride,3] */
+    float* weights; /* [N] */
+    float* centroids; /* [N,3] */
+    float* scales; /* [N,3] */
+    float* rotations; /* [N,4] */
+} dgmr_scene_grads;
+
+dgmr_status dgmr_splat_batch_workspace_size(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, int64_t pair_capacity,
+    size_t* frame_workspace_bytes, size_t* pair_workspace_bytes);
+
+/* First half only: preprocess of every view and the pair count of the whole
+ * batch into stats->n_pairs (to size pair_capacity, like the reference's
+ * .item() read of the pair count, splat_forward.cu:141). */
+dgmr_status dgmr_splat_batch_preprocess(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream);
+
+dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Backward of the last batched forward run in these workspaces.  Gradients of
+ * every scene are written (not accumulated): the sum over that scene's views,
+ * added in view order. */
+dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
+    const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
+    int64_t pair_capacity, dgmr_stream stream);
+
 /* ---------------------------------------------------------- vol_marcher */
 
 /* The reference's ForwardCache plus framebuffer (vol_marcher_forward.h:28-41,

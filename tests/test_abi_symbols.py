@@ -52,3 +52,45 @@ def test_bad_arguments_are_rejected_on_the_host():
     scene.sh_stride = 1
     assert lib.dgmr_splat_forward(scene, cam, None, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
     assert lib.dgmr_vm_set_const_samples(5, None) == _native.DGMR_ERR_BAD_ARG
+
+
+def _batch_tables(n_views, scene_index=0, n_scenes=1):
+    scenes = (_native.Scene * n_scenes)()
+    for s in scenes:
+        s.n_gaussians, s.sh_stride, s.sh_degree, s.dtype = 1000, 1, 0, 0
+        s.centroids = s.sh = s.weights = s.scales = s.rotations = 4096  # never dereferenced by the size query
+    views = (_native.BatchView * n_views)()
+    for k, v in enumerate(views):
+        v.scene = scene_index
+        v.camera.width, v.camera.height = 64 + 16 * k, 48
+        for i in (0, 5, 10, 15):
+            v.camera.view[i] = v.camera.proj[i] = 1.0
+        v.camera.tan_fovx = v.camera.tan_fovy = 0.5
+    return scenes, views
+
+
+def test_batch_workspace_query_without_gpu():
+    import ctypes as C
+    lib = _native.load()
+    fb, pb = C.c_size_t(0), C.c_size_t(0)
+    scenes, views = _batch_tables(3)
+    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 3, 1000, C.byref(fb), C.byref(pb)) == 0
+    three = (fb.value, pb.value)
+    scenes, views = _batch_tables(6)
+    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 6, 1000, C.byref(fb), C.byref(pb)) == 0
+    assert fb.value > three[0]  # twice the view-Gaussian slots
+    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 6, 100000, C.byref(fb), C.byref(pb)) == 0
+    assert pb.value > three[1]
+
+
+def test_batch_bad_arguments_without_gpu():
+    import ctypes as C
+    lib = _native.load()
+    fb, pb = C.c_size_t(0), C.c_size_t(0)
+    scenes, views = _batch_tables(2, scene_index=1)  # scene index out of range
+    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 2, 0, C.byref(fb), C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
+    scenes, views = _batch_tables(_native.BATCH_MAX_VIEWS + 1)
+    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, _native.BATCH_MAX_VIEWS + 1, 0, C.byref(fb),
+                                               C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
+    scenes, views = _batch_tables(2)
+    assert lib.dgmr_splat_batch_forward(scenes, 1, views, 2, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
