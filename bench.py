@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--slots", type=int, default=3, help="requests in flight")
     ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["served", "batched", "marcher"], default="served",
+                    help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
+                         "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512")
     return ap.parse_args()
 
 
@@ -376,10 +379,152 @@ def run_ours(args):
     return 0
 
 
+def _gpu_common():
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    return torch, torch.device("cuda", local), local
+
+
+def run_batched(args):
+    """3 resident scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras each,
+    resolutions cycling 256x256 / 800x600 / 1920x1080, forward + backward of
+    all 48 views per step: autotuned batch depth under CUDA graphs, against the
+    plain per-view calls (forward, pair count read back, backward)."""
+    torch, dev, local = _gpu_common()
+    from differentiable_gaussian_mixture_renderer_b200 import _native as N
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200 import splat
+    from differentiable_gaussian_mixture_renderer_b200.batch import BatchRenderer, autotune, chunks
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene
+    sizes = {"s50k": 50_000, "s300k": 300_000, "s1500k": 1_500_000}
+    res = [(256, 256), (800, 600), (1920, 1080)]
+    scenes = {k: GaussianScene.from_numpy(S.make_scene(n, seed=i), dev) for i, (k, n) in enumerate(sizes.items())}
+    views = []
+    for j, k in enumerate(sizes):
+        for v in range(16):
+            w, h = res[v % 3]
+            views.append((k, S.random_cameras(1, w, h, seed=100 * j + v)[0]))
+    px = sum(c.width * c.height for _, c in views)
+    r = BatchRenderer(scenes, dev)
+    best, timings = autotune(r, views, depths=(1, 4, 16, 48), backward=True, reps=2)
+    plans = [r.capture(r.plan(c, backward=True), backward=True) for c in chunks(views, best)]
+    gen = torch.Generator(device=dev).manual_seed(2)
+    for p in plans:
+        for g in p.grad_framebuffers:
+            g.copy_(torch.randn(g.shape, device=dev, generator=gen))
+    s0 = torch.cuda.current_stream(dev)
+
+    def step():
+        for p in plans:
+            p.stream.wait_stream(s0)
+            with torch.cuda.stream(p.stream):
+                p.graph.replay()
+        for p in plans:
+            s0.wait_stream(p.stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for _ in range(args.steps):
+            step()
+        e1.record(s0)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    overflow = any(p.overflowed() for p in plans)
+    # plain per-view calls, the reference's pattern (one view per call, P read back)
+    lat = []
+    for k, (sid, cam) in enumerate(views):
+        sc = scenes[sid]
+        torch.cuda.synchronize(dev)
+        e0.record(s0)
+        fb, frame = splat.splat_forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, cam.view, cam.proj,
+                                        cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
+                                        cam.tan_fovy, sc.sh_degree)
+        splat.splat_backward(frame, plans[0].grad_framebuffers[0].new_ones(fb.shape), sc.shs, sc.weights,
+                             sc.centroids, sc.scales, sc.rotations)
+        e1.record(s0)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+        del fb, frame
+    plain_ms = sum(lat)
+    line = {"metric": "batched views/s, forward+backward, 3 scenes x 16 views, mixed resolutions",
+            "value": len(views) / (ms * 1e-3), "unit": "views/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3 scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras (r=2.5-4), "
+                                   "resolutions cycling 256x256 / 800x600 / 1920x1080, forward + backward",
+                       "views": len(views), "megapixels_per_step": px / 1e6, "batch_depth": best,
+                       "l2": "working set of one step (~30M view-Gaussian slots) far above the 126 MB L2"},
+            "mpix_per_s": px / 1e6 / (ms * 1e-3), "autotune_ms": timings,
+            "plain_per_view": {"value": len(views) / (plain_ms * 1e-3), "unit": "views/s", "ms_per_step": plain_ms},
+            "batched_over_plain": plain_ms / ms, "pair_overflow": overflow,
+            "clocks": clk.summary(), "graph_replays": args.steps * len(plans)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_marcher(args):
+    """vol_marcher forward + backward through the reference-facing binding
+    (cpp_binding.forward / backward): 100k Gaussians, 512x512, fp32."""
+    torch, dev, local = _gpu_common()
+    from differentiable_gaussian_mixture_renderer_b200 import _native as N
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    n, W, H = 100_000, 512, 512
+    sc = S.make_scene(n, seed=0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
+    ins = (t(sc.sh), t(sc.weights).reshape(-1, 1), t(sc.centroids), t(sc.scales), t(sc.rotations))
+    cams = S.random_cameras(args.warmup + args.steps, W, H, seed=1)
+    G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
+    bg = torch.zeros(3, device=dev)
+
+    def step(cam):
+        v, p, c = t(cam.view), t(cam.proj), t(cam.campos)
+        cache = cpp_binding.forward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0)
+        e_mid.record()
+        cpp_binding.backward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache)
+        return cache
+
+    e_mid = torch.cuda.Event(enable_timing=True)
+    for cam in cams[:args.warmup]:
+        step(cam)
+    torch.cuda.synchronize(dev)
+    fwd, bwd = [], []
+    with ClockSampler(local) as clk:
+        l0 = N.lib().dgmr_launch_count()
+        for cam in cams[args.warmup:]:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step(cam)
+            e1.record()
+            e1.synchronize()
+            fwd.append(e0.elapsed_time(e_mid))
+            bwd.append(e_mid.elapsed_time(e1))
+        launches = N.lib().dgmr_launch_count() - l0
+    ms = (sum(fwd) + sum(bwd)) / len(fwd)
+    line = {"metric": "vol_marcher forward+backward ms/frame, 100k Gaussians, 512x512", "value": ms, "unit": "ms",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "vol_marcher forward + backward, 100000 Gaussians (config-0 distribution), "
+                                   "512x512, random cameras r=2.5-4, through cpp_binding.forward/backward"},
+            "forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+            "clocks": clk.summary(), "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "marcher":
+        return run_marcher(args)
     return run_ours(args)
 
 
