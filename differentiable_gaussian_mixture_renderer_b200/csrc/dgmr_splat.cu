@@ -413,6 +413,8 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
     __shared__ int s_max;
     const unsigned tile = blockIdx.x;
     const FrameRef f = frames.frame(tile);
+    if (!f.grad_fb) // a view without an image gradient (batched renders that only asked for the image)
+        return;
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
@@ -904,6 +906,8 @@ __global__ void __launch_bounds__(128) k_batch_bwd_gaussians(SplatBwdGauss state
     const uint32_t s = BatchTable::owner(tab.scene_off, tab.n_scenes, k);
     const BatchScene& sc = tab.scenes[s];
     const uint32_t i = k - tab.scene_off[s];
+    if (!sc.g_sh) // a scene entry without gradient outputs
+        return;
     SplatBwdGauss p = state;
     p.N = sc.n;
     p.centroids = sc.centroids;
@@ -921,7 +925,8 @@ __global__ void __launch_bounds__(128) k_batch_bwd_gaussians(SplatBwdGauss state
     zero_gaussian_grads(p, i);
     for (uint32_t q = sc.view_begin; q < sc.view_end; ++q) {
         const uint32_t v = tab.view_by_scene[q];
-        bwd_gaussian_one(p, tab.views[v].cam, i, tab.g_off[v] + i);
+        if (tab.views[v].grad_fb)
+            bwd_gaussian_one(p, tab.views[v].cam, i, tab.g_off[v] + i);
     }
 }
 
@@ -963,9 +968,9 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
         b.n = uint32_t(sc.n_gaussians);
         b.sh_stride = sc.sh_stride;
         b.sh_degree = sc.sh_degree;
-        if (grads) {
+        if (grads && grads[s].sh) {
             const dgmr_scene_grads& g = grads[s];
-            if (sc.n_gaussians > 0 && (!g.sh || !g.weights || !g.centroids || !g.scales || !g.rotations))
+            if (sc.n_gaussians > 0 && (!g.weights || !g.centroids || !g.scales || !g.rotations))
                 return DGMR_ERR_BAD_ARG;
             b.g_sh = g.sh;
             b.g_weights = g.weights;
@@ -1126,9 +1131,6 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     st = batch_check_ws(plan, frame_workspace, frame_workspace_bytes, pair_workspace, pair_workspace_bytes, pair_capacity);
     if (st != DGMR_OK)
         return st;
-    for (int v = 0; v < n_views; ++v)
-        if (!views[v].grad_framebuffer)
-            return DGMR_ERR_BAD_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const SplatLayout& L = plan.L;
     const uint32_t G = plan.tab.G;

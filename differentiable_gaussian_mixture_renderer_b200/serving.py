@@ -13,6 +13,7 @@ equals the plain per-call render.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import time
 from dataclasses import dataclass, field
@@ -209,3 +210,274 @@ class RenderServer:
         self.ref_event.record(self.slots[0].stream)
         self.t0 = time.perf_counter()
         self.ref_event.synchronize()
+
+
+# ---------------------------------------------------------------------------
+# Continuous batching over several resident scenes.
+#
+# Requests (render, or render + gradient against a caller-given image
+# gradient) arrive at any time.  Whenever a slot (a CUDA stream with its own
+# workspaces) is free, the queue head is cut into one batch -- as many waiting
+# requests as fit the view/scene limits of one batched launch and the free
+# HBM budget -- and launched with dgmr_splat_batch_forward (+ _backward).
+# Requests that arrive while batches are on the GPU wait only for the next
+# free slot; several batches run concurrently on their streams.  Every
+# request owns its output buffers (image, gradients), written in place by the
+# batched kernels, so a result is the same bits alone or in any mix: images
+# bit-identical, gradients equal up to the order of the per-pixel atomics.
+# A gradient request gets its own entry in the batch's scene table (same
+# tensors, its own gradient outputs), so its gradients never mix with another
+# request's.
+
+
+class HbmBudget:
+    """Bytes of device memory the server may hold for in-flight work.  A batch
+    is admitted only if its reservation fits next to what is in flight."""
+
+    def __init__(self, budget_bytes: int):
+        self.budget = int(budget_bytes)
+        self.in_use = 0
+        self.peak = 0
+
+    def fits(self, nbytes: int) -> bool:
+        return self.in_use + int(nbytes) <= self.budget
+
+    def reserve(self, nbytes: int) -> None:
+        if not self.fits(nbytes):
+            raise RuntimeError("reservation exceeds the HBM budget")
+        self.in_use += int(nbytes)
+        self.peak = max(self.peak, self.in_use)
+
+    def release(self, nbytes: int) -> None:
+        self.in_use = max(0, self.in_use - int(nbytes))
+
+
+def form_batch(queue: list, max_views: int, max_scene_entries: int, cost, budget: HbmBudget):
+    """Takes requests from the head of ``queue`` (arrival order, no
+    reordering) while the batch stays within the view and scene-entry limits
+    and ``cost(batch)`` (bytes) fits the budget.  Render requests of one scene
+    share a scene entry; each gradient request has its own.  Returns
+    (batch, bytes); the batch is empty when even the head does not fit."""
+    batch, scenes = [], set()
+    entries = 0
+    nbytes = 0
+    for req in queue:
+        if len(batch) >= max_views:
+            break
+        new_entry = req.backward or req.scene_id not in scenes
+        if new_entry and entries + 1 > max_scene_entries:
+            break
+        trial = batch + [req]
+        c = cost(trial)
+        if not budget.fits(c):
+            break
+        batch = trial
+        nbytes = c
+        if new_entry:
+            entries += 1
+        if not req.backward:
+            scenes.add(req.scene_id)
+    del queue[:len(batch)]
+    return batch, nbytes
+
+
+@dataclass
+class ServeRequest:
+    scene_id: str
+    camera: object
+    backward: bool = False
+    grad_image: torch.Tensor | None = None  # [3,H,W] device, for gradient requests
+    arrival: float = 0.0
+    t_launch: float = 0.0
+    t_done: float = 0.0
+    image: torch.Tensor | None = None
+    grads: tuple | None = None  # (sh, weights, centroids, scales, rotations)
+    batch_size: int = 0
+    rerendered: bool = False
+
+
+@dataclass
+class _BatchSlot:
+    stream: torch.cuda.Stream
+    frame_ws: torch.Tensor | None = None
+    pair_ws: torch.Tensor | None = None
+    stats: torch.Tensor | None = None
+    stats_host: torch.Tensor | None = None
+    done: torch.cuda.Event | None = None
+    batch: list = field(default_factory=list)
+    tables: tuple = ()
+    capacity: int = 0
+    reserved: int = 0
+
+
+class ContinuousServer:
+    """Continuous batching of render and gradient requests over resident scenes."""
+
+    def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.15):
+        self.device = torch.device(device or "cuda")
+        self.scenes = scenes
+        self.lib = N.lib()
+        self.slots = [_BatchSlot(torch.cuda.Stream(device=self.device)) for _ in range(n_slots)]
+        self.max_batch = min(max_batch, N.BATCH_MAX_VIEWS)
+        self.margin = capacity_margin
+        if hbm_budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget_bytes = int(free * 0.8)
+        self.budget = HbmBudget(hbm_budget_bytes)
+        self.queue: list = []
+        self.completed: list = []
+        self.capacity: dict = {}  # (scene_id, W, H) -> pairs
+        self.rerenders = 0
+        self.batches = 0
+        self.deferred = 0  # times the queue head waited for memory held by batches in flight
+
+    # ------------------------------------------------------------ sizing
+    def _pairs(self, req) -> int:
+        key = (req.scene_id, req.camera.width, req.camera.height)
+        if key not in self.capacity:
+            scene = self.scenes[req.scene_id]
+            ws = torch.empty(max(1, self.lib.dgmr_splat_frame_workspace_size(scene.n, key[1], key[2])),
+                             dtype=torch.uint8, device=self.device)
+            stats = torch.zeros(4, dtype=torch.int32, device=self.device)
+            N.check(self.lib.dgmr_splat_preprocess(scene.c_scene(), camera_struct(req.camera), N.ptr(ws), ws.numel(),
+                                                   N.ptr(stats), N.stream_handle()), "splat preprocess")
+            self.capacity[key] = int(math.ceil(int(stats[0].item()) * self.margin)) + 1024
+        return self.capacity[key]
+
+    def _tables(self, batch):
+        entries, scene_of_entry, index = [], [], {}
+        views = (N.BatchView * len(batch))()
+        for k, req in enumerate(batch):
+            if req.backward or req.scene_id not in index:
+                if not req.backward:
+                    index[req.scene_id] = len(entries)
+                entries.append(self.scenes[req.scene_id].c_scene())
+                scene_of_entry.append(req)
+                e = len(entries) - 1
+            else:
+                e = index[req.scene_id]
+            views[k].scene = e
+            views[k].camera = camera_struct(req.camera)
+        scenes = (N.Scene * len(entries))(*entries)
+        return scenes, views, scene_of_entry
+
+    def _cost(self, batch) -> int:
+        scenes, views, _ = self._tables(batch)
+        cap = sum(self._pairs(r) for r in batch)
+        fb, pb = C.c_size_t(0), C.c_size_t(0)
+        N.check(self.lib.dgmr_splat_batch_workspace_size(scenes, len(scenes), views, len(views), cap, C.byref(fb),
+                                                         C.byref(pb)), "batch workspace size")
+        out = sum(12 * r.camera.width * r.camera.height for r in batch)
+        grads = sum(self.scenes[r.scene_id].nbytes() for r in batch if r.backward)
+        return int(fb.value) + int(pb.value) + out + grads
+
+    # ------------------------------------------------------------ running
+    def submit(self, req: ServeRequest) -> ServeRequest:
+        if req.backward and (req.grad_image is None
+                             or tuple(req.grad_image.shape) != (3, req.camera.height, req.camera.width)):
+            raise ValueError("a gradient request needs grad_image [3, H, W]")
+        self.queue.append(req)
+        return req
+
+    def _launch(self, slot: _BatchSlot, batch: list, capacity: int):
+        scenes, views, owners = self._tables(batch)
+        dev = self.device
+        for k, req in enumerate(batch):
+            if req.image is None:
+                req.image = torch.empty((3, req.camera.height, req.camera.width), dtype=torch.float32, device=dev)
+            views[k].framebuffer = req.image.data_ptr()
+            if req.backward:
+                views[k].grad_framebuffer = req.grad_image.data_ptr()
+        grads = (N.SceneGrads * len(owners))()
+        any_bwd = False
+        for e, req in enumerate(owners):
+            if req.backward:
+                any_bwd = True
+                sc = self.scenes[req.scene_id]
+                if req.grads is None:
+                    req.grads = (torch.empty_like(sc.shs), torch.empty_like(sc.weights), torch.empty_like(sc.centroids),
+                                 torch.empty_like(sc.scales), torch.empty_like(sc.rotations))
+                g = req.grads
+                grads[e].sh, grads[e].weights, grads[e].centroids = g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr()
+                grads[e].scales, grads[e].rotations = g[3].data_ptr(), g[4].data_ptr()
+        fb, pb = C.c_size_t(0), C.c_size_t(0)
+        N.check(self.lib.dgmr_splat_batch_workspace_size(scenes, len(scenes), views, len(views), capacity, C.byref(fb),
+                                                         C.byref(pb)), "batch workspace size")
+        if slot.frame_ws is None or slot.frame_ws.numel() < fb.value:
+            slot.frame_ws = torch.empty(max(1, fb.value), dtype=torch.uint8, device=dev)
+        if slot.pair_ws is None or slot.pair_ws.numel() < pb.value:
+            slot.pair_ws = torch.empty(max(1, pb.value), dtype=torch.uint8, device=dev)
+        if slot.stats is None:
+            slot.stats = torch.zeros(4, dtype=torch.int32, device=dev)
+            slot.stats_host = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+        s = slot.stream
+        with torch.cuda.stream(s):
+            N.check(self.lib.dgmr_splat_batch_forward(scenes, len(scenes), views, len(views), N.ptr(slot.frame_ws),
+                                                      slot.frame_ws.numel(), N.ptr(slot.pair_ws), slot.pair_ws.numel(),
+                                                      capacity, N.ptr(slot.stats), s.cuda_stream), "batch forward")
+            slot.stats_host.copy_(slot.stats, non_blocking=True)
+            if any_bwd:
+                # render-only views and their scene entries carry null gradient pointers: skipped
+                N.check(self.lib.dgmr_splat_batch_backward(scenes, len(scenes), views, len(views), grads,
+                                                           N.ptr(slot.frame_ws), slot.frame_ws.numel(),
+                                                           N.ptr(slot.pair_ws), slot.pair_ws.numel(), capacity,
+                                                           s.cuda_stream), "batch backward")
+            slot.done = torch.cuda.Event()
+            slot.done.record(s)
+        slot.batch = batch
+        slot.tables = (scenes, views, grads)
+        slot.capacity = capacity
+
+    def _complete(self, slot: _BatchSlot, now: float):
+        n_pairs, flags = int(slot.stats_host[0]), int(slot.stats_host[1])
+        if flags & N.FLAG_PAIR_OVERFLOW:
+            # more pairs than the learnt capacities: grow them and render the batch again, exactly sized
+            self.rerenders += 1
+            for req in slot.batch:
+                key = (req.scene_id, req.camera.width, req.camera.height)
+                self.capacity[key] = int(math.ceil(self.capacity[key] * max(self.margin, n_pairs / slot.capacity)))
+                req.rerendered = True
+            self._launch(slot, slot.batch, int(math.ceil(n_pairs * self.margin)) + 1024)
+            slot.done.synchronize()
+            now = time.perf_counter()
+        for req in slot.batch:
+            req.t_done = now
+            req.batch_size = len(slot.batch)
+            self.completed.append(req)
+        self.budget.release(slot.reserved)
+        slot.batch, slot.tables, slot.reserved = [], (), 0
+
+    def poll(self) -> int:
+        """Completes finished batches and launches new ones on free slots.
+        Returns the number of requests in flight."""
+        now = time.perf_counter()
+        for slot in self.slots:
+            if slot.batch and slot.done.query():
+                self._complete(slot, now)
+        for slot in self.slots:
+            if slot.batch or not self.queue:
+                continue
+            batch, nbytes = form_batch(self.queue, self.max_batch, N.BATCH_MAX_SCENES, self._cost, self.budget)
+            if not batch:
+                if not any(s.batch for s in self.slots):
+                    raise RuntimeError("a single request does not fit the HBM budget")
+                self.deferred += 1
+                break
+            self.budget.reserve(nbytes)
+            slot.reserved = nbytes
+            t = time.perf_counter()
+            for req in batch:
+                req.t_launch = t
+            self._launch(slot, batch, sum(self._pairs(r) for r in batch))
+            self.batches += 1
+        return sum(len(s.batch) for s in self.slots)
+
+    def drain(self):
+        while self.queue or any(s.batch for s in self.slots):
+            if not self.poll():
+                continue
+            for slot in self.slots:
+                if slot.batch:
+                    slot.done.synchronize()
+                    break

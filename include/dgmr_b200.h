@@ -169,7 +169,7 @@ typedef struct dgmr_batch_view {
     int32_t reserved;
     dgmr_camera camera;
     float* framebuffer; /* [3,H,W] device, written by the forward */
-    const float* grad_framebuffer; /* [3,H,W] device, read by the backward */
+    const float* grad_framebuffer; /* [3,H,W] device, read by the backward; NULL = no gradient for this view */
 } dgmr_batch_view;
 
 typedef struct dgmr_scene_grads { /* device outputs of the batched backward, per scene */
@@ -193,8 +193,12 @@ dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes,
     size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
 
 /* Backward of the last batched forward run in these workspaces.  Gradients of
- * every scene are written (not accumulated): the sum over that scene's views,
- * added in view order. */
+ * every scene entry are written (not accumulated): the sum over that entry's
+ * views, added in view order.  A view with grad_framebuffer == NULL takes no
+ * part (its tiles are skipped), and a scene entry whose grads[s].sh is NULL
+ * gets no gradient -- so one batch can mix plain renders with gradient
+ * requests.  The same scene tensors may appear in several entries (one per
+ * gradient request) to keep their gradients apart. */
 dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
     const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
     int64_t pair_capacity, dgmr_stream stream);
