@@ -58,9 +58,10 @@ def parse():
     ap.add_argument("--slots", type=int, default=3, help="requests in flight")
     ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["served", "batched", "marcher"], default="served",
+    ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving"], default="served",
                     help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
-                         "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512")
+                         "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512; "
+                         "serving: 8 scenes, Poisson 200 req/s, mixed resolutions, 20%% gradient requests")
     return ap.parse_args()
 
 
@@ -517,6 +518,147 @@ def run_marcher(args):
     return 0
 
 
+def run_serving(args):
+    """8 resident scenes (100k-3M Gaussians, log-uniform), a Poisson request
+    stream at 200 req/s, resolutions drawn from 256^2 / 512^2 / 1280x720 /
+    1920x1080, 20 % of requests also asking for the gradient against an N(0,1)
+    image gradient.  The continuous-batching server against a serial server
+    that makes the plain per-request calls (preprocess, pair count read back,
+    render, backward) on the same arrival times."""
+    torch, dev, local = _gpu_common()
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200 import splat
+    from differentiable_gaussian_mixture_renderer_b200.serving import ContinuousServer, GaussianScene, ServeRequest
+    rng = np.random.default_rng(7)
+    counts = np.exp(rng.uniform(np.log(1e5), np.log(3e6), size=8)).astype(int)
+    scenes = {f"s{i}": GaussianScene.from_numpy(S.make_scene(int(n), seed=20 + i), dev) for i, n in enumerate(counts)}
+    res = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+    n_req = max(args.steps, 1) * 40
+    rate = 200.0
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    gen = torch.Generator(device=dev).manual_seed(3)
+
+    def make_requests():
+        out = []
+        r2 = np.random.default_rng(11)
+        for k in range(n_req):
+            sid = f"s{int(r2.integers(8))}"
+            w, h = res[int(r2.integers(4))]
+            cam = S.random_cameras(1, w, h, seed=1000 + k)[0]
+            bwd = bool(r2.uniform() < 0.2)
+            g = torch.randn((3, h, w), device=dev, generator=gen) if bwd else None
+            req = ServeRequest(sid, cam, backward=bwd, grad_image=g, arrival=float(arrivals[k]))
+            # the client owns its output buffers (a pool in a real deployment): no allocation in the loop
+            req.image = torch.empty((3, h, w), dtype=torch.float32, device=dev)
+            if bwd:
+                sc = scenes[sid]
+                req.grads = tuple(torch.empty_like(t) for t in (sc.shs, sc.weights, sc.centroids, sc.scales,
+                                                                 sc.rotations))
+            out.append(req)
+        return out
+
+    server = ContinuousServer(scenes, dev, n_slots=4, max_batch=8)
+    # warm-up: one pass over a request set of the same distribution (other cameras) learns every
+    # (scene, resolution) pair capacity and grows the slots' workspaces to their steady size
+    warm = make_requests()
+    rw = np.random.default_rng(5)
+    for r in warm:
+        r.camera = S.random_cameras(1, r.camera.width, r.camera.height, seed=int(rw.integers(1 << 30)))[0]
+    for _ in range(max(args.warmup, 1)):
+        for r in warm:
+            server.submit(r)
+        server.drain()
+    server.completed.clear()
+    del warm
+
+    def serve(reqs, poisson: bool):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(reqs) or server.queue or any(sl.batch for sl in server.slots):
+            now = time.perf_counter() - t0
+            while i < len(reqs) and (not poisson or reqs[i].arrival <= now):
+                reqs[i].arrival = reqs[i].arrival if poisson else 0.0
+                server.submit(reqs[i])
+                i += 1
+            server.poll()
+        torch.cuda.synchronize(dev)
+        lat = [(r.t_done - t0 - r.arrival) * 1e3 for r in reqs]
+        span = max(r.t_done for r in reqs) - t0
+        return len(reqs) / span, lat
+
+    def batch_log():
+        lg = server.log
+        server.log = []
+        if not lg:
+            return {}
+        inflight = [x[3] * 1e3 for x in lg]
+        gpu = [x[4] for x in lg]
+        worst = sorted(lg, key=lambda x: -x[3])[:3]
+        return {"batches": len(lg), "mean_requests": float(np.mean([x[0] for x in lg])),
+                "gpu_ms_p50": pct(gpu, 50), "gpu_ms_p99": pct(gpu, 99),
+                "worst": [{"requests": x[0], "in_flight_ms": x[3] * 1e3, "gpu_ms": x[4], "gradient": x[5],
+                           "rerendered": x[6]} for x in worst],
+                "pairs_over_capacity_max": float(max(x[2] / max(x[1], 1) for x in lg)),
+                "capacity_over_pairs_mean": float(np.mean([x[1] / max(x[2], 1) for x in lg])),
+                "in_flight_ms_p50": pct(inflight, 50), "in_flight_ms_p99": pct(inflight, 99)}
+
+    server.log = []
+    with ClockSampler(local) as clk:
+        reqs = make_requests()
+        r0, a0 = server.rerenders, server.reallocs
+        thr_poisson, lat_poisson = serve(reqs, True)
+        batch_sizes = [r.batch_size for r in reqs]
+        log_poisson = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+        reqs = make_requests()
+        r0, a0 = server.rerenders, server.reallocs
+        thr_sat, lat_sat = serve(reqs, False)
+        log_sat = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+    # plain per-request calls, one at a time, on the same arrival times
+    reqs = make_requests()
+    t_free = 0.0
+    lat_plain, service = [], []
+    for r in reqs:
+        sc = scenes[r.scene_id]
+        cam = r.camera
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        fb, frame = splat.splat_forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, cam.view, cam.proj,
+                                        cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
+                                        cam.tan_fovy, sc.sh_degree)
+        if r.backward:
+            splat.splat_backward(frame, r.grad_image, sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t
+        service.append(dt)
+        start = max(r.arrival, t_free)
+        t_free = start + dt
+        lat_plain.append((t_free - r.arrival) * 1e3)
+        del fb, frame
+    plain_thr = len(reqs) / sum(service)
+    line = {"metric": "served requests/s + p50/p99 ms, continuous batching, 8 scenes, Poisson 200 req/s",
+            "value": thr_sat, "unit": "requests/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * n_req / thr_sat / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "8 scenes (100k-3M Gaussians, log-uniform, config-0 distribution), random cameras "
+                                   "r=2.5-4, resolutions from 256x256 / 512x512 / 1280x720 / 1920x1080, 20% gradient "
+                                   "requests (N(0,1) image gradient)", "scene_gaussians": [int(n) for n in counts],
+                       "requests": n_req, "slots": 4, "max_batch": 8},
+            "saturation": {"requests_per_s": thr_sat, "p50_ms": pct(lat_sat, 50), "p99_ms": pct(lat_sat, 99),
+                           "note": "all requests queued at t=0", "batches": log_sat},
+            "poisson_200": {"requests_per_s": thr_poisson, "p50_ms": pct(lat_poisson, 50),
+                            "p99_ms": pct(lat_poisson, 99), "mean_batch": float(np.mean(batch_sizes)),
+                            "batches": log_poisson},
+            "plain_per_request": {"requests_per_s": plain_thr, "p50_ms": pct(lat_plain, 50),
+                                  "p99_ms": pct(lat_plain, 99),
+                                  "note": "serial per-request calls on the same Poisson arrivals"},
+            "served_over_plain": thr_sat / plain_thr, "rerenders": server.rerenders,
+            "hbm_budget_gb": server.budget.budget / 1e9, "hbm_peak_gb": server.budget.peak / 1e9,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -525,6 +667,8 @@ def main():
         return run_batched(args)
     if args.workload == "marcher":
         return run_marcher(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

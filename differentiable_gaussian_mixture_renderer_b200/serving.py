@@ -308,13 +308,14 @@ class _BatchSlot:
     tables: tuple = ()
     capacity: int = 0
     reserved: int = 0
+    start: torch.cuda.Event | None = None
 
 
 class ContinuousServer:
     """Continuous batching of render and gradient requests over resident scenes."""
 
     def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
-                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.15):
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3):
         self.device = torch.device(device or "cuda")
         self.scenes = scenes
         self.lib = N.lib()
@@ -328,9 +329,12 @@ class ContinuousServer:
         self.queue: list = []
         self.completed: list = []
         self.capacity: dict = {}  # (scene_id, W, H) -> pairs
+        self._unit_cost: dict = {}  # (scene_id, W, H, backward) -> bytes of a one-request batch
         self.rerenders = 0
         self.batches = 0
         self.deferred = 0  # times the queue head waited for memory held by batches in flight
+        self.reallocs = 0  # workspace growths (each one a fresh device allocation)
+        self.log: list = []  # per completed batch: (requests, capacity, pairs, host seconds in flight)
 
     # ------------------------------------------------------------ sizing
     def _pairs(self, req) -> int:
@@ -362,7 +366,7 @@ class ContinuousServer:
         scenes = (N.Scene * len(entries))(*entries)
         return scenes, views, scene_of_entry
 
-    def _cost(self, batch) -> int:
+    def _exact_cost(self, batch) -> int:
         scenes, views, _ = self._tables(batch)
         cap = sum(self._pairs(r) for r in batch)
         fb, pb = C.c_size_t(0), C.c_size_t(0)
@@ -371,6 +375,20 @@ class ContinuousServer:
         out = sum(12 * r.camera.width * r.camera.height for r in batch)
         grads = sum(self.scenes[r.scene_id].nbytes() for r in batch if r.backward)
         return int(fb.value) + int(pb.value) + out + grads
+
+    def _cost(self, batch) -> int:
+        """HBM a batch holds: the sum of its requests' one-request costs (every
+        workspace part is linear in the views' slots, tiles, pixels and pairs;
+        the per-request sum over-counts only the alignment padding)."""
+        total = 0
+        for r in batch:
+            key = (r.scene_id, r.camera.width, r.camera.height, r.backward)
+            c = self._unit_cost.get(key)
+            if c is None:
+                c = self._exact_cost([r])
+                self._unit_cost[key] = c
+            total += c
+        return total
 
     # ------------------------------------------------------------ running
     def submit(self, req: ServeRequest) -> ServeRequest:
@@ -405,14 +423,20 @@ class ContinuousServer:
         N.check(self.lib.dgmr_splat_batch_workspace_size(scenes, len(scenes), views, len(views), capacity, C.byref(fb),
                                                          C.byref(pb)), "batch workspace size")
         if slot.frame_ws is None or slot.frame_ws.numel() < fb.value:
-            slot.frame_ws = torch.empty(max(1, fb.value), dtype=torch.uint8, device=dev)
+            slot.frame_ws = None
+            slot.frame_ws = torch.empty(max(1, int(fb.value * 1.25)), dtype=torch.uint8, device=dev)
+            self.reallocs += 1
         if slot.pair_ws is None or slot.pair_ws.numel() < pb.value:
-            slot.pair_ws = torch.empty(max(1, pb.value), dtype=torch.uint8, device=dev)
+            slot.pair_ws = None
+            slot.pair_ws = torch.empty(max(1, int(pb.value * 1.25)), dtype=torch.uint8, device=dev)
+            self.reallocs += 1
         if slot.stats is None:
             slot.stats = torch.zeros(4, dtype=torch.int32, device=dev)
             slot.stats_host = torch.zeros(4, dtype=torch.int32, pin_memory=True)
         s = slot.stream
         with torch.cuda.stream(s):
+            slot.start = torch.cuda.Event(enable_timing=True)
+            slot.start.record(s)
             N.check(self.lib.dgmr_splat_batch_forward(scenes, len(scenes), views, len(views), N.ptr(slot.frame_ws),
                                                       slot.frame_ws.numel(), N.ptr(slot.pair_ws), slot.pair_ws.numel(),
                                                       capacity, N.ptr(slot.stats), s.cuda_stream), "batch forward")
@@ -423,7 +447,7 @@ class ContinuousServer:
                                                            N.ptr(slot.frame_ws), slot.frame_ws.numel(),
                                                            N.ptr(slot.pair_ws), slot.pair_ws.numel(), capacity,
                                                            s.cuda_stream), "batch backward")
-            slot.done = torch.cuda.Event()
+            slot.done = torch.cuda.Event(enable_timing=True)
             slot.done.record(s)
         slot.batch = batch
         slot.tables = (scenes, views, grads)
@@ -432,15 +456,21 @@ class ContinuousServer:
     def _complete(self, slot: _BatchSlot, now: float):
         n_pairs, flags = int(slot.stats_host[0]), int(slot.stats_host[1])
         if flags & N.FLAG_PAIR_OVERFLOW:
-            # more pairs than the learnt capacities: grow them and render the batch again, exactly sized
+            # more pairs than the learnt capacities: grow them and render the batch again with the
+            # exact count, asynchronously -- the slot stays busy and completes on a later poll
             self.rerenders += 1
+            grow = n_pairs / max(slot.capacity, 1)
             for req in slot.batch:
                 key = (req.scene_id, req.camera.width, req.camera.height)
-                self.capacity[key] = int(math.ceil(self.capacity[key] * max(self.margin, n_pairs / slot.capacity)))
+                self.capacity[key] = int(math.ceil(self.capacity[key] * max(self.margin, grow)))
+                self._unit_cost.pop((*key, False), None)
+                self._unit_cost.pop((*key, True), None)
                 req.rerendered = True
-            self._launch(slot, slot.batch, int(math.ceil(n_pairs * self.margin)) + 1024)
-            slot.done.synchronize()
-            now = time.perf_counter()
+            self._launch(slot, slot.batch, n_pairs + 1024)
+            return
+        self.log.append((len(slot.batch), slot.capacity, n_pairs, now - slot.batch[0].t_launch,
+                         slot.start.elapsed_time(slot.done), any(r.backward for r in slot.batch),
+                         slot.batch[0].rerendered))
         for req in slot.batch:
             req.t_done = now
             req.batch_size = len(slot.batch)
