@@ -123,7 +123,9 @@ def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matr
         c = N.VmCache(*[N.ptr(t) if (t is not None and t.numel() > 0) else None for t in cache])
         if c.b_point_list is None:
             c.b_point_list = N.ptr(cache[9])  # never read: the tile ranges are all empty
-        ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, 0, N.dtype_code(dt)), dtype=torch.uint8, device=dev)
+        # sized with the frame's pair count: the march uses the room for its per-ray Gaussian masks
+        n_pairs = int(cache[11].numel()) if cache[11] is not None else 0
+        ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, n_pairs, N.dtype_code(dt)), dtype=torch.uint8, device=dev)
         N.check(lib.dgmr_vm_backward(scene, cam, c, N.ptr(grad_framebuffer), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
                                      N.ptr(g_s), N.ptr(g_q), N.ptr(ws), ws.numel(), None, N.stream_handle()),
                 "vol_marcher backward")

@@ -59,6 +59,25 @@ inline VmLayout<T> vm_layout(uint32_t N, uint32_t cap, void* base)
     return L;
 }
 
+// Words of the per-ray Gaussian masks for a frame with cap pairs and n_tiles
+// tiles (see k_vm_march): one 64-bit mask per (pixel, 64-Gaussian batch of
+// its tile list).  Batch slots of tile t start at b_t / 64 + t, which never
+// overlap between tiles, so cap / 64 + n_tiles + 1 slots are enough.
+inline size_t vm_ray_mask_words(uint32_t cap, uint32_t n_tiles);
+
+// Any workspace beyond the layout's bytes holds the ray masks.
+inline void vm_ray_masks(void* base, size_t layout_bytes, size_t workspace_bytes, uint32_t** masks, size_t* words)
+{
+    const size_t off = align_up(layout_bytes);
+    if (!base || workspace_bytes <= off) {
+        *masks = nullptr;
+        *words = 0;
+        return;
+    }
+    *masks = reinterpret_cast<uint32_t*>(static_cast<char*>(base) + off);
+    *words = (workspace_bytes - off) / sizeof(uint32_t);
+}
+
 // depth keys (float bits of the cached depth) and the identity permutation
 template <class T>
 __global__ void k_depth_keys(const T* __restrict__ depths, uint32_t N, uint32_t* __restrict__ depth_key, uint32_t* __restrict__ perm)
@@ -205,6 +224,8 @@ struct VmMarch {
     T* acc; // backward only: [N,10]
     T* g_centroids; // backward only: [N,3]
     uint32_t* stats;
+    uint32_t* ray_masks; // per-ray Gaussian masks (may be null)
+    size_t ray_mask_words;
     ConstSamplesT<T> cs;
 };
 
@@ -215,6 +236,52 @@ struct VmMarch {
 constexpr unsigned kMarchThreads = 64;
 constexpr unsigned kMarchRows = kMarchThreads / kTile;
 constexpr unsigned kMarchParts = kTile / kMarchRows;
+
+inline size_t vm_ray_mask_words(uint32_t cap, uint32_t n_tiles)
+{
+    return (size_t(cap) / kMarchThreads + n_tiles + 1) * kMarchParts * 2 * kMarchThreads;
+}
+
+// Which Gaussians of the tile list a ray can use.  Both passes of every large
+// step only act on a Gaussian that passes its gate -- pass 1's (mass on the
+// ray in (1/255, 1000], positive variance, finite centre) or pass 2's
+// (gaussian_on_ray) -- and the gates depend on the ray alone, not on the
+// step.  So the first pass over the tile records, per pixel and per batch of
+// 64 list entries, a 64-bit mask of the entries that pass either gate, and the
+// large steps only intersect those.  Pass 1's depth break also only needs
+// them: the list is in depth order, so the first entry with depth > end of
+// the section set that is skipped here would be followed by a masked entry
+// with a depth at least as large, checked against the same end.  The results
+// are identical; the per-step cost drops from the tile's list to the ray's
+// own Gaussians.
+template <class T>
+__device__ __forceinline__ bool ray_can_use(const Gauss1d<T>& g, T mass)
+{
+    const T mor = g.weight * mass;
+    const bool pass1 = !(mor <= T(1.0f / 255.f) || mor > T(1000)) && !(g.C <= T(0)) && !dgmr_fm::isnan_f(g.centre);
+    T sd, mor2;
+    const bool pass2 = gaussian_on_ray(g, mass, &sd, &mor2);
+    return pass1 || pass2;
+}
+
+// the ray's masks of one block: batch i, word w at m[i * kMarchParts * 2 * kMarchThreads + w * kMarchThreads + tid]
+struct RayMasks {
+    uint32_t* m;
+    __device__ __forceinline__ uint64_t get(int i) const
+    {
+        if (!m)
+            return ~0ull;
+        const size_t o = size_t(i) * kMarchParts * 2 * kMarchThreads + threadIdx.x;
+        return uint64_t(m[o]) | (uint64_t(m[o + kMarchThreads]) << 32);
+    }
+    __device__ __forceinline__ void put(int i, uint64_t bits) const
+    {
+        const size_t o = size_t(i) * kMarchParts * 2 * kMarchThreads + threadIdx.x;
+        m[o] = uint32_t(bits);
+        m[o + kMarchThreads] = uint32_t(bits >> 32);
+    }
+};
+
 
 template <class T>
 struct MarchShared {
@@ -253,9 +320,33 @@ __device__ __forceinline__ S3<T> shared_Q(const MarchShared<T>& sh, int j)
 
 // Pass 1 of a large step: sample sections from the Gaussians on the ray
 // (vol_marcher_forward.cu:351-403), block-synchronous over batches.
+__device__ __forceinline__ uint64_t batch_bits(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
+
+// first pass over the tile: the ray masks (see RayMasks)
+template <class T>
+__device__ __forceinline__ void build_ray_masks(const RayMasks& rm, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool inside, V3<T> o,
+    V3<T> d)
+{
+    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
+        __syncthreads();
+        load_batch(sh, a, base + int32_t(threadIdx.x), e);
+        __syncthreads();
+        const int n = min(int(kMarchThreads), e - base);
+        uint64_t m = 0;
+        if (inside)
+            for (int j = 0; j < n; ++j) {
+                const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
+                if (ray_can_use(intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d), sh.mass[j]))
+                    m |= 1ull << j;
+            }
+        rm.put((base - b) / int32_t(kMarchThreads), m);
+    }
+    __syncthreads();
+}
+
 template <class T>
 __device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done,
-    V3<T> o, V3<T> d)
+    V3<T> o, V3<T> d, const RayMasks& rm)
 {
     if (a.cs.n > 0) {
         if (!done)
@@ -272,7 +363,10 @@ __device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec
         if (done1)
             continue;
         const int n = min(int(kMarchThreads), e - base);
-        for (int j = 0; j < n; ++j) {
+        uint64_t m = rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n);
+        while (m) {
+            const int j = __ffsll((long long)m) - 1;
+            m &= m - 1ull;
             const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
             const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
             const T sd = dgmr_fm::sqrt_f(g.C);
@@ -298,7 +392,7 @@ __device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec
 // Pass 2: CDF-difference bin masses of every Gaussian in the tile list
 template <class T>
 __device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done, V3<T> o,
-    V3<T> d)
+    V3<T> d, const RayMasks& rm)
 {
     for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
         if (__syncthreads_count(done) == int(kMarchThreads))
@@ -308,12 +402,29 @@ __device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchS
         if (done)
             continue;
         const int n = min(int(kMarchThreads), e - base);
-        for (int j = 0; j < n; ++j) {
+        uint64_t m = rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n);
+        while (m) {
+            const int j = __ffsll((long long)m) - 1;
+            m &= m - 1ull;
             const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
             const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
             sample_gaussian(g, sh.mass[j], V3<T> { sh.rgb[0][j], sh.rgb[1][j], sh.rgb[2][j] }, borders, bins);
         }
     }
+}
+
+// this block's ray masks, or none (every entry used) if the workspace has no room for them
+template <class T>
+__device__ __forceinline__ RayMasks block_masks(const VmMarch<T>& a, unsigned tile, unsigned part, int32_t b, int32_t e)
+{
+    RayMasks rm { nullptr };
+    if (!a.ray_masks || e <= b || b < 0)
+        return rm;
+    const size_t n_batches = size_t(e - b + int32_t(kMarchThreads) - 1) / kMarchThreads;
+    const size_t slot = size_t(uint32_t(b) / kMarchThreads) + tile;
+    if ((slot + n_batches) * kMarchParts * 2 * kMarchThreads <= a.ray_mask_words)
+        rm.m = a.ray_masks + (slot * kMarchParts + part) * 2 * kMarchThreads;
+    return rm;
 }
 
 template <class T>
@@ -327,6 +438,9 @@ __global__ void __launch_bounds__(kMarchThreads) k_vm_march(VmMarch<T> a, Camera
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
     const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    const RayMasks rm = block_masks(a, tile, part, b, e);
+    if (rm.m)
+        build_ray_masks(rm, sh, a, b, e, inside, o, d);
     bool done = !inside;
     V3<T> colour = { T(0), T(0), T(0) };
     T tr = T(1);
@@ -343,11 +457,11 @@ __global__ void __launch_bounds__(kMarchThreads) k_vm_march(VmMarch<T> a, Camera
             break;
         }
         sec.reset(start);
-        collect_sections(sec, sh, a, b, e, done, o, d);
+        collect_sections(sec, sh, a, b, e, done, o, d, rm);
         sample_positions(sec, borders);
         for (unsigned k = 0; k < kBins; ++k)
             bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
-        fill_bins(bins, borders, sh, a, b, e, done, o, d);
+        fill_bins(bins, borders, sh, a, b, e, done, o, d, rm);
         if (!done) {
             integrate_bins(colour, tr, bins);
             done = sec.n == 0 || tr < T(1.f / 255.f);
@@ -387,6 +501,9 @@ __global__ void __launch_bounds__(kMarchThreads) k_vm_march_bwd(VmMarch<T> a, Ca
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
     const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    const RayMasks rm = block_masks(a, tile, part, b, e);
+    if (rm.m)
+        build_ray_masks(rm, sh, a, b, e, inside, o, d);
     const size_t pix = size_t(py) * cam.W + px;
     const size_t plane = size_t(cam.W) * cam.H;
     bool done = !inside;
@@ -415,11 +532,11 @@ __global__ void __launch_bounds__(kMarchThreads) k_vm_march_bwd(VmMarch<T> a, Ca
             break;
         }
         sec.reset(start);
-        collect_sections(sec, sh, a, b, e, done, o, d);
+        collect_sections(sec, sh, a, b, e, done, o, d, rm);
         sample_positions(sec, borders);
         for (unsigned k = 0; k < kBins; ++k)
             bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
-        fill_bins(bins, borders, sh, a, b, e, done, o, d);
+        fill_bins(bins, borders, sh, a, b, e, done, o, d, rm);
         if (!done)
             grad_integrate_bins(colour, tr, final_T, bins, gc, gt, gbins);
         // pass 3: adjoint of the bin masses, per Gaussian
@@ -429,13 +546,18 @@ __global__ void __launch_bounds__(kMarchThreads) k_vm_march_bwd(VmMarch<T> a, Ca
             load_batch(sh, a, base + int32_t(threadIdx.x), e);
             __syncthreads();
             const int n = min(int(kMarchThreads), e - base);
-            for (int j = 0; j < n; ++j) {
+            const uint64_t mine = done ? 0ull : (rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n));
+            uint64_t todo = uint64_t(__reduce_or_sync(0xffffffffu, uint32_t(mine)))
+                | (uint64_t(__reduce_or_sync(0xffffffffu, uint32_t(mine >> 32))) << 32);
+            while (todo) {
+                const int j = __ffsll((long long)todo) - 1;
+                todo &= todo - 1ull;
                 T v[10];
                 V3<T> gmu = { T(0), T(0), T(0) };
 #pragma unroll
                 for (int q = 0; q < 10; ++q)
                     v[q] = T(0);
-                if (!done) {
+                if ((mine >> j) & 1ull) {
                     const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
                     V3<T> grgb = { T(0), T(0), T(0) };
                     S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
@@ -644,6 +766,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.remaining_T = static_cast<T*>(c->remaining_transparency);
     a.stats = st_dev;
     a.cs = const_samples<T>();
+    vm_ray_masks(workspace, L.bytes, workspace_bytes, &a.ray_masks, &a.ray_mask_words);
     k_vm_march<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
     note_launch();
     return launch_status();
@@ -678,6 +801,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     a.g_centroids = static_cast<T*>(g_centroids);
     a.stats = st_dev;
     a.cs = const_samples<T>();
+    vm_ray_masks(workspace, L.bytes, workspace_bytes, &a.ray_masks, &a.ray_mask_words);
     k_vm_march_bwd<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
     VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
@@ -704,9 +828,11 @@ size_t dgmr_vm_workspace_size(int32_t n_gaussians, int32_t width, int32_t height
 {
     if (n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
         return 0;
+    const uint32_t n_tiles = ((uint32_t(width) + kTile - 1) / kTile) * ((uint32_t(height) + kTile - 1) / kTile);
+    const size_t masks = vm_ray_mask_words(uint32_t(pair_capacity), n_tiles) * sizeof(uint32_t);
     if (dtype == DGMR_F64)
-        return vm_layout<double>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes;
-    return vm_layout<float>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes;
+        return align_up(vm_layout<double>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;
+    return align_up(vm_layout<float>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;
 }
 
 dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, void* workspace, size_t workspace_bytes,
