@@ -1,0 +1,452 @@
+// Volume march with one warp per ray (included by dgmr_marcher.cu).
+//
+// A ray's work is mostly its pass 2: for every Gaussian it can use, 127
+// CDF differences -- and the heaviest rays of a frame set its duration.  With
+// one thread per ray that work is a long dependent chain on one lane (with
+// the 127 bins in local memory), so the kernel ends up waiting on a few
+// rays while the SMs idle.  Here the 32 lanes of a warp share one ray:
+//  * the tile list is walked 32 entries at a time, one entry per lane
+//    (intersection with the ray, gates), results exchanged by shuffles;
+//  * lane l owns bins l, l+32, l+64, l+96 (four register bins); for each
+//    Gaussian, in list order, every lane evaluates the CDF at its own
+//    borders and takes the next border's value from its neighbour;
+//  * the strictly sequential parts -- section insertion (pass 1), sample
+//    positions, the blend and its adjoint peel -- run on every lane in
+//    lockstep from shared values, so no lane waits on another.
+// Per bin, Gaussian order and every arithmetic operation are those of the
+// one-thread loops (vol_marcher_forward.cu:295-501, math.h:412-468), so the
+// image is the same bits.  Warps are independent (no block barrier); blocks
+// of kRayWarps rays are launched heaviest tile first.
+#pragma once
+
+namespace dgmr {
+
+constexpr unsigned kRayWarps = 4; // rays per block
+constexpr unsigned kRayRounds = 4; // 4 x 32 lanes >= 128 borders
+constexpr unsigned kRayMaskRegs = 4; // ray masks kept in registers: 4 x 32 batches of 32 entries
+
+template <class T>
+struct RayWarpShared {
+    T borders[kSmallSteps];
+    Bin<T> bins[kSmallSteps]; // forward: (r, g, b, exp(-mass)); backward: (r, g, b, mass)
+};
+
+template <class T>
+struct RayWarpSharedBwd {
+    T borders[kSmallSteps];
+    Bin<T> bins[kSmallSteps];
+    Bin<T> gbins[kSmallSteps]; // bin adjoints
+};
+
+// The gates of both passes (see ray_can_use) as a 32-bit mask per batch of 32
+// list entries, held in registers: lane l keeps the masks of batches l, l+32,
+// l+64, l+96.  Batches past that get every entry (the gates are re-checked).
+struct WarpRayMasks {
+    uint32_t r[kRayMaskRegs];
+    __device__ __forceinline__ uint32_t get(unsigned i) const
+    {
+        if (i >= 32 * kRayMaskRegs)
+            return 0xffffffffu;
+        const unsigned q = i >> 5;
+        uint32_t v = r[0];
+#pragma unroll
+        for (unsigned k = 1; k < kRayMaskRegs; ++k)
+            if (q == k)
+                v = r[k];
+        return __shfl_sync(0xffffffffu, v, int(i & 31u));
+    }
+    __device__ __forceinline__ void set(unsigned i, uint32_t m, unsigned lane)
+    {
+        if (i >= 32 * kRayMaskRegs || (i & 31u) != lane)
+            return;
+#pragma unroll
+        for (unsigned k = 0; k < kRayMaskRegs; ++k)
+            if ((i >> 5) == k)
+                r[k] = m;
+    }
+};
+
+__device__ __forceinline__ uint32_t lanes_below(int n) { return n >= 32 ? 0xffffffffu : ((1u << n) - 1u); }
+
+// One list entry as seen by its lane.
+template <class T>
+struct RayEntry {
+    uint32_t id;
+    V3<T> mu;
+    S3<T> Q;
+    T mass;
+};
+
+template <class T>
+__device__ __forceinline__ RayEntry<T> load_entry(const VmMarch<T>& a, int32_t k)
+{
+    RayEntry<T> en;
+    en.id = uint32_t(a.list[k]);
+    const size_t id = en.id;
+    en.mu = { a.centroids[3 * id], a.centroids[3 * id + 1], a.centroids[3 * id + 2] };
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        en.Q.v[c] = a.inv_cov[6 * id + c];
+    en.mass = a.masses[id];
+    return en;
+}
+
+// Tile work order for the march: heaviest tile first (k_tile_order), so the
+// longest rays start at the head of the grid.
+template <class T>
+__device__ __forceinline__ bool ray_pixel(const CameraT<T>& cam, const uint32_t* order, unsigned* tile, unsigned* px, unsigned* py)
+{
+    const unsigned groups = kTilePixels / kRayWarps;
+    const unsigned item = blockIdx.x / groups, group = blockIdx.x % groups;
+    *tile = order ? order[item] : item;
+    const unsigned p = group * kRayWarps + (threadIdx.x >> 5);
+    *px = (*tile % cam.gx) * kTile + (p % kTile);
+    *py = (*tile / cam.gx) * kTile + (p / kTile);
+    return *px < cam.W && *py < cam.H;
+}
+
+// pass 0: the ray's masks (one intersection per list entry, lane-parallel)
+template <class T>
+__device__ __forceinline__ WarpRayMasks warp_ray_masks(const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d, unsigned lane)
+{
+    WarpRayMasks rm;
+#pragma unroll
+    for (unsigned k = 0; k < kRayMaskRegs; ++k)
+        rm.r[k] = 0u;
+    unsigned i = 0;
+    for (int32_t base = b; base < e && i < 32 * kRayMaskRegs; base += 32, ++i) {
+        const int32_t k = base + int32_t(lane);
+        bool can = false;
+        if (k < e) {
+            const RayEntry<T> en = load_entry(a, k);
+            can = ray_can_use(intersect_with_ray_inv_C(en.mu, en.Q, o, d), en.mass);
+        }
+        rm.set(i, __ballot_sync(0xffffffffu, can), lane);
+    }
+    return rm;
+}
+
+} // namespace dgmr
+
+namespace dgmr {
+
+// Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
+// intersected lane-parallel, then walked in list order by every lane alike.
+template <class T>
+__device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
+    const WarpRayMasks& rm, unsigned lane)
+{
+    if (a.cs.n > 0) {
+        for (int i = 0; i < a.cs.n; ++i)
+            sec.put(Section<T> { a.cs.s[i][0], a.cs.s[i][1], a.cs.s[i][2] });
+        return;
+    }
+    unsigned i = 0;
+    for (int32_t base = b; base < e; base += 32, ++i) {
+        uint32_t m = rm.get(i) & lanes_below(e - base);
+        if (!m)
+            continue;
+        T depth = T(0), s0 = T(0), s1 = T(0), dt = T(0);
+        bool ok = false;
+        if ((m >> lane) & 1u) {
+            const RayEntry<T> en = load_entry(a, base + int32_t(lane));
+            const Gauss1d<T> g = intersect_with_ray_inv_C(en.mu, en.Q, o, d);
+            const T sd = dgmr_fm::sqrt_f(g.C);
+            depth = a.depths[en.id];
+            const T mor = g.weight * en.mass;
+            ok = !(mor <= T(1.0f / 255.f) || mor > T(1000)) && !(g.C <= T(0)) && !dgmr_fm::isnan_f(g.centre);
+            s0 = g.centre - sd * T(kRelevanceSigma);
+            s1 = g.centre + sd * T(kRelevanceSigma);
+            dt = ((sd * T(kRelevanceSigma)) * T(2)) / T(float(kStepsPerGaussian - 1));
+        }
+        const uint32_t okm = __ballot_sync(0xffffffffu, ok);
+        bool stop = false;
+        while (m) {
+            const int j = __ffs(int(m)) - 1;
+            m &= m - 1u;
+            const T dj = __shfl_sync(0xffffffffu, depth, j);
+            if (sec.hi < dj) {
+                stop = true;
+                break;
+            }
+            if (!((okm >> j) & 1u))
+                continue;
+            sec.put(Section<T> { __shfl_sync(0xffffffffu, s0, j), __shfl_sync(0xffffffffu, s1, j), __shfl_sync(0xffffffffu, dt, j) });
+        }
+        if (stop)
+            break;
+    }
+}
+
+// CDF differences of one Gaussian into the lane's bins 32 r + lane
+// (math.h:461-467).  Every lane evaluates the CDF at its own borders; the
+// right border of a bin is the next lane's left one.
+template <class T>
+__device__ __forceinline__ void warp_bins(Bin<T> (&acc)[kRayRounds], const T* borders, T centre, T inv_sd, T mor, V3<T> rgb, unsigned lane)
+{
+    T cs[kRayRounds];
+#pragma unroll
+    for (unsigned r = 0; r < kRayRounds; ++r) {
+        const unsigned k = 32 * r + lane;
+        cs[r] = (k <= kBins) ? cdf_inv_SD(centre, inv_sd, borders[k]) : T(0);
+    }
+#pragma unroll
+    for (unsigned r = 0; r < kRayRounds; ++r) {
+        T ce = __shfl_down_sync(0xffffffffu, cs[r], 1);
+        const T next = (r + 1 < kRayRounds) ? __shfl_sync(0xffffffffu, cs[(r + 1 < kRayRounds) ? r + 1 : r], 0) : T(0);
+        if (lane == 31)
+            ce = next;
+        const unsigned k = 32 * r + lane;
+        if (k < kBins) {
+            const T m = max_f(T(0), (ce - cs[r]) * mor);
+            if (!(m < T(0.00001f))) {
+                acc[r].r = acc[r].r + rgb.x * m;
+                acc[r].g = acc[r].g + rgb.y * m;
+                acc[r].b = acc[r].b + rgb.z * m;
+                acc[r].m = acc[r].m + m;
+            }
+        }
+    }
+}
+
+// The 1-D Gaussian of a masked entry if it reaches the bins (the early-outs of
+// math.h:442-459); the same test in the forward and backward.
+template <class T>
+__device__ __forceinline__ bool warp_entry_on_bins(const RayEntry<T>& en, V3<T> o, V3<T> d, const T* borders, Gauss1d<T>* g_out, T* sd_out, T* inv_sd_out,
+    T* mor_out)
+{
+    const Gauss1d<T> g = intersect_with_ray_inv_C(en.mu, en.Q, o, d);
+    T sd, mor;
+    if (!gaussian_on_ray(g, en.mass, &sd, &mor))
+        return false;
+    const T inv_sd = T(1) / sd;
+    const T mib = mor * (cdf_inv_SD(g.centre, inv_sd, borders[kBins]) - cdf_inv_SD(g.centre, inv_sd, borders[0]));
+    if (mib < T(0.0001f))
+        return false;
+    *g_out = g;
+    *sd_out = sd;
+    *inv_sd_out = inv_sd;
+    *mor_out = mor;
+    return true;
+}
+
+// Pass 2 (vol_marcher_forward.cu:405-437): Gaussians in list order, bins spread over the lanes
+template <class T>
+__device__ __forceinline__ void warp_fill(Bin<T> (&acc)[kRayRounds], const T* borders, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
+    const WarpRayMasks& rm, unsigned lane)
+{
+#pragma unroll
+    for (unsigned r = 0; r < kRayRounds; ++r)
+        acc[r] = Bin<T> { T(0), T(0), T(0), T(0) };
+    unsigned i = 0;
+    for (int32_t base = b; base < e; base += 32, ++i) {
+        const uint32_t m = rm.get(i) & lanes_below(e - base);
+        if (!m)
+            continue;
+        T centre = T(0), inv_sd = T(0), mor = T(0);
+        V3<T> rgb = { T(0), T(0), T(0) };
+        bool ok = false;
+        if ((m >> lane) & 1u) {
+            const RayEntry<T> en = load_entry(a, base + int32_t(lane));
+            Gauss1d<T> g;
+            T sd;
+            ok = warp_entry_on_bins(en, o, d, borders, &g, &sd, &inv_sd, &mor);
+            if (ok) {
+                centre = g.centre;
+                rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
+            }
+        }
+        uint32_t okm = __ballot_sync(0xffffffffu, ok);
+        while (okm) {
+            const int j = __ffs(int(okm)) - 1;
+            okm &= okm - 1u;
+            const V3<T> c = { __shfl_sync(0xffffffffu, rgb.x, j), __shfl_sync(0xffffffffu, rgb.y, j), __shfl_sync(0xffffffffu, rgb.z, j) };
+            warp_bins(acc, borders, __shfl_sync(0xffffffffu, centre, j), __shfl_sync(0xffffffffu, inv_sd, j), __shfl_sync(0xffffffffu, mor, j), c, lane);
+        }
+    }
+}
+
+// bins to shared memory in order (.m = exp(-mass) for the blend, the mass itself for the peel)
+template <class T>
+__device__ __forceinline__ void warp_store_bins(Bin<T>* bins, const Bin<T> (&acc)[kRayRounds], unsigned lane, bool transmittance)
+{
+#pragma unroll
+    for (unsigned r = 0; r < kRayRounds; ++r) {
+        const unsigned k = 32 * r + lane;
+        if (k < kBins)
+            bins[k] = Bin<T> { acc[r].r, acc[r].g, acc[r].b, transmittance ? dgmr_fm::exp_f(-acc[r].m) : acc[r].m };
+    }
+    __syncwarp();
+}
+
+template <class T>
+__global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+{
+    __shared__ RayWarpShared<T> shared_rays[kRayWarps];
+    RayWarpShared<T>& sm = shared_rays[threadIdx.x >> 5];
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned tile, px, py;
+    if (!ray_pixel(cam, order, &tile, &px, &py))
+        return; // the whole warp: no block-level barrier below
+    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<T> d = pixel_dir(cam, px, py);
+    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    const WarpRayMasks rm = warp_ray_masks(a, b, e, o, d, lane);
+    V3<T> colour = { T(0), T(0), T(0) };
+    T tr = T(1);
+    T start = T(0);
+    SectionSet<kLargeSteps, T> sec;
+    for (unsigned step = 0;; ++step) {
+        if (step >= kMaxLargeSteps) {
+            if (lane == 0)
+                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
+            break;
+        }
+        sec.reset(start);
+        warp_collect(sec, a, b, e, o, d, rm, lane);
+        if (lane == 0)
+            sample_positions(sec, sm.borders);
+        __syncwarp();
+        Bin<T> acc[kRayRounds];
+        warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
+        warp_store_bins(sm.bins, acc, lane, true);
+        // math.h:412-428, identical on every lane
+        for (unsigned k = 0; k < kBins; ++k) {
+            const Bin<T> bk = sm.bins[k];
+            colour.x = colour.x + bk.r * tr;
+            colour.y = colour.y + bk.g * tr;
+            colour.z = colour.z + bk.b * tr;
+            tr = tr * bk.m;
+            if (tr < T(1. / 255.))
+                break;
+        }
+        const bool done = sec.n == 0 || tr < T(1.f / 255.f);
+        start = sm.borders[kSmallSteps - 1];
+        __syncwarp();
+        if (done)
+            break;
+    }
+    if (lane == 0) {
+        const size_t pix = size_t(py) * cam.W + px;
+        const size_t plane = size_t(cam.W) * cam.H;
+        a.fb[pix] = colour.x + tr * cam.bg[0];
+        a.fb[plane + pix] = colour.y + tr * cam.bg[1];
+        a.fb[2 * plane + pix] = colour.z + tr * cam.bg[2];
+        a.remaining_T[pix] = tr;
+    }
+}
+
+} // namespace dgmr
+
+namespace dgmr {
+
+// Pass 3 (grad/math.h:559-620): the ray's Gaussians of a batch are taken one
+// per lane, and each lane runs the whole adjoint of its Gaussian over the
+// bins in shared memory -- in bin order, so its sums round exactly as the
+// one-thread loop does -- then adds the result to the per-Gaussian
+// accumulators.
+template <class T>
+__device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
+    const WarpRayMasks& rm, unsigned lane)
+{
+    unsigned i = 0;
+    for (int32_t base = b; base < e; base += 32, ++i) {
+        const uint32_t m = rm.get(i) & lanes_below(e - base);
+        if (!((m >> lane) & 1u))
+            continue;
+        const RayEntry<T> en = load_entry(a, base + int32_t(lane));
+        const V3<T> rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
+        T g_mass = T(0);
+        V3<T> grgb = { T(0), T(0), T(0) }, gmu = { T(0), T(0), T(0) };
+        S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
+        grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ);
+        T* dst = a.acc + size_t(en.id) * 10;
+        const T v[10] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5] };
+#pragma unroll
+        for (int q = 0; q < 10; ++q)
+            if (v[q] != T(0))
+                atomicAdd(dst + q, v[q]);
+        T* gm = a.g_centroids + size_t(en.id) * 3;
+        if (gmu.x != T(0))
+            atomicAdd(gm, gmu.x);
+        if (gmu.y != T(0))
+            atomicAdd(gm + 1, gmu.y);
+        if (gmu.z != T(0))
+            atomicAdd(gm + 2, gmu.z);
+    }
+}
+
+// vol_marcher_backward.cu:115-319 with one warp per ray
+template <class T>
+__global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp_bwd(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+{
+    __shared__ RayWarpSharedBwd<T> shared_rays[kRayWarps];
+    RayWarpSharedBwd<T>& sm = shared_rays[threadIdx.x >> 5];
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned tile, px, py;
+    if (!ray_pixel(cam, order, &tile, &px, &py))
+        return;
+    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
+    const V3<T> d = pixel_dir(cam, px, py);
+    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
+    const WarpRayMasks rm = warp_ray_masks(a, b, e, o, d, lane);
+    const size_t pix = size_t(py) * cam.W + px;
+    const size_t plane = size_t(cam.W) * cam.H;
+    const T final_T = a.remaining_T[pix];
+    V3<T> colour = { a.fb[pix] - final_T * cam.bg[0], a.fb[plane + pix] - final_T * cam.bg[1], a.fb[2 * plane + pix] - final_T * cam.bg[2] };
+    const V3<T> gc = { a.grad_fb[pix], a.grad_fb[plane + pix], a.grad_fb[2 * plane + pix] };
+    const T gt = (gc.x * cam.bg[0] + gc.y * cam.bg[1]) + gc.z * cam.bg[2];
+    T tr = T(1);
+    T start = T(0);
+    SectionSet<kLargeSteps, T> sec;
+    for (unsigned step = 0;; ++step) {
+        if (step >= kMaxLargeSteps) {
+            if (lane == 0)
+                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
+            break;
+        }
+        sec.reset(start);
+        warp_collect(sec, a, b, e, o, d, rm, lane);
+        if (lane == 0)
+            sample_positions(sec, sm.borders);
+        __syncwarp();
+        Bin<T> acc[kRayRounds];
+        warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
+        warp_store_bins(sm.bins, acc, lane, false);
+        // grad/math.h:529-557, identical on every lane; lane 0 stores the bin adjoints
+        unsigned k = 0;
+        for (; k < kBins; ++k) {
+            const Bin<T> bk = sm.bins[k];
+            Bin<T> gb;
+            gb.r = tr * gc.x;
+            gb.g = tr * gc.y;
+            gb.b = tr * gc.z;
+            const T tk = dgmr_fm::exp_f(-bk.m);
+            const T inv_tk = min_f(T(255), T(1) / tk);
+            colour.x = (colour.x - bk.r) * inv_tk;
+            colour.y = (colour.y - bk.g) * inv_tk;
+            colour.z = (colour.z - bk.b) * inv_tk;
+            const T g_tk = (final_T * inv_tk) * gt + dot3(gc, colour) * tr;
+            gb.m = T(0) - g_tk * tk;
+            if (lane == 0)
+                sm.gbins[k] = gb;
+            tr = tr * tk;
+            if (tr < T(1. / 255.)) {
+                ++k;
+                break;
+            }
+        }
+        for (; k < kBins; ++k)
+            if (lane == 0)
+                sm.gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
+        __syncwarp();
+        warp_grad(sm.gbins, sm.borders, a, b, e, o, d, rm, lane);
+        const bool done = sec.n == 0 || tr < T(1.f / 255.f);
+        start = sm.borders[kSmallSteps - 1];
+        __syncwarp();
+        if (done)
+            break;
+    }
+}
+
+} // namespace dgmr

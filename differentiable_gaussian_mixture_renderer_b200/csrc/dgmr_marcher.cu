@@ -59,25 +59,6 @@ inline VmLayout<T> vm_layout(uint32_t N, uint32_t cap, void* base)
     return L;
 }
 
-// Words of the per-ray Gaussian masks for a frame with cap pairs and n_tiles
-// tiles (see k_vm_march): one 64-bit mask per (pixel, 64-Gaussian batch of
-// its tile list).  Batch slots of tile t start at b_t / 64 + t, which never
-// overlap between tiles, so cap / 64 + n_tiles + 1 slots are enough.
-inline size_t vm_ray_mask_words(uint32_t cap, uint32_t n_tiles);
-
-// Any workspace beyond the layout's bytes holds the ray masks.
-inline void vm_ray_masks(void* base, size_t layout_bytes, size_t workspace_bytes, uint32_t** masks, size_t* words)
-{
-    const size_t off = align_up(layout_bytes);
-    if (!base || workspace_bytes <= off) {
-        *masks = nullptr;
-        *words = 0;
-        return;
-    }
-    *masks = reinterpret_cast<uint32_t*>(static_cast<char*>(base) + off);
-    *words = (workspace_bytes - off) / sizeof(uint32_t);
-}
-
 // depth keys (float bits of the cached depth) and the identity permutation
 template <class T>
 __global__ void k_depth_keys(const T* __restrict__ depths, uint32_t N, uint32_t* __restrict__ depth_key, uint32_t* __restrict__ perm)
@@ -224,36 +205,20 @@ struct VmMarch {
     T* acc; // backward only: [N,10]
     T* g_centroids; // backward only: [N,3]
     uint32_t* stats;
-    uint32_t* ray_masks; // per-ray Gaussian masks (may be null)
-    size_t ray_mask_words;
     ConstSamplesT<T> cs;
 };
-
-// A march block covers kMarchRows pixel rows of one 16x16 tile (kMarchParts
-// blocks per tile).  Small blocks let the blocks of a heavy tile spread over
-// several SMs and retire independently; every block reads the tile's whole
-// Gaussian list in batches of kMarchThreads.
-constexpr unsigned kMarchThreads = 64;
-constexpr unsigned kMarchRows = kMarchThreads / kTile;
-constexpr unsigned kMarchParts = kTile / kMarchRows;
-
-inline size_t vm_ray_mask_words(uint32_t cap, uint32_t n_tiles)
-{
-    return (size_t(cap) / kMarchThreads + n_tiles + 1) * kMarchParts * 2 * kMarchThreads;
-}
 
 // Which Gaussians of the tile list a ray can use.  Both passes of every large
 // step only act on a Gaussian that passes its gate -- pass 1's (mass on the
 // ray in (1/255, 1000], positive variance, finite centre) or pass 2's
 // (gaussian_on_ray) -- and the gates depend on the ray alone, not on the
-// step.  So the first pass over the tile records, per pixel and per batch of
-// 64 list entries, a 64-bit mask of the entries that pass either gate, and the
-// large steps only intersect those.  Pass 1's depth break also only needs
-// them: the list is in depth order, so the first entry with depth > end of
-// the section set that is skipped here would be followed by a masked entry
-// with a depth at least as large, checked against the same end.  The results
-// are identical; the per-step cost drops from the tile's list to the ray's
-// own Gaussians.
+// step.  So a first pass over the tile records, per ray and per batch of list
+// entries, a mask of the entries that pass either gate, and the large steps
+// only intersect those.  Pass 1's depth break also only needs them: the list
+// is in depth order, so the first entry with depth > end of the section set
+// that is skipped here would be followed by a masked entry with a depth at
+// least as large, checked against the same end.  The results are identical;
+// the per-step cost drops from the tile's list to the ray's own Gaussians.
 template <class T>
 __device__ __forceinline__ bool ray_can_use(const Gauss1d<T>& g, T mass)
 {
@@ -264,347 +229,11 @@ __device__ __forceinline__ bool ray_can_use(const Gauss1d<T>& g, T mass)
     return pass1 || pass2;
 }
 
-// the ray's masks of one block: batch i, word w at m[i * kMarchParts * 2 * kMarchThreads + w * kMarchThreads + tid]
-struct RayMasks {
-    uint32_t* m;
-    __device__ __forceinline__ uint64_t get(int i) const
-    {
-        if (!m)
-            return ~0ull;
-        const size_t o = size_t(i) * kMarchParts * 2 * kMarchThreads + threadIdx.x;
-        return uint64_t(m[o]) | (uint64_t(m[o + kMarchThreads]) << 32);
-    }
-    __device__ __forceinline__ void put(int i, uint64_t bits) const
-    {
-        const size_t o = size_t(i) * kMarchParts * 2 * kMarchThreads + threadIdx.x;
-        m[o] = uint32_t(bits);
-        m[o + kMarchThreads] = uint32_t(bits >> 32);
-    }
-};
+} // namespace dgmr
 
+#include "dgmr_march_warp.cuh"
 
-template <class T>
-struct MarchShared {
-    uint32_t id[kMarchThreads];
-    T mu[3][kMarchThreads];
-    T Q[6][kMarchThreads];
-    T mass[kMarchThreads];
-    T rgb[3][kMarchThreads];
-    T depth[kMarchThreads];
-};
-
-template <class T>
-__device__ __forceinline__ void load_batch(MarchShared<T>& sh, const VmMarch<T>& a, int32_t k, int32_t e)
-{
-    if (k < e) {
-        const uint32_t id = uint32_t(a.list[k]);
-        sh.id[threadIdx.x] = id;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            sh.mu[c][threadIdx.x] = a.centroids[3 * size_t(id) + c];
-            sh.rgb[c][threadIdx.x] = a.rgb[3 * size_t(id) + c];
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-            sh.Q[c][threadIdx.x] = a.inv_cov[6 * size_t(id) + c];
-        sh.mass[threadIdx.x] = a.masses[id];
-        sh.depth[threadIdx.x] = a.depths[id];
-    }
-}
-
-template <class T>
-__device__ __forceinline__ S3<T> shared_Q(const MarchShared<T>& sh, int j)
-{
-    return S3<T> { { sh.Q[0][j], sh.Q[1][j], sh.Q[2][j], sh.Q[3][j], sh.Q[4][j], sh.Q[5][j] } };
-}
-
-// Pass 1 of a large step: sample sections from the Gaussians on the ray
-// (vol_marcher_forward.cu:351-403), block-synchronous over batches.
-__device__ __forceinline__ uint64_t batch_bits(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
-
-// first pass over the tile: the ray masks (see RayMasks)
-template <class T>
-__device__ __forceinline__ void build_ray_masks(const RayMasks& rm, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool inside, V3<T> o,
-    V3<T> d)
-{
-    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
-        __syncthreads();
-        load_batch(sh, a, base + int32_t(threadIdx.x), e);
-        __syncthreads();
-        const int n = min(int(kMarchThreads), e - base);
-        uint64_t m = 0;
-        if (inside)
-            for (int j = 0; j < n; ++j) {
-                const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
-                if (ray_can_use(intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d), sh.mass[j]))
-                    m |= 1ull << j;
-            }
-        rm.put((base - b) / int32_t(kMarchThreads), m);
-    }
-    __syncthreads();
-}
-
-template <class T>
-__device__ __forceinline__ void collect_sections(SectionSet<kLargeSteps, T>& sec, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done,
-    V3<T> o, V3<T> d, const RayMasks& rm)
-{
-    if (a.cs.n > 0) {
-        if (!done)
-            for (int i = 0; i < a.cs.n; ++i)
-                sec.put(Section<T> { a.cs.s[i][0], a.cs.s[i][1], a.cs.s[i][2] });
-        return;
-    }
-    bool done1 = done;
-    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
-        if (__syncthreads_count(done1) == int(kMarchThreads))
-            break;
-        load_batch(sh, a, base + int32_t(threadIdx.x), e);
-        __syncthreads();
-        if (done1)
-            continue;
-        const int n = min(int(kMarchThreads), e - base);
-        uint64_t m = rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n);
-        while (m) {
-            const int j = __ffsll((long long)m) - 1;
-            m &= m - 1ull;
-            const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
-            const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
-            const T sd = dgmr_fm::sqrt_f(g.C);
-            if (sec.hi < sh.depth[j]) {
-                done1 = true;
-                break;
-            }
-            const T mor = g.weight * sh.mass[j];
-            if (mor <= T(1.0f / 255.f) || mor > T(1000))
-                continue;
-            if (g.C <= T(0))
-                continue;
-            if (dgmr_fm::isnan_f(g.centre))
-                continue;
-            const T start = g.centre - sd * T(kRelevanceSigma);
-            const T end = g.centre + sd * T(kRelevanceSigma);
-            const T delta_t = ((sd * T(kRelevanceSigma)) * T(2)) / T(float(kStepsPerGaussian - 1));
-            sec.put(Section<T> { start, end, delta_t });
-        }
-    }
-}
-
-// Pass 2: CDF-difference bin masses of every Gaussian in the tile list
-template <class T>
-__device__ __forceinline__ void fill_bins(Bin<T>* bins, const T* borders, MarchShared<T>& sh, const VmMarch<T>& a, int32_t b, int32_t e, bool done, V3<T> o,
-    V3<T> d, const RayMasks& rm)
-{
-    for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
-        if (__syncthreads_count(done) == int(kMarchThreads))
-            break;
-        load_batch(sh, a, base + int32_t(threadIdx.x), e);
-        __syncthreads();
-        if (done)
-            continue;
-        const int n = min(int(kMarchThreads), e - base);
-        uint64_t m = rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n);
-        while (m) {
-            const int j = __ffsll((long long)m) - 1;
-            m &= m - 1ull;
-            const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
-            const Gauss1d<T> g = intersect_with_ray_inv_C(mu, shared_Q(sh, j), o, d);
-            sample_gaussian(g, sh.mass[j], V3<T> { sh.rgb[0][j], sh.rgb[1][j], sh.rgb[2][j] }, borders, bins);
-        }
-    }
-}
-
-// this block's ray masks, or none (every entry used) if the workspace has no room for them
-template <class T>
-__device__ __forceinline__ RayMasks block_masks(const VmMarch<T>& a, unsigned tile, unsigned part, int32_t b, int32_t e)
-{
-    RayMasks rm { nullptr };
-    if (!a.ray_masks || e <= b || b < 0)
-        return rm;
-    const size_t n_batches = size_t(e - b + int32_t(kMarchThreads) - 1) / kMarchThreads;
-    const size_t slot = size_t(uint32_t(b) / kMarchThreads) + tile;
-    if ((slot + n_batches) * kMarchParts * 2 * kMarchThreads <= a.ray_mask_words)
-        rm.m = a.ray_masks + (slot * kMarchParts + part) * 2 * kMarchThreads;
-    return rm;
-}
-
-template <class T>
-__global__ void __launch_bounds__(kMarchThreads) k_vm_march(VmMarch<T> a, CameraT<T> cam)
-{
-    __shared__ MarchShared<T> sh;
-    const unsigned tile = blockIdx.x / kMarchParts, part = blockIdx.x % kMarchParts;
-    const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + part * kMarchRows + (threadIdx.x >> 4);
-    const bool inside = px < cam.W && py < cam.H;
-    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
-    const V3<T> d = pixel_dir(cam, px, py);
-    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
-    const RayMasks rm = block_masks(a, tile, part, b, e);
-    if (rm.m)
-        build_ray_masks(rm, sh, a, b, e, inside, o, d);
-    bool done = !inside;
-    V3<T> colour = { T(0), T(0), T(0) };
-    T tr = T(1);
-    T start = T(0);
-    SectionSet<kLargeSteps, T> sec;
-    T borders[kSmallSteps];
-    Bin<T> bins[kBins];
-    for (unsigned step = 0;; ++step) {
-        if (__syncthreads_count(done) == int(kMarchThreads))
-            break;
-        if (step >= kMaxLargeSteps) {
-            if (!done)
-                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
-            break;
-        }
-        sec.reset(start);
-        collect_sections(sec, sh, a, b, e, done, o, d, rm);
-        sample_positions(sec, borders);
-        for (unsigned k = 0; k < kBins; ++k)
-            bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
-        fill_bins(bins, borders, sh, a, b, e, done, o, d, rm);
-        if (!done) {
-            integrate_bins(colour, tr, bins);
-            done = sec.n == 0 || tr < T(1.f / 255.f);
-        }
-        start = borders[kSmallSteps - 1];
-    }
-    if (!inside)
-        return;
-    const size_t pix = size_t(py) * cam.W + px;
-    const size_t plane = size_t(cam.W) * cam.H;
-    a.fb[pix] = colour.x + tr * cam.bg[0];
-    a.fb[plane + pix] = colour.y + tr * cam.bg[1];
-    a.fb[2 * plane + pix] = colour.z + tr * cam.bg[2];
-    a.remaining_T[pix] = tr;
-}
-
-template <class T>
-__device__ __forceinline__ T warp_sum_t(T v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// vol_marcher_backward.cu:115-319.  The 10 per-(pixel, Gaussian) atomics of
-// the reference are replaced by a warp-level shuffle sum and one atomic per
-// value per warp.
-template <class T>
-__global__ void __launch_bounds__(kMarchThreads) k_vm_march_bwd(VmMarch<T> a, CameraT<T> cam)
-{
-    __shared__ MarchShared<T> sh;
-    const unsigned tile = blockIdx.x / kMarchParts, part = blockIdx.x % kMarchParts;
-    const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + part * kMarchRows + (threadIdx.x >> 4);
-    const bool inside = px < cam.W && py < cam.H;
-    const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
-    const V3<T> d = pixel_dir(cam, px, py);
-    const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
-    const RayMasks rm = block_masks(a, tile, part, b, e);
-    if (rm.m)
-        build_ray_masks(rm, sh, a, b, e, inside, o, d);
-    const size_t pix = size_t(py) * cam.W + px;
-    const size_t plane = size_t(cam.W) * cam.H;
-    bool done = !inside;
-    V3<T> gc = { T(0), T(0), T(0) };
-    V3<T> colour = { T(0), T(0), T(0) };
-    T final_T = T(1), gt = T(0);
-    if (inside) {
-        final_T = a.remaining_T[pix];
-        colour = { a.fb[pix] - final_T * cam.bg[0], a.fb[plane + pix] - final_T * cam.bg[1], a.fb[2 * plane + pix] - final_T * cam.bg[2] };
-        gc = { a.grad_fb[pix], a.grad_fb[plane + pix], a.grad_fb[2 * plane + pix] };
-        gt = (gc.x * cam.bg[0] + gc.y * cam.bg[1]) + gc.z * cam.bg[2];
-    }
-    T tr = T(1);
-    T start = T(0);
-    const int lane = threadIdx.x & 31;
-    SectionSet<kLargeSteps, T> sec;
-    T borders[kSmallSteps];
-    Bin<T> bins[kBins];
-    Bin<T> gbins[kBins];
-    for (unsigned step = 0;; ++step) {
-        if (__syncthreads_count(done) == int(kMarchThreads))
-            break;
-        if (step >= kMaxLargeSteps) {
-            if (!done)
-                atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
-            break;
-        }
-        sec.reset(start);
-        collect_sections(sec, sh, a, b, e, done, o, d, rm);
-        sample_positions(sec, borders);
-        for (unsigned k = 0; k < kBins; ++k)
-            bins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
-        fill_bins(bins, borders, sh, a, b, e, done, o, d, rm);
-        if (!done)
-            grad_integrate_bins(colour, tr, final_T, bins, gc, gt, gbins);
-        // pass 3: adjoint of the bin masses, per Gaussian
-        for (int32_t base = b; base < e; base += int32_t(kMarchThreads)) {
-            if (__syncthreads_count(done) == int(kMarchThreads))
-                break;
-            load_batch(sh, a, base + int32_t(threadIdx.x), e);
-            __syncthreads();
-            const int n = min(int(kMarchThreads), e - base);
-            const uint64_t mine = done ? 0ull : (rm.get((base - b) / int32_t(kMarchThreads)) & batch_bits(n));
-            uint64_t todo = uint64_t(__reduce_or_sync(0xffffffffu, uint32_t(mine)))
-                | (uint64_t(__reduce_or_sync(0xffffffffu, uint32_t(mine >> 32))) << 32);
-            while (todo) {
-                const int j = __ffsll((long long)todo) - 1;
-                todo &= todo - 1ull;
-                T v[10];
-                V3<T> gmu = { T(0), T(0), T(0) };
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    v[q] = T(0);
-                if ((mine >> j) & 1ull) {
-                    const V3<T> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
-                    V3<T> grgb = { T(0), T(0), T(0) };
-                    S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
-                    grad_sample_gaussian(mu, shared_Q(sh, j), o, d, sh.mass[j], V3<T> { sh.rgb[0][j], sh.rgb[1][j], sh.rgb[2][j] }, borders, gbins, &v[0], &grgb,
-                        &gmu, &gQ);
-                    v[1] = grgb.x;
-                    v[2] = grgb.y;
-                    v[3] = grgb.z;
-#pragma unroll
-                    for (int q = 0; q < 6; ++q)
-                        v[4 + q] = gQ.v[q];
-                }
-                bool any = false;
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    any = any || v[q] != T(0);
-                any = any || gmu.x != T(0) || gmu.y != T(0) || gmu.z != T(0);
-                if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-                    for (int q = 0; q < 10; ++q)
-                        v[q] = warp_sum_t(v[q]);
-                    gmu.x = warp_sum_t(gmu.x);
-                    gmu.y = warp_sum_t(gmu.y);
-                    gmu.z = warp_sum_t(gmu.z);
-                    if (lane == 0) {
-                        const uint32_t id = sh.id[j];
-                        T* dst = a.acc + size_t(id) * 10;
-#pragma unroll
-                        for (int q = 0; q < 10; ++q)
-                            if (v[q] != T(0))
-                                atomicAdd(dst + q, v[q]);
-                        T* gm = a.g_centroids + size_t(id) * 3;
-                        if (gmu.x != T(0))
-                            atomicAdd(gm, gmu.x);
-                        if (gmu.y != T(0))
-                            atomicAdd(gm + 1, gmu.y);
-                        if (gmu.z != T(0))
-                            atomicAdd(gm + 2, gmu.z);
-                    }
-                }
-            }
-        }
-        if (!done)
-            done = sec.n == 0 || tr < T(1.f / 255.f);
-        start = borders[kSmallSteps - 1];
-    }
-}
+namespace dgmr {
 
 template <class T>
 struct VmBwdGauss {
@@ -703,6 +332,22 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     p.g_centroids[3 * i + 2] += g_mu.z;
 }
 
+// Heaviest-tile-first order of the march's blocks, in the workspace past the
+// layout (none -- natural order -- if the workspace has no room for it).
+template <class T>
+inline const uint32_t* march_order(const int32_t* ranges, const CameraT<T>& cam, void* workspace, size_t layout_bytes, size_t workspace_bytes,
+    cudaStream_t s)
+{
+    const uint32_t n_tiles = cam.gx * cam.gy;
+    const size_t off = align_up(layout_bytes);
+    if (!workspace || workspace_bytes < off + size_t(n_tiles) * sizeof(uint32_t))
+        return nullptr;
+    uint32_t* order = reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) + off);
+    k_tile_order<<<1, 1024, 0, s>>>(ranges, n_tiles, order);
+    note_launch();
+    return order;
+}
+
 template <class T>
 inline T aa_multiplier(const CameraT<T>& cam)
 {
@@ -766,8 +411,8 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.remaining_T = static_cast<T*>(c->remaining_transparency);
     a.stats = st_dev;
     a.cs = const_samples<T>();
-    vm_ray_masks(workspace, L.bytes, workspace_bytes, &a.ray_masks, &a.ray_mask_words);
-    k_vm_march<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
+    const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
+    k_vm_march_warp<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
     note_launch();
     return launch_status();
 }
@@ -801,8 +446,9 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     a.g_centroids = static_cast<T*>(g_centroids);
     a.stats = st_dev;
     a.cs = const_samples<T>();
-    vm_ray_masks(workspace, L.bytes, workspace_bytes, &a.ray_masks, &a.ray_mask_words);
-    k_vm_march_bwd<T><<<cam.gx * cam.gy * kMarchParts, kMarchThreads, 0, s>>>(a, cam);
+    const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
+    k_vm_march_warp_bwd<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
+    note_launch();
     VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
         c->tiles_touched, L.acc, static_cast<T*>(g_sh), static_cast<T*>(g_weights), static_cast<T*>(g_centroids), static_cast<T*>(g_scales),
@@ -829,7 +475,7 @@ size_t dgmr_vm_workspace_size(int32_t n_gaussians, int32_t width, int32_t height
     if (n_gaussians < 0 || width <= 0 || height <= 0 || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
         return 0;
     const uint32_t n_tiles = ((uint32_t(width) + kTile - 1) / kTile) * ((uint32_t(height) + kTile - 1) / kTile);
-    const size_t masks = vm_ray_mask_words(uint32_t(pair_capacity), n_tiles) * sizeof(uint32_t);
+    const size_t masks = size_t(n_tiles) * sizeof(uint32_t); // march order
     if (dtype == DGMR_F64)
         return align_up(vm_layout<double>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;
     return align_up(vm_layout<float>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;

@@ -1,6 +1,7 @@
 // Per-ray state of the volume marcher: the capacity-bounded section set that
-// chooses sample positions, the 128-sample walk over it, and the per-bin
-// accumulation / blending helpers with their adjoints.
+// chooses sample positions, the 128-sample walk over it, and the adjoint of
+// one Gaussian's bin masses (the forward accumulation and the blend live in
+// the warp-per-ray march, dgmr_march_warp.cuh).
 //
 // Semantics follow src/dgmr/marching_steps.h:35-220 (DensityArray, sample),
 // src/dgmr/math.h:412-468 (integrate_bins, sample_gaussian) and
@@ -57,8 +58,9 @@ __device__ __forceinline__ bool gaussian_on_ray(const Gauss1d<T>& g, T mass, T* 
 // skipped by the mass test anyway.  For double the cut is |z| >= 5, where the
 // tail mass (< 1e-12) times the largest accepted mass on the ray (1000) stays
 // far below the 1e-5 per-bin threshold.  The borders are non-decreasing, so
-// both ends are found by binary search; the loops below then visit exactly
-// the bins that could pass the test, in the same order, with the same values.
+// both ends are found by binary search; the adjoint loop below then visits
+// exactly the bins that could pass the test, in the same order, with the same
+// values.
 template <class T>
 __device__ __forceinline__ T tail_z();
 template <>
@@ -92,81 +94,6 @@ __device__ __forceinline__ void live_bins(const T* borders, T c, T inv_sd, int* 
     const int j1 = first_border<T, false>(borders, int(kSmallSteps), c, inv_sd, tail_z<T>());
     *k_first = i0 > 0 ? i0 - 1 : 0;
     *k_last = j1 - 1 < int(kBins) - 1 ? j1 - 1 : int(kBins) - 1;
-}
-
-// math.h:430-468
-template <class T>
-__device__ __forceinline__ void sample_gaussian(const Gauss1d<T>& g, T mass, V3<T> rgb, const T* borders, Bin<T>* bins)
-{
-    T sd, mor;
-    if (!gaussian_on_ray(g, mass, &sd, &mor))
-        return;
-    const T inv_sd = T(1) / sd;
-    const T centre = g.centre;
-    const T mib = mor * (cdf_inv_SD(centre, inv_sd, borders[kBins]) - cdf_inv_SD(centre, inv_sd, borders[0]));
-    if (mib < T(0.0001f))
-        return;
-    int k0, k1;
-    live_bins(borders, centre, inv_sd, &k0, &k1);
-    T cdf_start = cdf_inv_SD(centre, inv_sd, borders[k0]);
-    for (int k = k0; k <= k1; ++k) {
-        const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
-        const T m = max_f(T(0), (cdf_end - cdf_start) * mor);
-        cdf_start = cdf_end;
-        if (m < T(0.00001f))
-            continue;
-        Bin<T> b = bins[k];
-        b.r = b.r + rgb.x * m;
-        b.g = b.g + rgb.y * m;
-        b.b = b.b + rgb.z * m;
-        b.m = b.m + m;
-        bins[k] = b;
-    }
-}
-
-// math.h:412-428
-template <class T>
-__device__ __forceinline__ void integrate_bins(V3<T>& colour, T& transparency, const Bin<T>* bins)
-{
-    for (unsigned k = 0; k < kBins; ++k) {
-        const Bin<T> b = bins[k];
-        const T tk = dgmr_fm::exp_f(-b.m);
-        colour.x = colour.x + b.r * transparency;
-        colour.y = colour.y + b.g * transparency;
-        colour.z = colour.z + b.b * transparency;
-        transparency = transparency * tk;
-        if (transparency < T(1. / 255.))
-            break;
-    }
-}
-
-// grad/math.h:529-557 (colour peeling, front to back); gbins fully written
-template <class T>
-__device__ __forceinline__ void grad_integrate_bins(V3<T>& colour, T& transparency, T final_transparency, const Bin<T>* bins, V3<T> gc, T gt, Bin<T>* gbins)
-{
-    unsigned k = 0;
-    for (; k < kBins; ++k) {
-        const Bin<T> b = bins[k];
-        Bin<T> gb;
-        gb.r = transparency * gc.x;
-        gb.g = transparency * gc.y;
-        gb.b = transparency * gc.z;
-        const T tk = dgmr_fm::exp_f(-b.m);
-        const T inv_tk = min_f(T(255), T(1) / tk);
-        colour.x = (colour.x - b.r) * inv_tk;
-        colour.y = (colour.y - b.g) * inv_tk;
-        colour.z = (colour.z - b.b) * inv_tk;
-        const T g_tk = (final_transparency * inv_tk) * gt + dot3(gc, colour) * transparency;
-        gb.m = T(0) - g_tk * tk;
-        gbins[k] = gb;
-        transparency = transparency * tk;
-        if (transparency < T(1. / 255.)) {
-            ++k;
-            break;
-        }
-    }
-    for (; k < kBins; ++k)
-        gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
 }
 
 // grad/math.h:559-620; accumulates into the outputs

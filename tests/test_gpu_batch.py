@@ -93,7 +93,8 @@ def test_batch_graph_replay_matches_eager(cuda):
         assert torch.equal(a, b)
     for k in eager_g:
         for a, b in zip(p.grads[k], eager_g[k]):
-            assert torch.allclose(a, b, rtol=1e-4, atol=1e-6)
+            # the per-pixel gradient sums use atomics: equal up to their order
+            assert float((a - b).abs().max()) <= 1e-4 * float(b.abs().max()) + 1e-7
 
 
 def test_batch_capacity_overflow_is_flagged(cuda):
