@@ -36,6 +36,7 @@ struct RayWarpSharedBwd {
     T borders[kSmallSteps];
     Bin<T> bins[kSmallSteps];
     Bin<T> gbins[kSmallSteps]; // bin adjoints
+    int32_t queue[32]; // pass 3: list entries waiting for a lane
 };
 
 // The gates of both passes (see ray_can_use) as a 32-bit mask per batch of 32
@@ -340,40 +341,81 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, 
 
 namespace dgmr {
 
-// Pass 3 (grad/math.h:559-620): the ray's Gaussians of a batch are taken one
-// per lane, and each lane runs the whole adjoint of its Gaussian over the
-// bins in shared memory -- in bin order, so its sums round exactly as the
-// one-thread loop does -- then adds the result to the per-Gaussian
-// accumulators.
+// Adjoint of one Gaussian's bin masses (grad/math.h:559-620), run by one lane
+// over the bins in shared memory -- in bin order, so its sums round exactly
+// as the one-thread loop does -- then added to the per-Gaussian accumulators.
 template <class T>
-__device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
+__device__ __forceinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, const Bin<T>* gbins, const T* borders, V3<T> o, V3<T> d)
+{
+    const RayEntry<T> en = load_entry(a, k);
+    const V3<T> rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
+    T g_mass = T(0);
+    V3<T> grgb = { T(0), T(0), T(0) }, gmu = { T(0), T(0), T(0) };
+    S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
+    grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ);
+    T* dst = a.acc + size_t(en.id) * 10;
+    const T v[10] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5] };
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+        if (v[q] != T(0))
+            atomicAdd(dst + q, v[q]);
+    T* gm = a.g_centroids + size_t(en.id) * 3;
+    if (gmu.x != T(0))
+        atomicAdd(gm, gmu.x);
+    if (gmu.y != T(0))
+        atomicAdd(gm + 1, gmu.y);
+    if (gmu.z != T(0))
+        atomicAdd(gm + 2, gmu.z);
+}
+
+// Pass 3: the ray's Gaussians that reach the bins are gathered, in list
+// order, into a queue of 32 and run one per lane, so the lanes stay busy
+// however sparse the ray's entries are in the tile list.  (Each Gaussian's
+// adjoint is independent of the others'; only the atomic additions of
+// different pixels meet, in no fixed order, as in the one-thread kernel.)
+template <class T>
+__device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders, int32_t* queue, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
     const WarpRayMasks& rm, unsigned lane)
 {
-    unsigned i = 0;
+    unsigned i = 0, fill = 0;
     for (int32_t base = b; base < e; base += 32, ++i) {
         const uint32_t m = rm.get(i) & lanes_below(e - base);
-        if (!((m >> lane) & 1u))
+        if (!m)
             continue;
-        const RayEntry<T> en = load_entry(a, base + int32_t(lane));
-        const V3<T> rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
-        T g_mass = T(0);
-        V3<T> grgb = { T(0), T(0), T(0) }, gmu = { T(0), T(0), T(0) };
-        S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
-        grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ);
-        T* dst = a.acc + size_t(en.id) * 10;
-        const T v[10] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5] };
-#pragma unroll
-        for (int q = 0; q < 10; ++q)
-            if (v[q] != T(0))
-                atomicAdd(dst + q, v[q]);
-        T* gm = a.g_centroids + size_t(en.id) * 3;
-        if (gmu.x != T(0))
-            atomicAdd(gm, gmu.x);
-        if (gmu.y != T(0))
-            atomicAdd(gm + 1, gmu.y);
-        if (gmu.z != T(0))
-            atomicAdd(gm + 2, gmu.z);
+        bool ok = false;
+        if ((m >> lane) & 1u) {
+            const RayEntry<T> en = load_entry(a, base + int32_t(lane));
+            Gauss1d<T> g;
+            T sd, inv_sd, mor;
+            ok = warp_entry_on_bins(en, o, d, borders, &g, &sd, &inv_sd, &mor);
+        }
+        const uint32_t okm = __ballot_sync(0xffffffffu, ok);
+        const unsigned n_ok = unsigned(__popc(okm));
+        if (ok) {
+            const unsigned slot = fill + unsigned(__popc(okm & lanes_below(int(lane))));
+            if (slot < 32)
+                queue[slot] = base + int32_t(lane);
+        }
+        __syncwarp();
+        if (fill + n_ok >= 32) {
+            lane_grad_entry(a, queue[lane], gbins, borders, o, d);
+            __syncwarp();
+            // the entries that did not fit go to the front of the emptied queue
+            const unsigned left = fill + n_ok - 32;
+            if (ok) {
+                const unsigned slot = fill + unsigned(__popc(okm & lanes_below(int(lane))));
+                if (slot >= 32)
+                    queue[slot - 32] = base + int32_t(lane);
+            }
+            __syncwarp();
+            fill = left;
+        } else {
+            fill += n_ok;
+        }
     }
+    if (lane < fill)
+        lane_grad_entry(a, queue[lane], gbins, borders, o, d);
+    __syncwarp();
 }
 
 // vol_marcher_backward.cu:115-319 with one warp per ray
@@ -440,7 +482,7 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp_bwd(VmMarch<T>
             if (lane == 0)
                 sm.gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
         __syncwarp();
-        warp_grad(sm.gbins, sm.borders, a, b, e, o, d, rm, lane);
+        warp_grad(sm.gbins, sm.borders, sm.queue, a, b, e, o, d, rm, lane);
         const bool done = sec.n == 0 || tr < T(1.f / 255.f);
         start = sm.borders[kSmallSteps - 1];
         __syncwarp();
