@@ -68,6 +68,13 @@ class SceneGrads(C.Structure):
                 ("rotations", C.c_void_p)]
 
 
+VR_RENDER_FULL, VR_RENDER_BINS, VR_RENDER_DEPTH = 0, 1, 2
+
+
+class VrOptions(C.Structure):
+    _fields_ = [("render_mode", C.c_int32), ("debug_bin", C.c_int32), ("max_depth", C.c_double)]
+
+
 # every symbol include/dgmr_b200.h declares, with its ctypes signature
 _SIGNATURES = {
     "dgmr_splat_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
@@ -96,6 +103,11 @@ _SIGNATURES = {
     "dgmr_splat_batch_backward": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
                                             C.POINTER(SceneGrads), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
                                             C.c_int64, C.c_void_p]),
+    "dgmr_vr_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "dgmr_vr_pair_workspace_size": (C.c_size_t, [C.c_int32, C.c_int64]),
+    "dgmr_vr_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "dgmr_vr_forward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VrOptions), C.c_void_p, C.c_void_p, C.c_size_t,
+                                  C.c_void_p, C.c_size_t, C.c_int64, C.c_void_p, C.c_void_p]),
     "dgmr_vm_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
     "dgmr_vm_forward_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p,
                                              C.c_size_t, C.c_void_p, C.c_void_p]),

@@ -203,6 +203,35 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
     int64_t pair_capacity, dgmr_stream stream);
 
+/* ---------------------------------------------------------- vol_raster */
+
+/* Replaces dgmr::vol_raster_forward(VolRasterForwardData&)
+ * (src/dgmr/vol_raster_forward.h:70, .cu:39-520): forward-only volume
+ * rasteriser, float.  Per pixel 32 depth bins placed by a RasterBinSizer,
+ * piecewise-linear blend with 256 steps per bin.  Same two-workspace scheme as
+ * the splat renderer (the binning is the same); dgmr_vr_preprocess leaves the
+ * pair count in stats->n_pairs for callers that size the pair workspace from
+ * the frame.  An empty frame renders the background (the reference leaves the
+ * framebuffer unwritten). */
+typedef enum dgmr_vr_render_mode {
+    DGMR_VR_RENDER_FULL = 0, /* RenderMode::Full */
+    DGMR_VR_RENDER_BINS = 1, /* RenderMode::Bins (the reference draws nothing: background) */
+    DGMR_VR_RENDER_DEPTH = 2, /* RenderMode::Depth: end of debug_bin / max_depth */
+} dgmr_vr_render_mode;
+
+typedef struct dgmr_vr_options { /* VolRasterForwardData's debug fields; NULL = Full */
+    int32_t render_mode;
+    int32_t debug_bin; /* -1 = last bin */
+    double max_depth; /* 20 in the reference */
+} dgmr_vr_options;
+
+size_t dgmr_vr_frame_workspace_size(int32_t n_gaussians, int32_t width, int32_t height);
+size_t dgmr_vr_pair_workspace_size(int32_t n_gaussians, int64_t pair_capacity);
+dgmr_status dgmr_vr_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, void* frame_workspace, size_t frame_workspace_bytes,
+    dgmr_frame_stats* stats, dgmr_stream stream);
+dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vr_options* options, float* framebuffer, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
 /* ---------------------------------------------------------- vol_marcher */
 
 /* The reference's ForwardCache plus framebuffer (vol_marcher_forward.h:28-41,

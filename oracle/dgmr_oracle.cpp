@@ -29,6 +29,7 @@
 #endif
 
 #include "dgmr_oracle_marching.h"
+#include "../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_volume_fit.h"
 
 using namespace orc;
 
@@ -1125,6 +1126,225 @@ SceneIn<T> make_scene(int N, const T* centroids, const T* sh, int sh_stride, int
     return s;
 }
 
+// ------------------------------------------------------------- vol_raster
+// src/dgmr/vol_raster_forward.cu:39-520 (float only, as in the reference)
+constexpr unsigned VR_BINS = 32; // vol_raster_forward.h:61
+constexpr unsigned VR_STEPS_PER_BIN = 256; // vol_raster_forward.h:62
+constexpr float VR_TRANSMISSION = 0.005f; // vol_raster_forward.h:63
+constexpr float VR_RELEVANCE_SIGMA = 3.f; // vol_raster_forward.h:64
+
+struct VrCache {
+    float *rgb, *depths, *xy, *inv_cov, *masses;
+    uint8_t* clamped;
+    int32_t *rects, *tiles_touched;
+};
+
+// vol_raster_forward.cu:86-136
+void vr_preprocess(const SceneIn<float>& s, VrCache& c)
+{
+    const unsigned W = unsigned(s.W), H = unsigned(s.H);
+    const unsigned gx = (W + TILE - 1) / TILE, gy = (H + TILE - 1) / TILE;
+    Camera<float> cam;
+    cam.view = s.view;
+    cam.proj = s.proj;
+    cam.focal_y = float(H) / (2.0f * s.tan_fovy);
+    cam.focal_x = float(W) / (2.0f * s.tan_fovx);
+    cam.tan_fovx = s.tan_fovx;
+    cam.tan_fovy = s.tan_fovy;
+    cam.W = W;
+    cam.H = H;
+    const float aa = vm_aa_multiplier(s);
+    const V3<float> campos = load3(s.campos, 0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < s.N; ++i) {
+        c.tiles_touched[i] = 0;
+        c.rects[2 * i] = c.rects[2 * i + 1] = 0;
+        c.xy[2 * i] = c.xy[2 * i + 1] = 0.f;
+        c.depths[i] = 0.f;
+        c.masses[i] = 0.f;
+        for (int k = 0; k < 3; ++k) {
+            c.rgb[3 * i + k] = 0.f;
+            c.clamped[3 * i + k] = 0;
+        }
+        for (int k = 0; k < 6; ++k)
+            c.inv_cov[6 * i + k] = 0.f;
+        const V3<float> mu = load3(s.centroids, size_t(i));
+        if (mat4_mul_point(s.view, mu).z < 0.2f)
+            continue;
+        const float w = s.weights[i];
+        const V3<float> sc = mul(load3(s.scales, size_t(i)), s.cov_scale_multiplier);
+        const float* q = s.rotations + 4 * size_t(i);
+        const Gaussian2d<float> g = splat(Formulation::Ots, w, mu, sc, q, cam, 0.3f);
+        const S3<float> cov3 = compute_cov(sc, q);
+        const float fks = length(sub(mu, campos)) * aa;
+        const float fks2 = fks * fks;
+        S3<float> filtered = cov3;
+        filtered.v[0] = filtered.v[0] + fks2;
+        filtered.v[3] = filtered.v[3] + fks2;
+        filtered.v[5] = filtered.v[5] + fks2;
+        // weight_to_mass<Ots> of the scales plus the squared filter size (vol_raster_forward.cu:106)
+        c.masses[i] = weight_to_mass(Formulation::Ots, w, V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 }, g.cov);
+        const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
+        const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
+        c.rects[2 * i] = ex;
+        c.rects[2 * i + 1] = ey;
+        const URect r = get_rect(g.centroid.x, g.centroid.y, ex, ey, gx, gy);
+        const unsigned touched = (r.x1 - r.x0) * (r.y1 - r.y0);
+        if (touched == 0)
+            continue;
+        c.tiles_touched[i] = int32_t(touched);
+        c.xy[2 * i] = g.centroid.x;
+        c.xy[2 * i + 1] = g.centroid.y;
+        c.depths[i] = length(sub(campos, mu));
+        const V3<float> v = sub(mu, campos);
+        const V3<float> dir = mul(v, 1.f / dgmr_fm::sqrt_f(dot(v, v)));
+        V3<float> sh16[16];
+        load_sh16(s, unsigned(i), 0.f, sh16);
+        bool cl[3];
+        const V3<float> col = sh_to_colour(sh16, s.sh_degree, dir, cl);
+        c.rgb[3 * i] = col.x;
+        c.rgb[3 * i + 1] = col.y;
+        c.rgb[3 * i + 2] = col.z;
+        for (int k = 0; k < 3; ++k)
+            c.clamped[3 * i + k] = cl[k] ? 1 : 0;
+        const S3<float> inv = inverse_sym3(filtered);
+        for (int k = 0; k < 6; ++k)
+            c.inv_cov[6 * i + k] = inv.v[k];
+    }
+}
+
+// exp(-(x - c)^2 / (2 var)), the unnormalised 1-D Gaussian
+inline float eval_exponential_1d(float c, float var, float x)
+{
+    const float dx = x - c;
+    return dgmr_fm::exp_f((-0.5f * (dx * dx)) / var);
+}
+
+// Ray through the pixel corner at NDC z = -1 (vol_raster_forward.cu:263-268)
+Ray<float> vr_pixel_ray(const float* inv_proj, V3<float> campos, unsigned px, unsigned py, unsigned W, unsigned H)
+{
+    const float nx = float(px * 2u) / float(W) - 1.f;
+    const float ny = float(py * 2u) / float(H) - 1.f;
+    V4<float> v = mat4_mul_vec4(inv_proj, V4<float> { nx, ny, -1.f, 1.f });
+    v.x = v.x / v.w;
+    v.y = v.y / v.w;
+    v.z = v.z / v.w;
+    const V3<float> dvec = { v.x - campos.x, v.y - campos.y, v.z - campos.z };
+    const float il = 1.f / dgmr_fm::sqrt_f(dot(dvec, dvec));
+    Ray<float> r;
+    r.o = campos;
+    r.d = mul(dvec, il);
+    return r;
+}
+
+// vol_raster_forward.cu:253-517: bin sizing, rasterisation into bins, piecewise-linear blend
+void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges, const uint32_t* list, float* fb)
+{
+    const unsigned W = unsigned(s.W), H = unsigned(s.H);
+    const unsigned gx = (W + TILE - 1) / TILE, gy = (H + TILE - 1) / TILE;
+    float inv_proj[16];
+    inverse4(s.proj, inv_proj);
+    const V3<float> campos = load3(s.campos, 0);
+    const V3<float> bg = load3(s.bg, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int tile = 0; tile < int(gx * gy); ++tile) {
+        const unsigned tx = unsigned(tile) % gx, ty = unsigned(tile) / gx;
+        const int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
+        for (unsigned ly = 0; ly < TILE; ++ly)
+            for (unsigned lx = 0; lx < TILE; ++lx) {
+                const unsigned px = tx * TILE + lx, py = ty * TILE + ly;
+                if (px >= W || py >= H)
+                    continue;
+                const Ray<float> ray = vr_pixel_ray(inv_proj, campos, px, py, W, H);
+                dgmr::RasterBinSizer<VR_BINS> sizer;
+                sizer.init(VR_RELEVANCE_SIGMA, VR_TRANSMISSION);
+                for (int32_t k = b; k < e; ++k) { // pass A: bin sizes
+                    const uint32_t id = list[k];
+                    S3<float> Q;
+                    for (int j = 0; j < 6; ++j)
+                        Q.v[j] = c.inv_cov[6 * size_t(id) + j];
+                    const Gauss1d<float> g = intersect_with_ray_inv_C(load3(s.centroids, id), Q, ray);
+                    const float mor = g.weight * c.masses[id];
+                    if (mor < 0.001f || mor > 1000.f)
+                        continue;
+                    if (g.C + 0.f <= 0.f)
+                        continue;
+                    sizer.add_gaussian(mor, g.centre, dgmr_fm::sqrt_f(g.C + 0.f));
+                    if (sizer.is_full())
+                        break;
+                }
+                sizer.finalise();
+                float bin_mass[VR_BINS][4] = {};
+                float bin_eval[VR_BINS + 1][4] = {};
+                for (int32_t k = b; k < e; ++k) { // pass B: masses and border values per bin
+                    const uint32_t id = list[k];
+                    S3<float> Q;
+                    for (int j = 0; j < 6; ++j)
+                        Q.v[j] = c.inv_cov[6 * size_t(id) + j];
+                    const Gauss1d<float> g = intersect_with_ray_inv_C(load3(s.centroids, id), Q, ray);
+                    const float centre = g.centre;
+                    const float variance = g.C + 0.f;
+                    const float sd = dgmr_fm::sqrt_f(variance);
+                    const float inv_sd = 1.f / sd;
+                    const float weight = g.weight * c.masses[id];
+                    if (variance <= 0.f || dgmr_fm::isnan_f(variance) || dgmr_fm::isnan_f(weight) || weight > 100000.f)
+                        continue;
+                    if (weight * integrate_normalised_inv_SD(centre, inv_sd, 0.f, sizer.end_of(VR_BINS - 1)) <= 0.001f)
+                        continue;
+                    const V3<float> rgb = load3(c.rgb, id);
+                    float cdf_start = cdf_inv_SD(centre, inv_sd, 0.f);
+                    for (unsigned q = 0; q < VR_BINS; ++q) {
+                        const float cdf_end = cdf_inv_SD(centre, inv_sd, sizer.end_of(q));
+                        const float mass = (cdf_end - cdf_start) * weight;
+                        cdf_start = cdf_end;
+                        if (mass < 0.0001f)
+                            continue;
+                        bin_mass[q][0] = bin_mass[q][0] + rgb.x * mass;
+                        bin_mass[q][1] = bin_mass[q][1] + rgb.y * mass;
+                        bin_mass[q][2] = bin_mass[q][2] + rgb.z * mass;
+                        bin_mass[q][3] = bin_mass[q][3] + mass;
+                        const float ev = weight * eval_exponential_1d(centre, variance, sizer.begin_of(q));
+                        bin_eval[q][0] = bin_eval[q][0] + rgb.x * ev;
+                        bin_eval[q][1] = bin_eval[q][1] + rgb.y * ev;
+                        bin_eval[q][2] = bin_eval[q][2] + rgb.z * ev;
+                        bin_eval[q][3] = bin_eval[q][3] + ev;
+                    }
+                    const float ev = weight * eval_exponential_1d(centre, variance, sizer.end_of(VR_BINS - 1));
+                    bin_eval[VR_BINS][0] = bin_eval[VR_BINS][0] + rgb.x * ev;
+                    bin_eval[VR_BINS][1] = bin_eval[VR_BINS][1] + rgb.y * ev;
+                    bin_eval[VR_BINS][2] = bin_eval[VR_BINS][2] + rgb.z * ev;
+                    bin_eval[VR_BINS][3] = bin_eval[VR_BINS][3] + ev;
+                }
+                // blend (RenderMode::Full).  The split of a bin's mass between its halves
+                // evaluates to 0.5 for every bin and channel (vol_raster_forward.cu:473).
+                float res[3] = { 0.f, 0.f, 0.f };
+                float transparency = 1.f;
+                const float half[4] = { 0.5f, 0.5f, 0.5f, 0.5f };
+                for (unsigned q = 0; q < VR_BINS; ++q) {
+                    const float t_right = sizer.end_of(q) - sizer.begin_of(q);
+                    if (t_right <= 0.f)
+                        continue;
+                    const dgmr::FunctionGroup<float> f = dgmr::create_approximation(half, bin_mass[q], bin_eval[q], bin_eval[q + 1], t_right);
+                    const float dt = f.t_right / float(VR_STEPS_PER_BIN);
+                    float t = dt / 2.f;
+                    for (unsigned i = 0; i < VR_STEPS_PER_BIN; ++i) {
+                        const float e0 = f.sample(0, t), e1 = f.sample(1, t), e2 = f.sample(2, t), e3 = f.sample(3, t);
+                        res[0] = res[0] + (e0 * transparency) * dt;
+                        res[1] = res[1] + (e1 * transparency) * dt;
+                        res[2] = res[2] + (e2 * transparency) * dt;
+                        transparency = transparency * dgmr_fm::max_f(0.f, 1.f - e3 * dt);
+                        t = t + dt;
+                    }
+                }
+                // final colour C + T * background with T = 1 in this mode (vol_raster_forward.cu:509-513)
+                const size_t pix = size_t(py) * W + px;
+                fb[pix] = res[0] + 1.f * bg.x;
+                fb[size_t(W) * H + pix] = res[1] + 1.f * bg.y;
+                fb[2 * size_t(W) * H + pix] = res[2] + 1.f * bg.z;
+            }
+    }
+}
+
 } // namespace
 
 // ======================================================================= C ABI
@@ -1264,6 +1484,32 @@ DEF_VM(float, f32)
 DEF_VM(double, f64)
 
 // ------------------------------------------------- known-answer test hooks
+// vol_raster forward (float).  Returns P; the sorted point list is written
+// when P <= pair_capacity.
+int64_t orc_vr_forward_f32(SCENE_ARGS(float), float* fb, int32_t* rects, float* rgb, uint8_t* clamped, float* depths, float* xy, float* inv_cov,
+    float* masses, int32_t* tiles_touched, int32_t* point_offsets, int32_t* i_ranges, uint32_t* point_list, int64_t pair_capacity)
+{
+    const SceneIn<float> s = make_scene<float>(SCENE_PASS);
+    const unsigned gx = (unsigned(W) + TILE - 1) / TILE, gy = (unsigned(H) + TILE - 1) / TILE;
+    VrCache c { rgb, depths, xy, inv_cov, masses, clamped, rects, tiles_touched };
+    vr_preprocess(s, c);
+    inclusive_scan(N, tiles_touched, point_offsets);
+    const Binning b = bin_gaussians(N, rects, xy, depths, tiles_touched, point_offsets, gx, gy);
+    std::memcpy(i_ranges, b.ranges.data(), b.ranges.size() * 4);
+    const int64_t P = int64_t(b.vals.size());
+    if (P <= pair_capacity && point_list)
+        std::memcpy(point_list, b.vals.data(), size_t(P) * 4);
+    if (P == 0) {
+        // no pair: the framebuffer is the background (the reference returns before writing it)
+        for (size_t k = 0; k < size_t(W) * size_t(H); ++k)
+            for (int ch = 0; ch < 3; ++ch)
+                fb[size_t(ch) * size_t(W) * size_t(H) + k] = bg[ch];
+        return 0;
+    }
+    vr_render(s, c, b.ranges.data(), b.vals.data(), fb);
+    return P;
+}
+
 } // extern "C"
 
 namespace {

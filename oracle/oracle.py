@@ -54,6 +54,9 @@ def _declare(L):
     L.orc_splat_forward_f32.argtypes = _scene_types(_f32p) + [
         _f32p, _i32p, _f32p, _u8p, _f32p, _f32p, _f32p, _i32p, _i32p, _i32p,
         C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.orc_vr_forward_f32.restype = C.c_int64
+    L.orc_vr_forward_f32.argtypes = _scene_types(_f32p) + [
+        _f32p, _i32p, _f32p, _u8p, _f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _i32p, C.c_void_p, C.c_int64]
     L.orc_splat_backward_f32.restype = None
     L.orc_splat_backward_f32.argtypes = _scene_types(_f32p) + [
         _f32p, _u8p, _f32p, _f32p, _i32p, _i32p, _u32p, _f32p, _i32p, _f32p,
@@ -190,6 +193,33 @@ def _vm_cache(N, W, H, gx, gy, dt):
 
 _VM_ORDER = ("fb", "rects", "rgb", "rgb_sh_clamped", "depths", "points_xy_image", "inverse_filtered_cov3d",
              "filtered_masses", "tiles_touched", "point_offsets", "i_ranges", "remaining_transparency")
+
+
+def vr_forward(scene, cam, bg=None, cov_mult=1.0, want_list=False):
+    """vol_raster forward (float32).  Returns a dict of numpy outputs: the
+    framebuffer and the per-Gaussian preprocess, ranges and (optionally) the
+    sorted point list."""
+    L = lib()
+    N, W, H = scene.n, cam.width, cam.height
+    gx, gy = tiles(cam)
+    out = dict(fb=np.zeros((3, H, W), np.float32), rects=np.zeros((N, 2), np.int32), rgb=np.zeros((N, 3), np.float32),
+               clamped=np.zeros((N, 3), np.uint8), depths=np.zeros(N, np.float32), xy=np.zeros((N, 2), np.float32),
+               inverse_filtered_cov3d=np.zeros((N, 6), np.float32), filtered_masses=np.zeros(N, np.float32),
+               tiles_touched=np.zeros(N, np.int32), point_offsets=np.zeros(N, np.int32),
+               i_ranges=np.zeros((gx * gy, 2), np.int32))
+    args = _scene_args(scene, cam, np.float32, bg, cov_mult)
+    outs = [out[k] for k in ("fb", "rects", "rgb", "clamped", "depths", "xy", "inverse_filtered_cov3d",
+                             "filtered_masses", "tiles_touched", "point_offsets", "i_ranges")]
+    lst, cap = None, 0
+    if want_list:
+        P = L.orc_vr_forward_f32(*args, *outs, None, 0)
+        lst = np.zeros(max(P, 1), np.uint32)
+        cap = P
+    P = L.orc_vr_forward_f32(*args, *outs, lst.ctypes.data if lst is not None else None, cap)
+    out["n_pairs"] = P
+    if want_list:
+        out["point_list"] = lst[:P]
+    return out
 
 
 def vm_forward(scene, cam, bg=None, dtype=np.float32, cov_mult=1.0):
