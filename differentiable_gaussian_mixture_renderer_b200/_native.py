@@ -68,10 +68,10 @@ class SceneGrads(C.Structure):
                 ("rotations", C.c_void_p)]
 
 
-VR_RENDER_FULL, VR_RENDER_BINS, VR_RENDER_DEPTH = 0, 1, 2
+RENDER_FULL, RENDER_BINS, RENDER_DEPTH = 0, 1, 2
 
 
-class VrOptions(C.Structure):
+class RenderOptions(C.Structure):
     _fields_ = [("render_mode", C.c_int32), ("debug_bin", C.c_int32), ("max_depth", C.c_double)]
 
 
@@ -106,13 +106,16 @@ _SIGNATURES = {
     "dgmr_vr_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "dgmr_vr_pair_workspace_size": (C.c_size_t, [C.c_int32, C.c_int64]),
     "dgmr_vr_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
-    "dgmr_vr_forward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VrOptions), C.c_void_p, C.c_void_p, C.c_size_t,
+    "dgmr_vr_forward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderOptions), C.c_void_p, C.c_void_p, C.c_size_t,
                                   C.c_void_p, C.c_size_t, C.c_int64, C.c_void_p, C.c_void_p]),
     "dgmr_vm_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
     "dgmr_vm_forward_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p,
                                              C.c_size_t, C.c_void_p, C.c_void_p]),
     "dgmr_vm_forward_render": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_int64,
                                          C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "dgmr_vm_forward_render_options": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderOptions),
+                                                 C.POINTER(VmCache), C.c_int64, C.c_void_p, C.c_size_t, C.c_void_p,
+                                                 C.c_void_p]),
     "dgmr_vm_backward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                    C.c_void_p, C.c_void_p]),

@@ -49,8 +49,15 @@ def _contig(t):
     return t if t.is_contiguous() else t.contiguous()
 
 
+_MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
+
+
 def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
-            background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int):
+            background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
+            render_mode: str = "full", debug_render_bin: int = -1, max_depth: float = 20.0):
+    """``render_mode`` / ``debug_render_bin`` / ``max_depth`` are
+    vol_marcher::ForwardData's debug fields (vol_marcher.h:48-56), which the
+    reference's Python binding leaves at their defaults (Full, -1, 20)."""
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -89,7 +96,10 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
         cache[11] = torch.empty((n_pairs,), dtype=torch.int32, **opt)
         c.b_point_list = N.ptr(cache[11]) if n_pairs > 0 else None
         ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, n_pairs, dcode), dtype=torch.uint8, **opt)
-        N.check(lib.dgmr_vm_forward_render(scene, cam, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
+        if render_mode not in _MODES:
+            raise ValueError(f"render_mode must be one of {sorted(_MODES)}")
+        opts = N.RenderOptions(_MODES[render_mode], int(debug_render_bin), float(max_depth))
+        N.check(lib.dgmr_vm_forward_render_options(scene, cam, opts, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
                 "vol_marcher forward render")
     return cache
 

@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, 
     V3<T> colour = { T(0), T(0), T(0) };
     T tr = T(1);
     T start = T(0);
+    T distance = T(0); // Depth mode
     SectionSet<kLargeSteps, T> sec;
     for (unsigned step = 0;; ++step) {
         if (step >= kMaxLargeSteps) {
@@ -310,16 +311,37 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, 
         __syncwarp();
         Bin<T> acc[kRayRounds];
         warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
-        warp_store_bins(sm.bins, acc, lane, true);
-        // math.h:412-428, identical on every lane
-        for (unsigned k = 0; k < kBins; ++k) {
-            const Bin<T> bk = sm.bins[k];
-            colour.x = colour.x + bk.r * tr;
-            colour.y = colour.y + bk.g * tr;
-            colour.z = colour.z + bk.b * tr;
-            tr = tr * bk.m;
-            if (tr < T(1. / 255.))
-                break;
+        warp_store_bins(sm.bins, acc, lane, a.mode != DGMR_RENDER_BINS);
+        if (a.mode == DGMR_RENDER_FULL) {
+            // math.h:412-428, identical on every lane
+            for (unsigned k = 0; k < kBins; ++k) {
+                const Bin<T> bk = sm.bins[k];
+                colour.x = colour.x + bk.r * tr;
+                colour.y = colour.y + bk.g * tr;
+                colour.z = colour.z + bk.b * tr;
+                tr = tr * bk.m;
+                if (tr < T(1. / 255.))
+                    break;
+            }
+        } else if (a.mode == DGMR_RENDER_BINS) {
+            // vol_marcher_forward.cu:453-465: the sum of one bin's four channels
+            const Bin<T> bk = sm.bins[min(unsigned(a.debug_bin), kBins - 1)];
+            const T mass = ((bk.r + bk.g) + bk.b) + bk.m;
+            colour = { mass * a.max_depth, mass * a.max_depth, mass * a.max_depth };
+            if (mass == T(0))
+                colour = { T(0), T(1), T(0) };
+            if (dgmr_fm::isnan_f(mass))
+                colour = { T(1), T(0), T(0.5) };
+            if (mass < T(0))
+                colour = { T(1), T(0), T(0) };
+            tr = T(0);
+        } else {
+            // vol_marcher_forward.cu:466-481: the distance marched so far
+            for (unsigned k = 0; k < kBins; ++k)
+                tr = tr * sm.bins[k].m;
+            distance = max_f(sec.hi, distance);
+            const T dd = distance / a.max_depth;
+            colour = { dd, dd, dd };
         }
         const bool done = sec.n == 0 || tr < T(1.f / 255.f);
         start = sm.borders[kSmallSteps - 1];

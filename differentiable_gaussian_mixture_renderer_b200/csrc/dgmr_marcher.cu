@@ -206,6 +206,9 @@ struct VmMarch {
     T* g_centroids; // backward only: [N,3]
     uint32_t* stats;
     ConstSamplesT<T> cs;
+    int mode; // dgmr_render_mode (forward)
+    int debug_bin;
+    T max_depth;
 };
 
 // Which Gaussians of the tile list a ray can use.  Both passes of every large
@@ -381,7 +384,7 @@ dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dg
 
 template <class T>
 dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* c, int64_t cap64, void* workspace, size_t workspace_bytes,
-    dgmr_frame_stats* stats, cudaStream_t s)
+    dgmr_frame_stats* stats, cudaStream_t s, const dgmr_render_options* options)
 {
     const uint32_t N = uint32_t(scene->n_gaussians), cap = uint32_t(cap64);
     const VmLayout<T> L = vm_layout<T>(N, cap, workspace);
@@ -411,6 +414,9 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.remaining_T = static_cast<T*>(c->remaining_transparency);
     a.stats = st_dev;
     a.cs = const_samples<T>();
+    a.mode = options ? options->render_mode : DGMR_RENDER_FULL;
+    a.debug_bin = options ? options->debug_bin : -1;
+    a.max_depth = options ? T(options->max_depth) : T(20);
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
     k_vm_march_warp<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
     note_launch();
@@ -495,18 +501,26 @@ dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camer
     return vm_preprocess<float>(scene, camera, cache, workspace, workspace_bytes, stats, s);
 }
 
-dgmr_status dgmr_vm_forward_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace,
-    size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
+dgmr_status dgmr_vm_forward_render_options(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options,
+    dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
 {
     dgmr_status st = check_scene(scene, camera, -1);
     if (st != DGMR_OK)
         return st;
     if (!cache_ok(cache, pair_capacity > 0) || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
         return DGMR_ERR_BAD_ARG;
+    if (options && options->render_mode != DGMR_RENDER_FULL && options->render_mode != DGMR_RENDER_BINS && options->render_mode != DGMR_RENDER_DEPTH)
+        return DGMR_ERR_BAD_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (scene->dtype == DGMR_F64)
-        return vm_render<double>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s);
-    return vm_render<float>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s);
+        return vm_render<double>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s, options);
+    return vm_render<float>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s, options);
+}
+
+dgmr_status dgmr_vm_forward_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace,
+    size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    return dgmr_vm_forward_render_options(scene, camera, nullptr, cache, pair_capacity, workspace, workspace_bytes, stats, stream);
 }
 
 dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* cache, const void* grad_framebuffer, void* grad_sh,

@@ -169,7 +169,7 @@ struct VrRender {
     float* fb;
     uint32_t N, cap;
     uint32_t* stats;
-    int mode; // dgmr_vr_render_mode
+    int mode; // dgmr_render_mode
     int debug_bin;
     float max_depth;
 };
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kVrThreads) k_vr_render(VrRender a, CameraT<fl
     sizer.finalise();
     float res[3] = { 0.f, 0.f, 0.f };
     float transparency = 1.f; // of the final colour: 1 in Full and Bins mode, 0 in Depth mode
-    if (a.mode == DGMR_VR_RENDER_FULL) {
+    if (a.mode == DGMR_RENDER_FULL) {
         // pass B: bin masses and border values of every Gaussian of the tile
         float bin_mass[kVrBins][4];
         float bin_eval[kVrBins + 1][4];
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kVrThreads) k_vr_render(VrRender a, CameraT<fl
                 t = t + dt;
             }
         }
-    } else if (a.mode == DGMR_VR_RENDER_DEPTH) {
+    } else if (a.mode == DGMR_RENDER_DEPTH) {
         // vol_raster_forward.cu:495-507
         const unsigned bin = min(unsigned(a.debug_bin), kVrBins - 1);
         const float distance = sizer.end_of(bin);
@@ -452,13 +452,13 @@ dgmr_status dgmr_vr_preprocess(const dgmr_scene* scene, const dgmr_camera* camer
     return launch_status();
 }
 
-dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vr_options* options, float* framebuffer, void* frame_workspace,
+dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options, float* framebuffer, void* frame_workspace,
     size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
 {
     if (vr_bad(scene, camera, pair_capacity) || !framebuffer || !frame_workspace || (pair_capacity > 0 && !pair_workspace))
         return DGMR_ERR_BAD_ARG;
-    const int mode = options ? options->render_mode : DGMR_VR_RENDER_FULL;
-    if (mode != DGMR_VR_RENDER_FULL && mode != DGMR_VR_RENDER_BINS && mode != DGMR_VR_RENDER_DEPTH)
+    const int mode = options ? options->render_mode : DGMR_RENDER_FULL;
+    if (mode != DGMR_RENDER_FULL && mode != DGMR_RENDER_BINS && mode != DGMR_RENDER_DEPTH)
         return DGMR_ERR_BAD_ARG;
     const uint32_t N = uint32_t(scene->n_gaussians), cap = uint32_t(pair_capacity);
     VrLayout L = vr_layout(N, uint32_t(camera->width), uint32_t(camera->height), cap, frame_workspace, pair_workspace);

@@ -12,7 +12,7 @@ import torch
 
 from . import _native as N
 
-_MODES = {"full": N.VR_RENDER_FULL, "bins": N.VR_RENDER_BINS, "depth": N.VR_RENDER_DEPTH}
+_MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
 
 
 def forward(sh, weights, centroids, scales, rotations, view, proj, campos, background, width: int, height: int,
@@ -37,7 +37,7 @@ def forward(sh, weights, centroids, scales, rotations, view, proj, campos, backg
     with torch.cuda.device(dev):
         scene = N.make_scene(sh, weights, centroids, scales, rotations, sh_degree)
         cam = N.make_camera(view, proj, campos, background, W, H, tan_fovx, tan_fovy, cov_scale_multiplier)
-        opts = N.VrOptions(_MODES[render_mode], int(debug_bin), float(max_depth))
+        opts = N.RenderOptions(_MODES[render_mode], int(debug_bin), float(max_depth))
         s = N.stream_handle(stream)
         stats = torch.zeros(4, dtype=torch.int32, device=dev)
         frame_ws = torch.empty(max(1, lib.dgmr_vr_frame_workspace_size(n, W, H)), dtype=torch.uint8, device=dev)

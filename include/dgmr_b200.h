@@ -213,23 +213,25 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
  * pair count in stats->n_pairs for callers that size the pair workspace from
  * the frame.  An empty frame renders the background (the reference leaves the
  * framebuffer unwritten). */
-typedef enum dgmr_vr_render_mode {
-    DGMR_VR_RENDER_FULL = 0, /* RenderMode::Full */
-    DGMR_VR_RENDER_BINS = 1, /* RenderMode::Bins (the reference draws nothing: background) */
-    DGMR_VR_RENDER_DEPTH = 2, /* RenderMode::Depth: end of debug_bin / max_depth */
-} dgmr_vr_render_mode;
+typedef enum dgmr_render_mode {
+    DGMR_RENDER_FULL = 0, /* RenderMode::Full */
+    DGMR_RENDER_BINS = 1, /* RenderMode::Bins (vol_raster: nothing drawn, background; marcher: one bin's sum) */
+    DGMR_RENDER_DEPTH = 2, /* RenderMode::Depth (vol_raster: end of debug_bin; marcher: distance marched), over max_depth */
+} dgmr_render_mode;
 
-typedef struct dgmr_vr_options { /* VolRasterForwardData's debug fields; NULL = Full */
-    int32_t render_mode;
+/* The debug fields of VolRasterForwardData (vol_raster_forward.h:46-54) and of
+ * vol_marcher::ForwardData (vol_marcher.h:48-56).  NULL options = Full. */
+typedef struct dgmr_render_options {
+    int32_t render_mode; /* dgmr_render_mode */
     int32_t debug_bin; /* -1 = last bin */
     double max_depth; /* 20 in the reference */
-} dgmr_vr_options;
+} dgmr_render_options;
 
 size_t dgmr_vr_frame_workspace_size(int32_t n_gaussians, int32_t width, int32_t height);
 size_t dgmr_vr_pair_workspace_size(int32_t n_gaussians, int64_t pair_capacity);
 dgmr_status dgmr_vr_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, void* frame_workspace, size_t frame_workspace_bytes,
     dgmr_frame_stats* stats, dgmr_stream stream);
-dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vr_options* options, float* framebuffer, void* frame_workspace,
+dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options, float* framebuffer, void* frame_workspace,
     size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
 
 /* ---------------------------------------------------------- vol_marcher */
@@ -266,6 +268,13 @@ dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camer
  * i_ranges, then the ray march into framebuffer and remaining_transparency. */
 dgmr_status dgmr_vm_forward_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace,
     size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* dgmr_vm_forward_render with the reference's debug render modes
+ * (vol_marcher_forward.cu:448-482): Full, Bins (the sum of one bin's channels
+ * of the first large step, times max_depth) or Depth (distance marched over
+ * max_depth).  options = NULL is Full. */
+dgmr_status dgmr_vm_forward_render_options(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options,
+    dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream);
 
 /* Replaces dgmr::vol_marcher::backward<T> (vol_marcher_backward.cu:53-386).
  * grad_framebuffer [3,H,W] T.  Grads are written (not accumulated): sh

@@ -53,6 +53,14 @@ struct ConstSamples {
 };
 ConstSamples g_const_samples;
 
+// The marcher's debug render mode (vol_marcher.h:48-56): 0 Full, 1 Bins, 2 Depth.
+struct RenderMode {
+    int mode = 0;
+    int bin = -1;
+    double max_depth = 20.0;
+};
+RenderMode g_render_mode;
+
 template <class T>
 struct SceneIn {
     int N;
@@ -531,6 +539,7 @@ void vm_march(const SceneIn<T>& s, const int32_t* list, VmCache<T>& c, int32_t* 
                 T start = T(0);
                 V3<T> colour = { 0, 0, 0 };
                 T Tr = T(1);
+                T distance = T(0);
                 for (unsigned step = 0;; ++step) {
                     if (step >= MAX_LARGE_STEPS) {
 #pragma omp atomic write
@@ -543,7 +552,27 @@ void vm_march(const SceneIn<T>& s, const int32_t* list, VmCache<T>& c, int32_t* 
                     sample<N_SMALL>(sections, borders);
                     std::fill(bins.begin(), bins.end(), Bin4<T> { 0, 0, 0, 0 });
                     fill_bins(ray, list, b, e, s.centroids, c.inv_cov, c.masses, c.rgb, borders, bins.data());
-                    integrate_bins<T, N_SMALL - 1>(colour, Tr, bins.data());
+                    if (g_render_mode.mode == 1) { // vol_marcher_forward.cu:453-465
+                        const Bin4<T>& bk = bins[std::min(unsigned(g_render_mode.bin), N_SMALL - 2)];
+                        const T mass = ((bk.r + bk.g) + bk.b) + bk.m;
+                        const T md = T(g_render_mode.max_depth);
+                        colour = { mass * md, mass * md, mass * md };
+                        if (mass == T(0))
+                            colour = { T(0), T(1), T(0) };
+                        if (dgmr_fm::isnan_f(mass))
+                            colour = { T(1), T(0), T(0.5) };
+                        if (mass < T(0))
+                            colour = { T(1), T(0), T(0) };
+                        Tr = T(0);
+                    } else if (g_render_mode.mode == 2) { // vol_marcher_forward.cu:466-481
+                        for (unsigned k = 0; k < N_SMALL - 1; ++k)
+                            Tr = Tr * dgmr_fm::exp_f(-bins[k].m);
+                        distance = max_f(sections.end(), distance);
+                        const T dd = distance / T(g_render_mode.max_depth);
+                        colour = { dd, dd, dd };
+                    } else {
+                        integrate_bins<T, N_SMALL - 1>(colour, Tr, bins.data());
+                    }
                     if (sections.size() == 0 || Tr < T(1.f / 255.f))
                         break;
                     start = borders[N_SMALL - 1];
@@ -1374,6 +1403,14 @@ void orc_set_num_threads(int n)
 }
 
 uint32_t orc_higher_msb(uint32_t n) { return higher_msb(n); }
+
+// the marcher's debug render mode for the following vol_marcher forwards (0 Full, 1 Bins, 2 Depth)
+void orc_set_render_mode(int mode, int bin, double max_depth)
+{
+    g_render_mode.mode = mode;
+    g_render_mode.bin = bin;
+    g_render_mode.max_depth = max_depth;
+}
 
 // n fixed (start, end, delta_t) sections for the marcher's gradient-check mode; n = 0 turns it off
 void orc_set_const_samples(int n, const double* sections)

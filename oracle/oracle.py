@@ -88,6 +88,8 @@ def _declare(L):
         f = getattr(L, f"orc_density_randomised_{sfx}")
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.orc_set_render_mode.restype = None
+    L.orc_set_render_mode.argtypes = [C.c_int, C.c_int, C.c_double]
     L.orc_set_const_samples.restype = None
     L.orc_set_const_samples.argtypes = [C.c_int, _f64p]
     L.orc_fmath_f32.restype = None
@@ -222,10 +224,11 @@ def vr_forward(scene, cam, bg=None, cov_mult=1.0, want_list=False):
     return out
 
 
-def vm_forward(scene, cam, bg=None, dtype=np.float32, cov_mult=1.0):
+def vm_forward(scene, cam, bg=None, dtype=np.float32, cov_mult=1.0, render_mode=0, debug_bin=-1, max_depth=20.0):
     """vol_marcher forward.  Returns the reference's 13-entry cache as a dict
-    (plus 'keys' and 'status')."""
+    (plus 'keys' and 'status').  render_mode: 0 Full, 1 Bins, 2 Depth."""
     L = lib()
+    L.orc_set_render_mode(int(render_mode), int(debug_bin), float(max_depth))
     sfx = "f32" if dtype == np.float32 else "f64"
     N, W, H = scene.n, cam.width, cam.height
     gx, gy = tiles(cam)

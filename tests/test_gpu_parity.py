@@ -150,6 +150,26 @@ def test_vol_marcher_forward_matches_oracle(cuda, dtype, n, w, h, seed):
     assert np.abs(got["remaining_transparency"] - ref["remaining_transparency"]).max() <= IMAGE_TOL
 
 
+@pytest.mark.parametrize("mode,code", [("bins", 1), ("depth", 2)])
+def test_vol_marcher_debug_modes_match_oracle(cuda, mode, code):
+    """vol_marcher_forward.cu:448-482: Bins (one bin's channel sum of the first
+    large step) and Depth (distance marched, inf while the section set is open)."""
+    sc = S.make_scene(20000, seed=6, sh_degree=0)
+    cam = S.make_camera(40, 32, eye=(0.1, -0.2, -3.0))
+    ref = O.vm_forward(sc, cam, render_mode=code, debug_bin=30, max_depth=10.0)
+    O.vm_forward(sc, cam)  # back to Full for the other tests
+    shs, w, mu, s, q = to_dev(sc, cuda, torch.float32)
+    view, proj, campos, bgt = cam_tensors(cam, cuda, torch.float32, (0.0, 0.0, 0.0))
+    cache = cpp_binding.forward(shs, w, mu, s, q, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx,
+                                cam.tan_fovy, sc.sh_degree, render_mode=mode, debug_render_bin=30, max_depth=10.0)
+    got = cache[0].cpu().numpy()
+    np.testing.assert_array_equal(np.isinf(got), np.isinf(ref["fb"]))
+    fin = np.isfinite(ref["fb"])
+    if fin.any():
+        assert np.abs(got[fin] - ref["fb"][fin]).max() <= IMAGE_TOL
+    np.testing.assert_array_equal(cache[12].cpu().numpy(), ref["remaining_transparency"])
+
+
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 def test_vol_marcher_backward_matches_oracle(cuda, dtype):
     npdt = np.float32 if dtype == torch.float32 else np.float64
