@@ -24,7 +24,24 @@ class DgmrError(RuntimeError):
 class Scene(C.Structure):
     _fields_ = [("n_gaussians", C.c_int32), ("sh_stride", C.c_int32), ("sh_degree", C.c_int32), ("dtype", C.c_int32),
                 ("centroids", C.c_void_p), ("sh", C.c_void_p), ("weights", C.c_void_p), ("scales", C.c_void_p),
-                ("rotations", C.c_void_p)]
+                ("rotations", C.c_void_p), ("formulation", C.c_int32), ("reserved", C.c_int32)]
+
+
+# dgmr_formulation codes (types.h:26-32 plus 1; 0 keeps each renderer's reference default)
+FORMULATIONS = {None: 0, "opacity": 1, "mass": 2, "density": 3, "ots": 4, "ols": 5}
+
+
+def formulation_code(f) -> int:
+    """Maps a formulation name (or None for the renderer's default, or a code)
+    to its dgmr_formulation value; raises ValueError for anything else."""
+    if isinstance(f, int) and not isinstance(f, bool):
+        if 0 <= f <= 5:
+            return f
+    elif f is None or isinstance(f, str):
+        key = f.lower() if isinstance(f, str) else f
+        if key in FORMULATIONS:
+            return FORMULATIONS[key]
+    raise ValueError(f"unknown formulation {f!r}: one of opacity, mass, density, ots, ols")
 
 
 class Camera(C.Structure):
@@ -183,8 +200,9 @@ def dtype_code(dtype: torch.dtype) -> int:
     raise TypeError("All input tensors must be of the same type (float32 or float64)")
 
 
-def make_scene(shs, weights, centroids, scales, rotations, sh_degree: int) -> Scene:
+def make_scene(shs, weights, centroids, scales, rotations, sh_degree: int, formulation=None) -> Scene:
     s = Scene()
+    s.formulation = formulation_code(formulation)
     s.n_gaussians = int(centroids.shape[0])
     s.sh_stride = int(shs.shape[1])
     s.sh_degree = int(sh_degree)

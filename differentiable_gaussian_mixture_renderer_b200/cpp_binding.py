@@ -54,10 +54,14 @@ _MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
 
 def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
             background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
-            render_mode: str = "full", debug_render_bin: int = -1, max_depth: float = 20.0):
+            render_mode: str = "full", debug_render_bin: int = -1, max_depth: float = 20.0,
+            formulation: str | None = None):
     """``render_mode`` / ``debug_render_bin`` / ``max_depth`` are
     vol_marcher::ForwardData's debug fields (vol_marcher.h:48-56), which the
-    reference's Python binding leaves at their defaults (Full, -1, 20)."""
+    reference's Python binding leaves at their defaults (Full, -1, 20).
+    ``formulation`` (opacity, mass, density, ots, ols) replaces the compile-time
+    vol_marcher::config::gaussian_mixture_formulation (vol_marcher.h:66); None
+    keeps its Opacity.  backward must be given the same one."""
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -68,7 +72,7 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
     sh_params, weights, centroids = _contig(sh_params), _contig(weights), _contig(centroids)
     cov_scales, cov_rotations = _contig(cov_scales), _contig(cov_rotations)
     with torch.cuda.device(dev):
-        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree)
+        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree, formulation)
         cam = N.make_camera(view_matrix, proj_matrix, cam_position, background, W, H, _f32(tan_fovx), _f32(tan_fovy))
         gx, gy = (W + 15) // 16, (H + 15) // 16
         opt = dict(device=dev)
@@ -106,7 +110,7 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
 
 def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
              background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
-             grad_framebuffer, cache_vector):
+             grad_framebuffer, cache_vector, formulation: str | None = None):
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -121,7 +125,7 @@ def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matr
     grad_framebuffer = _contig(grad_framebuffer)
     cache = [_contig(t) if t is not None else None for t in cache_vector]
     with torch.cuda.device(dev):
-        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree)
+        scene = N.make_scene(sh_params, weights, centroids, cov_scales, cov_rotations, sh_degree, formulation)
         cam = N.make_camera(view_matrix, proj_matrix, cam_position, background, W, H, _f32(tan_fovx), _f32(tan_fovy))
         opt = dict(device=dev, dtype=dt)
         k = int(sh_params.shape[1])

@@ -25,7 +25,17 @@ inline dgmr_status check_scene(const dgmr_scene* scene, const dgmr_camera* camer
     if (scene->n_gaussians > 0
         && (!scene->centroids || !scene->sh || !scene->weights || !scene->scales || !scene->rotations))
         return DGMR_ERR_BAD_ARG;
+    if (scene->formulation < DGMR_FORMULATION_DEFAULT || scene->formulation > DGMR_FORMULATION_OLS)
+        return DGMR_ERR_BAD_ARG;
     return DGMR_OK;
+}
+
+// the scene's formulation, or the renderer's reference default
+inline Formulation scene_formulation(const dgmr_scene* scene, Formulation renderer_default)
+{
+    if (!scene || scene->formulation == DGMR_FORMULATION_DEFAULT)
+        return renderer_default;
+    return Formulation(scene->formulation - 1);
 }
 
 // glm::inverse of a 4x4 (glm layout) by cofactors, evaluated in double

@@ -140,11 +140,13 @@ __device__ __forceinline__ void grad_compute_cov(V3<T> s, T qw, T qx, T qy, T qz
     gq[3] += gz;
 }
 
-// Adjoint of splat_project<Ots> for one Gaussian (grad/math.h:333-527 with the
-// derivative of the 1.3*tanfov clamp limits w.r.t. view depth included).
+// Adjoint of splat_project for one Gaussian (grad/math.h:333-527 with the
+// derivative of the fov clamp limits w.r.t. t.z included), every formulation.
+// g_w2, g_xy, g_cov: adjoints of the screen-space weight, centroid and
+// (filtered) covariance.
 template <class T>
-__device__ __forceinline__ void grad_splat_ots(T weight, V3<T> mu, V3<T> s, T qw, T qx, T qy, T qz, const CameraT<T>& cam, T filter, T g_w2, V2<T> g_xy,
-    S2<T> g_cov, T* g_weight, V3<T>* g_mu, V3<T>* g_s, T* g_q)
+__device__ __forceinline__ void grad_splat(Formulation f, T weight, V3<T> mu, V3<T> s, T qw, T qx, T qy, T qz, const CameraT<T>& cam, T filter, T g_w2,
+    V2<T> g_xy, S2<T> g_cov, T* g_weight, V3<T>* g_mu, V3<T>* g_s, T* g_q)
 {
     const V4<T> tu = mat4_point(cam.view, mu);
     const T lim_x = (T(1.3) * cam.tan_fovx) * tu.z;
@@ -156,24 +158,54 @@ __device__ __forceinline__ void grad_splat_ots(T weight, V3<T> mu, V3<T> s, T qw
     const M3<T> Tm = matmul3(SJ, W);
     const M3<T> R = quat_to_mat3(qw, qx, qy, qz);
     const S3<T> cov3 = compute_cov(s, R);
-    S2<T> cov2 = affine_transform_and_cut(cov3, Tm);
+    const S2<T> c = affine_transform_and_cut(cov3, Tm); // before the filter
+    S2<T> cov2 = c;
     cov2.v[0] = cov2.v[0] + filter;
     cov2.v[2] = cov2.v[2] + filter;
     const T detSJ = det3(SJ);
-    const V2<T> l2 = larger2(s);
-    const T i2p = (two_pi<T>() * l2.x) * l2.y;
-    const T dc = det2(cov2);
-    const T i2 = integrate_exponential_cov2(cov2);
-    *g_weight = *g_weight + g_w2 * detSJ * i2p / i2;
-    const T g_detSJ = g_w2 * weight * i2p / i2;
-    const T g_i2p = g_w2 * weight * detSJ / i2;
-    const T g_i2 = -g_w2 * weight * detSJ * i2p / (i2 * i2);
-    const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dc)) : T(0);
-    g_cov.v[0] = g_cov.v[0] + g_dc * cov2.v[2];
-    g_cov.v[1] = g_cov.v[1] - g_dc * T(2) * cov2.v[1];
-    g_cov.v[2] = g_cov.v[2] + g_dc * cov2.v[0];
-    const V2<T> g_l2 = { g_i2p * two_pi<T>() * l2.y, g_i2p * two_pi<T>() * l2.x };
-    *g_s = add3(*g_s, grad_larger2(s, g_l2));
+    T g_detSJ = T(0);
+    if (f == Formulation::Opacity) {
+        // weight2d = w sqrt(max(eps, det c / det(c + filter)))
+        const T dcv = det2(c), dn = det2(cov2);
+        const T r = dcv / dn;
+        const T factor = dgmr_fm::sqrt_f(max_f(T(0.000025), r));
+        *g_weight = *g_weight + g_w2 * factor;
+        if (T(0.000025) < r) {
+            const T g_r = (g_w2 * weight) / (T(2) * factor);
+            const T g_dc = g_r / dn;
+            const T g_dn = -g_r * dcv / (dn * dn);
+            g_cov.v[0] = (g_cov.v[0] + g_dc * c.v[2]) + g_dn * cov2.v[2];
+            g_cov.v[1] = (g_cov.v[1] - g_dc * T(2) * c.v[1]) - g_dn * T(2) * cov2.v[1];
+            g_cov.v[2] = (g_cov.v[2] + g_dc * c.v[0]) + g_dn * cov2.v[0];
+        }
+    } else {
+        // weight2d = w detSJ A(s) / i2(cov2), A = 1 (Mass), i3(s) (Density), i2(larger / smaller two scales) (Ots / Ols)
+        T A = T(1);
+        if (f == Formulation::Density)
+            A = integrate_exponential3(s);
+        else if (f == Formulation::Ots)
+            A = integrate_exponential2(larger2(s));
+        else if (f == Formulation::Ols)
+            A = integrate_exponential2(smaller2(s));
+        const T dc = det2(cov2);
+        const T i2 = integrate_exponential_cov2(cov2);
+        *g_weight = *g_weight + g_w2 * detSJ * A / i2;
+        g_detSJ = g_w2 * weight * A / i2;
+        const T g_A = g_w2 * weight * detSJ / i2;
+        const T g_i2 = -g_w2 * weight * detSJ * A / (i2 * i2);
+        const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dc)) : T(0);
+        g_cov.v[0] = g_cov.v[0] + g_dc * cov2.v[2];
+        g_cov.v[1] = g_cov.v[1] - g_dc * T(2) * cov2.v[1];
+        g_cov.v[2] = g_cov.v[2] + g_dc * cov2.v[0];
+        if (f == Formulation::Density) {
+            const T k = g_A * two_pi_pow_1_5<T>();
+            *g_s = add3(*g_s, V3<T> { k * s.y * s.z, k * s.x * s.z, k * s.x * s.y });
+        } else if (f == Formulation::Ots || f == Formulation::Ols) {
+            const V2<T> l2 = f == Formulation::Ots ? larger2(s) : smaller2(s);
+            const V2<T> g_l2 = { g_A * two_pi<T>() * l2.y, g_A * two_pi<T>() * l2.x };
+            *g_s = add3(*g_s, f == Formulation::Ots ? grad_larger2(s, g_l2) : grad_smaller2(s, g_l2));
+        }
+    }
     M3<T> g_SJ = cofactor3(SJ);
 #pragma unroll
     for (int i = 0; i < 3; ++i)

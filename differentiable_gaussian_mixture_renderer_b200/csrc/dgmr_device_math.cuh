@@ -235,6 +235,12 @@ __device__ __forceinline__ constexpr T two_pi_pow_1_5() { return T(15.7496099457
 template <class T>
 __device__ __forceinline__ T integrate_exponential_cov2(const S2<T>& c) { return two_pi<T>() * dgmr_fm::sqrt_f(det2(c)); }
 
+// math.h:76-87: integral of the unnormalised Gaussian with these standard deviations
+template <class T>
+__device__ __forceinline__ T integrate_exponential2(V2<T> s) { return (two_pi<T>() * s.x) * s.y; }
+template <class T>
+__device__ __forceinline__ T integrate_exponential3(V3<T> s) { return ((two_pi_pow_1_5<T>() * s.x) * s.y) * s.z; }
+
 // math.h:112-133
 template <class T>
 __device__ __forceinline__ V2<T> larger2(V3<T> v)
@@ -256,6 +262,32 @@ __device__ __forceinline__ V3<T> grad_larger2(V3<T> v, V2<T> g)
             return { T(0), g.x, g.y };
     } else {
         if (v.y < v.z)
+            return { g.x, T(0), g.y };
+    }
+    return { g.x, g.y, T(0) };
+}
+
+// math.h:136-155
+template <class T>
+__device__ __forceinline__ V2<T> smaller2(V3<T> v)
+{
+    if (v.x > v.y) {
+        if (v.x > v.z)
+            return { v.y, v.z };
+    } else {
+        if (v.y > v.z)
+            return { v.x, v.z };
+    }
+    return { v.x, v.y };
+}
+template <class T>
+__device__ __forceinline__ V3<T> grad_smaller2(V3<T> v, V2<T> g)
+{
+    if (v.x > v.y) {
+        if (v.x > v.z)
+            return { T(0), g.x, g.y };
+    } else {
+        if (v.y > v.z)
             return { g.x, T(0), g.y };
     }
     return { g.x, g.y, T(0) };
@@ -285,12 +317,16 @@ struct Gaussian2d {
     S2<T> cov;
 };
 
-enum class Formulation : int { Opacity = 0, Ots = 3 };
+// types.h:26-32.  Which formulation a renderer uses is a compile-time choice in
+// the reference (splat and vol_raster: Ots, splat_forward.h:58 and
+// vol_raster_forward.h:66; vol_marcher: Opacity, vol_marcher.h:66); here it
+// is a per-call value with those defaults.
+enum class Formulation : int { Opacity = 0, Mass = 1, Density = 2, Ots = 3, Ols = 4 };
 
-// math.h:322-410 for the two formulations on the path: Ots (splat,
-// splat_forward.h:58) and Opacity (vol_marcher rect, vol_marcher.h:66)
-template <Formulation F, class T>
-__device__ __forceinline__ Gaussian2d<T> splat_project(T weight, V3<T> mu, V3<T> s, const M3<T>& R, const CameraT<T>& cam, T filter)
+// math.h:322-410: the screen-space Gaussian of one 3-D Gaussian, with the
+// 1.3 tan(fov) clamp of t (:334-340) and the formulation's weight
+template <class T>
+__device__ __forceinline__ Gaussian2d<T> splat_project(Formulation f, T weight, V3<T> mu, V3<T> s, const M3<T>& R, const CameraT<T>& cam, T filter)
 {
     const V4<T> tu = mat4_point(cam.view, mu);
     const T lim_x = (T(1.3) * cam.tan_fovx) * tu.z;
@@ -309,22 +345,46 @@ __device__ __forceinline__ Gaussian2d<T> splat_project(T weight, V3<T> mu, V3<T>
     }
     const S3<T> cov3 = compute_cov(s, R);
     g.cov = affine_transform_and_cut(cov3, Tm);
-    if constexpr (F == Formulation::Opacity) {
+    if (f == Formulation::Opacity) {
         S2<T> nc = g.cov;
         nc.v[0] = nc.v[0] + filter;
         nc.v[2] = nc.v[2] + filter;
         const T factor = dgmr_fm::sqrt_f(max_f(T(0.000025), det2(g.cov) / det2(nc)));
         g.cov = nc;
         g.weight = weight * factor;
+        return g;
+    }
+    g.cov.v[0] = g.cov.v[0] + filter;
+    g.cov.v[2] = g.cov.v[2] + filter;
+    const T detSJ = det3(SJ);
+    if (f == Formulation::Mass) {
+        g.weight = (weight * detSJ) * (T(1) / integrate_exponential_cov2(g.cov));
+    } else if (f == Formulation::Density) {
+        g.weight = ((weight * detSJ) * integrate_exponential3(s)) / integrate_exponential_cov2(g.cov);
     } else {
-        g.cov.v[0] = g.cov.v[0] + filter;
-        g.cov.v[2] = g.cov.v[2] + filter;
-        const T detSJ = det3(SJ);
-        const V2<T> l2 = larger2(s);
-        const T i2p = (two_pi<T>() * l2.x) * l2.y;
+        const T i2p = integrate_exponential2(f == Formulation::Ots ? larger2(s) : smaller2(s));
         g.weight = ((weight * detSJ) * i2p) / integrate_exponential_cov2(g.cov);
     }
     return g;
+}
+
+// math.h:298-320: mass of a Gaussian from its weight
+template <class T>
+__device__ __forceinline__ T weight_to_mass(Formulation f, T weight, V3<T> s, const S2<T>& cov2d)
+{
+    switch (f) {
+    case Formulation::Opacity:
+        return weight * integrate_exponential_cov2(cov2d);
+    case Formulation::Mass:
+        return weight;
+    case Formulation::Density:
+        return weight * integrate_exponential3(s);
+    case Formulation::Ots:
+        return weight * integrate_exponential2(larger2(s));
+    case Formulation::Ols:
+        return weight * integrate_exponential2(smaller2(s));
+    }
+    return T(0);
 }
 
 // SH constants, constants.h:26-43

@@ -88,6 +88,7 @@ struct VmPre {
     T* masses;
     uint32_t* tiles_touched;
     T aa; // filter_kernel_SD * 2 * tan_fovx / width
+    Formulation form;
 };
 
 // vol_marcher_forward.cu:98-176
@@ -128,10 +129,10 @@ __global__ void __launch_bounds__(128) k_vm_preprocess(VmPre<T> p, CameraT<T> ca
     filtered.v[0] = filtered.v[0] + fks2;
     filtered.v[3] = filtered.v[3] + fks2;
     filtered.v[5] = filtered.v[5] + fks2;
-    const T mass = w * integrate_exponential_cov2(affine_transform_and_cut(cov3, upper3(cam.view)));
+    const T mass = weight_to_mass(p.form, w, sc, affine_transform_and_cut(cov3, upper3(cam.view)));
     if (mass <= T(0))
         return;
-    const Gaussian2d<T> g = splat_project<Formulation::Opacity>(w, mu, sc, R, cam, T(kFilterSD * kFilterSD));
+    const Gaussian2d<T> g = splat_project(p.form, w, mu, sc, R, cam, T(kFilterSD * kFilterSD));
     const auto iso = [](T wt, T var, T isoline) {
         const T sv = T(-2) * dgmr_fm::log_f(isoline / wt);
         if (sv <= T(0))
@@ -256,6 +257,7 @@ struct VmBwdGauss {
     T* g_scales;
     T* g_rotations;
     T aa;
+    Formulation form;
 };
 
 // vol_marcher_backward.cu:321-384
@@ -295,7 +297,7 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     filtered.v[5] = filtered.v[5] + fks * fks;
     const M3<T> W3 = upper3(cam.view);
     const S2<T> cov2d = affine_transform_and_cut(cov3, W3);
-    const T mass = w * integrate_exponential_cov2(cov2d);
+    const T mass = weight_to_mass(p.form, w, sc, cov2d);
     if (mass <= T(0))
         return;
     const V3<T> dir = { delta.x / dist, delta.y / dist, delta.z / dist };
@@ -308,18 +310,35 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     for (int k = 0; k < 6; ++k)
         g_inv.v[k] = a[4 + k];
     const S3<T> g_filtered = grad_inverse_sym3(filtered, g_inv);
+    // adjoint of weight_to_mass (math.h:298-320)
     const T g_mass = a[0];
-    const T dcov = det2(cov2d);
-    const T i2 = integrate_exponential_cov2(cov2d);
-    const T g_w = g_mass * i2;
-    const T g_i2 = g_mass * w;
-    const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
-    const S2<T> g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
+    T g_w = T(0);
+    S2<T> g_cov2d = { { T(0), T(0), T(0) } };
+    V3<T> g_s = { T(0), T(0), T(0) };
+    if (p.form == Formulation::Opacity) {
+        const T dcov = det2(cov2d);
+        const T i2 = integrate_exponential_cov2(cov2d);
+        g_w = g_mass * i2;
+        const T g_i2 = g_mass * w;
+        const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
+        g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
+    } else if (p.form == Formulation::Mass) {
+        g_w = g_mass;
+    } else if (p.form == Formulation::Density) {
+        g_w = g_mass * integrate_exponential3(sc);
+        const T k = (g_mass * w) * two_pi_pow_1_5<T>();
+        g_s = { k * sc.y * sc.z, k * sc.x * sc.z, k * sc.x * sc.y };
+    } else {
+        const V2<T> l2 = p.form == Formulation::Ots ? larger2(sc) : smaller2(sc);
+        g_w = g_mass * integrate_exponential2(l2);
+        const T k = (g_mass * w) * two_pi<T>();
+        const V2<T> g_l2 = { k * l2.y, k * l2.x };
+        g_s = p.form == Formulation::Ots ? grad_larger2(sc, g_l2) : grad_smaller2(sc, g_l2);
+    }
     S3<T> g_cov3 = g_filtered;
     const T g_fks2 = (g_filtered.v[0] + g_filtered.v[3]) + g_filtered.v[5];
     g_dist = g_dist + (g_fks2 * T(2) * fks) * p.aa;
     grad_affine_transform_and_cut(cov3, W3, g_cov2d, &g_cov3, static_cast<M3<T>*>(nullptr));
-    V3<T> g_s = { T(0), T(0), T(0) };
     T g_q[4] = { T(0), T(0), T(0), T(0) };
     grad_compute_cov(sc, q[0], q[1], q[2], q[3], g_cov3, &g_s, g_q);
     g_mu = add3(g_mu, mul3(delta, g_dist / dist));
@@ -373,7 +392,8 @@ dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dg
     VmPre<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rects, static_cast<T*>(c->rgb),
         c->rgb_sh_clamped, static_cast<T*>(c->depths), static_cast<T*>(c->points_xy_image), static_cast<T*>(c->inverse_filtered_cov3d),
-        static_cast<T*>(c->filtered_masses), reinterpret_cast<uint32_t*>(c->tiles_touched), aa_multiplier(cam) };
+        static_cast<T*>(c->filtered_masses), reinterpret_cast<uint32_t*>(c->tiles_touched), aa_multiplier(cam),
+        scene_formulation(scene, Formulation::Opacity) };
     k_vm_preprocess<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
     note_launch();
     inclusive_scan_u32(reinterpret_cast<uint32_t*>(c->tiles_touched), reinterpret_cast<uint32_t*>(c->point_offsets), N, Lw.pre_scan_tmp, s);
@@ -458,7 +478,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
         c->tiles_touched, L.acc, static_cast<T*>(g_sh), static_cast<T*>(g_weights), static_cast<T*>(g_centroids), static_cast<T*>(g_scales),
-        static_cast<T*>(g_rotations), aa_multiplier(cam) };
+        static_cast<T*>(g_rotations), aa_multiplier(cam), scene_formulation(scene, Formulation::Opacity) };
     k_vm_bwd_gaussians<T><<<(N + 127) / 128, 128, 0, s>>>(p, cam);
     note_launch(2);
     return launch_status();

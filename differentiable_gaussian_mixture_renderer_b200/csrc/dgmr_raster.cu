@@ -80,6 +80,7 @@ struct VrPre {
     const float* rotations;
     VrLayout L;
     float aa; // filter size per unit distance
+    Formulation form;
 };
 
 // vol_raster_forward.cu:86-136
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(128) k_vr_preprocess(VrPre p, CameraT<float> c
     const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
     const float* q = p.rotations + 4 * size_t(i);
     const M3<float> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
-    const Gaussian2d<float> g = splat_project<Formulation::Ots>(w, mu, sc, R, cam, 0.3f);
+    const Gaussian2d<float> g = splat_project(p.form, w, mu, sc, R, cam, 0.3f);
     const S3<float> cov3 = compute_cov(sc, R);
     const V3<float> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const float fks = len3(sub3(mu, campos)) * p.aa;
@@ -122,9 +123,8 @@ __global__ void __launch_bounds__(128) k_vr_preprocess(VrPre p, CameraT<float> c
     filtered.v[0] = filtered.v[0] + fks2;
     filtered.v[3] = filtered.v[3] + fks2;
     filtered.v[5] = filtered.v[5] + fks2;
-    // weight_to_mass<Ots> of the scales plus the squared filter size (vol_raster_forward.cu:106)
-    const V2<float> l2 = larger2(V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 });
-    L.masses[i] = w * ((two_pi<float>() * l2.x) * l2.y);
+    // weight_to_mass of the scales plus the squared filter size (vol_raster_forward.cu:106)
+    L.masses[i] = weight_to_mass(p.form, w, V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 }, g.cov);
     const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
     const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
     L.rects[2 * i] = ex;
@@ -409,7 +409,7 @@ void vr_launch_preprocess(const dgmr_scene* scene, const CameraT<float>& cam, co
         return;
     VrPre p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L,
-        ((kVrFilterSD * cam.tan_fovx) * 2.f) / float(cam.W) };
+        ((kVrFilterSD * cam.tan_fovx) * 2.f) / float(cam.W), scene_formulation(scene, Formulation::Ots) };
     k_vr_preprocess<<<(N + 127) / 128, 128, 0, s>>>(p, cam);
     note_launch();
     inclusive_scan_u32(L.tiles_touched, L.point_offsets, N, L.bin.scan_tmp, s);

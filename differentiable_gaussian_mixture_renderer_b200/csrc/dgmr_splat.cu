@@ -90,6 +90,7 @@ struct SplatPre {
     uint32_t* depth_key;
     uint32_t* perm;
     float4* blend_rec;
+    Formulation form;
 };
 
 // splat_forward.cu:70-118 for Gaussian i of the scene, written to output
@@ -119,7 +120,7 @@ __device__ __forceinline__ void preprocess_one(const SplatPre& p, const CameraT<
     const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
     const float* q = p.rotations + 4 * size_t(i);
     const M3<float> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
-    const Gaussian2d<float> g = splat_project<Formulation::Ots>(w, mu, sc, R, cam, 0.3f);
+    const Gaussian2d<float> g = splat_project(p.form, w, mu, sc, R, cam, 0.3f);
     const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
     const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
     p.rects[2 * o] = ex;
@@ -518,6 +519,7 @@ struct SplatBwdGauss {
     float* g_centroids;
     float* g_scales;
     float* g_rotations;
+    Formulation form;
 };
 
 __device__ __forceinline__ void zero_gaussian_grads(const SplatBwdGauss& p, uint32_t i)
@@ -547,7 +549,7 @@ __device__ __forceinline__ void bwd_gaussian_one(const SplatBwdGauss& p, const C
     const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
     const float* q = p.rotations + 4 * size_t(i);
     const M3<float> R = quat_to_mat3(q[0], q[1], q[2], q[3]);
-    const Gaussian2d<float> g2 = splat_project<Formulation::Ots>(p.weights[i], mu, sc, R, cam, 0.3f);
+    const Gaussian2d<float> g2 = splat_project(p.form, p.weights[i], mu, sc, R, cam, 0.3f);
     const S2<float> M = inverse2(g2.cov);
     const float G00 = a[2], G01 = a[3] * 0.5f, G11 = a[4];
     // H = -M G M (2x2 symmetric)
@@ -560,7 +562,7 @@ __device__ __forceinline__ void bwd_gaussian_one(const SplatBwdGauss& p, const C
     float g_weight = 0.f;
     V3<float> g_mu = { 0.f, 0.f, 0.f }, g_s = { 0.f, 0.f, 0.f };
     float g_q[4] = { 0.f, 0.f, 0.f, 0.f };
-    grad_splat_ots(p.weights[i], mu, sc, q[0], q[1], q[2], q[3], cam, 0.3f, a[5], V2<float> { a[0], a[1] }, g_cov, &g_weight, &g_mu, &g_s, g_q);
+    grad_splat(p.form, p.weights[i], mu, sc, q[0], q[1], q[2], q[3], cam, 0.3f, a[5], V2<float> { a[0], a[1] }, g_cov, &g_weight, &g_mu, &g_s, g_q);
     const V3<float> campos = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<float> v = sub3(mu, campos);
     const float vl = dgmr_fm::sqrt_f(dot3(v, v));
@@ -605,7 +607,8 @@ SplatPre make_pre(const dgmr_scene* scene, const SplatLayout& L)
 {
     return SplatPre { uint32_t(scene->n_gaussians), static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride,
         scene->sh_degree, static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations),
-        L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm, L.blend_rec };
+        L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched, L.bin.depth_key, L.bin.perm, L.blend_rec,
+        scene_formulation(scene, Formulation::Ots) };
 }
 
 SingleFrame single_frame(const CameraT<float>& cam, float* fb, const SplatLayout& L, const float* grad_fb = nullptr)
@@ -785,7 +788,7 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
         single_frame(cam, nullptr, L, grad_framebuffer));
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
-        L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations };
+        L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, scene_formulation(scene, Formulation::Ots) };
     k_splat_bwd_gaussians<<<(N + 127) / 128, 128, 0, s>>>(p, cam);
     note_launch(2);
     return launch_status();
@@ -822,6 +825,7 @@ struct BatchScene {
     uint32_t n;
     int sh_stride, sh_degree;
     uint32_t view_begin, view_end; // range in BatchTable::view_by_scene
+    Formulation form;
     float* g_sh;
     float* g_weights;
     float* g_centroids;
@@ -893,6 +897,7 @@ __global__ void __launch_bounds__(256) k_batch_preprocess(SplatPre out, const __
     p.weights = sc.weights;
     p.scales = sc.scales;
     p.rotations = sc.rotations;
+    p.form = sc.form;
     preprocess_one(p, bv.cam, g - tab.g_off[v], g);
 }
 
@@ -922,6 +927,7 @@ __global__ void __launch_bounds__(128) k_batch_bwd_gaussians(SplatBwdGauss state
     p.g_centroids = sc.g_centroids;
     p.g_scales = sc.g_scales;
     p.g_rotations = sc.g_rotations;
+    p.form = sc.form;
     zero_gaussian_grads(p, i);
     for (uint32_t q = sc.view_begin; q < sc.view_end; ++q) {
         const uint32_t v = tab.view_by_scene[q];
@@ -955,7 +961,8 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
     uint64_t G = 0, T = 0, px = 0, gs = 0;
     for (int s = 0; s < n_scenes; ++s) {
         const dgmr_scene& sc = scenes[s];
-        if (sc.dtype != DGMR_F32 || sc.n_gaussians < 0 || sc.sh_stride < 1 || sc.sh_stride > 16 || sc.sh_degree < 0 || sc.sh_degree > 3)
+        if (sc.dtype != DGMR_F32 || sc.n_gaussians < 0 || sc.sh_stride < 1 || sc.sh_stride > 16 || sc.sh_degree < 0 || sc.sh_degree > 3
+            || sc.formulation < DGMR_FORMULATION_DEFAULT || sc.formulation > DGMR_FORMULATION_OLS)
             return DGMR_ERR_BAD_ARG;
         if (sc.n_gaussians > 0 && (!sc.centroids || !sc.sh || !sc.weights || !sc.scales || !sc.rotations))
             return DGMR_ERR_BAD_ARG;
@@ -968,6 +975,7 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
         b.n = uint32_t(sc.n_gaussians);
         b.sh_stride = sc.sh_stride;
         b.sh_degree = sc.sh_degree;
+        b.form = scene_formulation(&sc, Formulation::Ots);
         if (grads && grads[s].sh) {
             const dgmr_scene_grads& g = grads[s];
             if (sc.n_gaussians > 0 && (!g.weights || !g.centroids || !g.scales || !g.rotations))
@@ -1028,7 +1036,7 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
 SplatPre batch_pre(const SplatLayout& L, uint32_t G)
 {
     return SplatPre { G, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.rects, L.rgb, L.clamped, L.depths, L.xy, L.conic_opacity, L.tiles_touched,
-        L.bin.depth_key, L.bin.perm, L.blend_rec };
+        L.bin.depth_key, L.bin.perm, L.blend_rec, Formulation::Ots };
 }
 
 // need_pairs = false for the preprocess alone, which touches no pair buffer
@@ -1141,7 +1149,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
     k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc, plan.tab);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
-        nullptr };
+        nullptr, Formulation::Ots };
     k_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);
     note_launch(2);
     return launch_status();

@@ -36,6 +36,7 @@ class Scene:
     scales: np.ndarray  # [N,3]
     rotations: np.ndarray  # [N,4] wxyz
     sh_degree: int = 0
+    formulation: str | None = None  # None = the renderer's default; else opacity/mass/density/ots/ols
 
     @property
     def n(self) -> int:

@@ -33,19 +33,21 @@ class GaussianScene:
     scales: torch.Tensor
     rotations: torch.Tensor
     sh_degree: int
+    formulation: str | None = None  # None = the splat renderer's Ots
 
     @classmethod
     def from_numpy(cls, scene, device) -> "GaussianScene":
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(device)
         return cls(t(scene.sh), t(scene.weights).reshape(-1), t(scene.centroids), t(scene.scales), t(scene.rotations),
-                   int(scene.sh_degree))
+                   int(scene.sh_degree), getattr(scene, "formulation", None))
 
     @property
     def n(self) -> int:
         return int(self.centroids.shape[0])
 
     def c_scene(self) -> N.Scene:
-        return N.make_scene(self.shs, self.weights, self.centroids, self.scales, self.rotations, self.sh_degree)
+        return N.make_scene(self.shs, self.weights, self.centroids, self.scales, self.rotations, self.sh_degree,
+                            self.formulation)
 
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for t in (self.shs, self.weights, self.centroids, self.scales,

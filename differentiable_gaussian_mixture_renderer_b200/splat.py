@@ -75,19 +75,25 @@ def _prepare(shs, opacity, means3D, scales, rotations):
 def splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, background, width: int, height: int,
                   tanfovx: float, tanfovy: float, sh_degree: int, cov_scale_multiplier: float = 1.0,
                   pair_capacity: int | None = None, framebuffer: torch.Tensor | None = None,
-                  stream: torch.cuda.Stream | None = None) -> tuple[torch.Tensor, SplatFrame]:
+                  stream: torch.cuda.Stream | None = None, formulation: str | None = None
+                  ) -> tuple[torch.Tensor, SplatFrame]:
     """Render one frame.
 
     Without ``pair_capacity`` the pair buffers are sized from the frame itself:
     preprocess, one device->host read of the pair count (the reference's
     .item() at splat_forward.cu:204), then binning and blend.  With it the call
     is asynchronous end to end; ``frame.stats[1] & 1`` then reports a frame
-    that needed more pairs than the capacity."""
+    that needed more pairs than the capacity.
+
+    ``formulation`` picks how a weight becomes a screen-space opacity
+    (math.h:322-380: opacity, mass, density, ots, ols); None keeps the splat
+    renderer's Ots (splat_forward.h:58).  The backward of the frame uses the
+    same one."""
     shs, opacity, means3D, scales, rotations = _prepare(shs, opacity, means3D, scales, rotations)
     lib = N.lib()
     dev = means3D.device
     n, W, H = int(means3D.shape[0]), int(width), int(height)
-    scene = N.make_scene(shs, opacity, means3D, scales, rotations, sh_degree)
+    scene = N.make_scene(shs, opacity, means3D, scales, rotations, sh_degree, formulation)
     cam = N.make_camera(view, proj, campos, background, W, H, tanfovx, tanfovy, cov_scale_multiplier)
     fb = framebuffer if framebuffer is not None else torch.empty((3, H, W), dtype=torch.float32, device=dev)
     stats = torch.zeros(4, dtype=torch.int32, device=dev)
@@ -133,9 +139,9 @@ def splat_backward(frame: SplatFrame, grad_framebuffer: torch.Tensor, shs, opaci
 class SplatRender(torch.autograd.Function):
     @staticmethod
     def forward(ctx, shs, opacity, means3D, scales, rotations, view, proj, campos, background, width: int,
-                height: int, tanfovx: float, tanfovy: float, sh_degree: int):
+                height: int, tanfovx: float, tanfovy: float, sh_degree: int, formulation: str | None = None):
         fb, frame = splat_forward(shs, opacity, means3D, scales, rotations, view, proj, campos, background, width,
-                                  height, tanfovx, tanfovy, sh_degree)
+                                  height, tanfovx, tanfovy, sh_degree, formulation=formulation)
         ctx.frame = frame
         ctx.save_for_backward(shs, opacity, means3D, scales, rotations)
         return fb
@@ -144,7 +150,7 @@ class SplatRender(torch.autograd.Function):
     def backward(ctx, grad_output):
         shs, opacity, means3D, scales, rotations = ctx.saved_tensors
         grads = splat_backward(ctx.frame, grad_output, shs, opacity, means3D, scales, rotations)
-        return (*grads, None, None, None, None, None, None, None, None, None)
+        return (*grads, None, None, None, None, None, None, None, None, None, None)
 
 
 render = SplatRender.apply

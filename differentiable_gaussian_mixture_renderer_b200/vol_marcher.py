@@ -6,7 +6,9 @@ tanfovx, tanfovy, active_sh_degree) -> image [3, H, W]`` with the reference's
 argument meaning (vol_marcher.py:19-65): float32 or float64 CUDA tensors,
 matrices in the transposed (torch) layout, SH [N, k<=16, 3], opacity [N] or
 [N, 1], rotations (w, x, y, z).  Backward returns gradients for the first five
-inputs and None for the other nine.
+inputs and None for the rest.  An optional 15th argument names the formulation
+(opacity, mass, density, ots, ols; vol_marcher.h:66 fixes Opacity at compile
+time, which None keeps).
 """
 from __future__ import annotations
 
@@ -19,13 +21,14 @@ class VolMarcher(torch.autograd.Function):
     @staticmethod
     def forward(ctx, shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
                 camera_center, bg_color, image_width: int, image_height: int, tanfovx: float, tanfovy: float,
-                active_sh_degree: int):
+                active_sh_degree: int, formulation: str | None = None):
         cache = cpp_binding.forward(shs, opacity, means3D, scales, rotations, world_view_transform,
                                     full_proj_transform, camera_center, bg_color, image_width, image_height, tanfovx,
-                                    tanfovy, active_sh_degree)
+                                    tanfovy, active_sh_degree, formulation=formulation)
         ctx.save_for_backward(shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
                               camera_center, bg_color, *cache)
         ctx.frame = (int(image_width), int(image_height), float(tanfovx), float(tanfovy), int(active_sh_degree))
+        ctx.formulation = formulation
         return cache[0]
 
     @staticmethod
@@ -37,10 +40,11 @@ class VolMarcher(torch.autograd.Function):
         cache = list(saved[9:])
         W, H, tfx, tfy, deg = ctx.frame
         g_sh, g_w, g_mu, g_s, g_q = cpp_binding.backward(shs, opacity, means3D, scales, rotations, view, proj, campos,
-                                                         bg, W, H, tfx, tfy, deg, grad_output, cache)
+                                                         bg, W, H, tfx, tfy, deg, grad_output, cache,
+                                                         formulation=ctx.formulation)
         if opacity.dim() == 1:
             g_w = g_w.reshape(-1)
-        return g_sh, g_w, g_mu, g_s, g_q, None, None, None, None, None, None, None, None, None
+        return g_sh, g_w, g_mu, g_s, g_q, None, None, None, None, None, None, None, None, None, None
 
 
 apply = VolMarcher.apply

@@ -18,10 +18,13 @@ _MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
 def forward(sh, weights, centroids, scales, rotations, view, proj, campos, background, width: int, height: int,
             tan_fovx: float, tan_fovy: float, sh_degree: int, cov_scale_multiplier: float = 1.0,
             render_mode: str = "full", debug_bin: int = -1, max_depth: float = 20.0,
-            stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+            stream: torch.cuda.Stream | None = None, formulation: str | None = None) -> torch.Tensor:
     """Render one frame; returns the framebuffer [3, H, W].  The pair buffers are
     sized from the frame (preprocess, pair count read back, then the render),
-    like the reference's .item() read of the pair count."""
+    like the reference's .item() read of the pair count.  ``formulation``
+    (opacity, mass, density, ots, ols) replaces the compile-time
+    vol_raster::config::gaussian_mixture_formulation (vol_raster_forward.h:66);
+    None keeps its Ots."""
     ts = [sh, weights, centroids, scales, rotations]
     for t in ts:
         if not isinstance(t, torch.Tensor) or t.dtype != torch.float32:
@@ -35,7 +38,7 @@ def forward(sh, weights, centroids, scales, rotations, view, proj, campos, backg
     dev = centroids.device
     n, W, H = int(centroids.shape[0]), int(width), int(height)
     with torch.cuda.device(dev):
-        scene = N.make_scene(sh, weights, centroids, scales, rotations, sh_degree)
+        scene = N.make_scene(sh, weights, centroids, scales, rotations, sh_degree, formulation)
         cam = N.make_camera(view, proj, campos, background, W, H, tan_fovx, tan_fovy, cov_scale_multiplier)
         opts = N.RenderOptions(_MODES[render_mode], int(debug_bin), float(max_depth))
         s = N.stream_handle(stream)

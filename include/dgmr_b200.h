@@ -59,7 +59,22 @@ typedef struct dgmr_scene {
     const void* weights;
     const void* scales;
     const void* rotations;
+    int32_t formulation; /* dgmr_formulation: how weights become masses / opacities */
+    int32_t reserved;
 } dgmr_scene;
+
+/* types.h:26-32.  The reference fixes one per renderer at compile time: Ots for
+ * the splat (splat_forward.h:58) and vol_raster (vol_raster_forward.h:66),
+ * Opacity for vol_marcher (vol_marcher.h:66); DGMR_FORMULATION_DEFAULT (0, a
+ * zero-initialised scene) selects exactly those. */
+typedef enum dgmr_formulation {
+    DGMR_FORMULATION_DEFAULT = 0,
+    DGMR_FORMULATION_OPACITY = 1,
+    DGMR_FORMULATION_MASS = 2,
+    DGMR_FORMULATION_DENSITY = 3,
+    DGMR_FORMULATION_OTS = 4,
+    DGMR_FORMULATION_OLS = 5,
+} dgmr_formulation;
 
 /* One camera (host values). */
 typedef struct dgmr_camera {

@@ -61,6 +61,11 @@ struct RenderMode {
 };
 RenderMode g_render_mode;
 
+// The formulation of the following calls (types.h:26-32): 0 = each renderer's
+// reference default (splat and vol_raster Ots, vol_marcher Opacity), else 1 + value.
+int g_formulation = 0;
+inline Formulation form_or(Formulation renderer_default) { return g_formulation == 0 ? renderer_default : Formulation(g_formulation - 1); }
+
 template <class T>
 struct SceneIn {
     int N;
@@ -215,7 +220,7 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
             continue;
         const T w = s.weights[i];
         const V3<T> sc = mul(load3(s.scales, size_t(i)), s.cov_scale_multiplier);
-        const Gaussian2d<T> g = splat(Formulation::Ots, w, mu, sc, s.rotations + 4 * size_t(i), cam, T(0.3f));
+        const Gaussian2d<T> g = splat(form_or(Formulation::Ots), w, mu, sc, s.rotations + 4 * size_t(i), cam, T(0.3f));
         const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(T(3.f) * dgmr_fm::sqrt_f(g.cov.v[0])));
         const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(T(3.f) * dgmr_fm::sqrt_f(g.cov.v[2])));
         rects[2 * i] = ex;
@@ -380,10 +385,10 @@ void vm_preprocess(const SceneIn<T>& s, VmCache<T>& c)
         filtered.v[0] = filtered.v[0] + fks2;
         filtered.v[3] = filtered.v[3] + fks2;
         filtered.v[5] = filtered.v[5] + fks2;
-        const T mass = weight_to_mass(Formulation::Opacity, w, sc, affine_transform_and_cut(cov3, W3));
+        const T mass = weight_to_mass(form_or(Formulation::Opacity), w, sc, affine_transform_and_cut(cov3, W3));
         if (mass <= T(0))
             continue;
-        const Gaussian2d<T> g = splat(Formulation::Opacity, w, mu, sc, q, cam, T(FILTER_SD * FILTER_SD));
+        const Gaussian2d<T> g = splat(form_or(Formulation::Opacity), w, mu, sc, q, cam, T(FILTER_SD * FILTER_SD));
         const auto iso = [](T wt, T var, T isoline) {
             const T sv = T(-2) * dgmr_fm::log_f(isoline / wt);
             if (sv <= T(0))
@@ -844,7 +849,7 @@ void vm_backward_impl(const SceneIn<T>& s, const VmCache<T>& c, const int32_t* l
         filtered.v[3] = filtered.v[3] + fks * fks;
         filtered.v[5] = filtered.v[5] + fks * fks;
         const S2<T> cov2d = affine_transform_and_cut(cov3, W3);
-        const T mass = weight_to_mass(Formulation::Opacity, w, sc, cov2d);
+        const T mass = weight_to_mass(form_or(Formulation::Opacity), w, sc, cov2d);
         if (mass <= T(0))
             continue;
         const V3<T> dir = { delta.x / dist, delta.y / dist, delta.z / dist };
@@ -867,18 +872,35 @@ void vm_backward_impl(const SceneIn<T>& s, const VmCache<T>& c, const int32_t* l
             g_invcov.v[j] = T(tot[size_t(i) * 13 + 7 + j]);
         const S3<T> g_filtered = grad_inverse_sym3(filtered, g_invcov);
         const T g_mass = T(tot[size_t(i) * 13]);
-        // mass = w * 2 pi sqrt(det cov2d)
-        const T dcov = det2(cov2d);
-        const T i2 = integrate_exponential_cov2(cov2d);
-        const T g_w = g_mass * i2;
-        const T g_i2 = g_mass * w;
-        const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
-        const S2<T> g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
+        // adjoint of weight_to_mass (math.h:298-320)
+        const Formulation f = form_or(Formulation::Opacity);
+        T g_w = T(0);
+        S2<T> g_cov2d = { { 0, 0, 0 } };
+        V3<T> g_s = { 0, 0, 0 };
+        if (f == Formulation::Opacity) { // mass = w * 2 pi sqrt(det cov2d)
+            const T dcov = det2(cov2d);
+            const T i2 = integrate_exponential_cov2(cov2d);
+            g_w = g_mass * i2;
+            const T g_i2 = g_mass * w;
+            const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
+            g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
+        } else if (f == Formulation::Mass) {
+            g_w = g_mass;
+        } else if (f == Formulation::Density) {
+            g_w = g_mass * integrate_exponential3(sc);
+            const T k = (g_mass * w) * two_pi_pow_1_5<T>();
+            g_s = { k * sc.y * sc.z, k * sc.x * sc.z, k * sc.x * sc.y };
+        } else {
+            const V2<T> l2 = f == Formulation::Ots ? larger2(sc) : smaller2(sc);
+            g_w = g_mass * integrate_exponential2(l2);
+            const T k = (g_mass * w) * two_pi<T>();
+            const V2<T> g_l2 = { k * l2.y, k * l2.x };
+            g_s = f == Formulation::Ots ? grad_larger2(sc, g_l2) : grad_smaller2(sc, g_l2);
+        }
         S3<T> g_cov3 = g_filtered;
         const T g_fks2 = (g_filtered.v[0] + g_filtered.v[3]) + g_filtered.v[5];
         g_dist = g_dist + (g_fks2 * T(2) * fks) * aa;
         grad_affine_transform_and_cut(cov3, W3, g_cov2d, &g_cov3, static_cast<M3<T>*>(nullptr));
-        V3<T> g_s = { 0, 0, 0 };
         T g_q[4] = { 0, 0, 0, 0 };
         grad_compute_cov(sc, q, g_cov3, &g_s, g_q);
         g_mu = add(g_mu, mul(delta, g_dist / dist));
@@ -894,10 +916,10 @@ void vm_backward_impl(const SceneIn<T>& s, const VmCache<T>& c, const int32_t* l
 }
 
 // --------------------------------------------------------------- splat bwd
-// Adjoint of splat<Ots> (grad/math.h:333-527 restated, with the derivative of
-// the fov clamp limits w.r.t. t.z included) for one Gaussian.
+// Adjoint of splat (grad/math.h:333-527 restated, with the derivative of the
+// fov clamp limits w.r.t. t.z included) for one Gaussian, every formulation.
 template <class T>
-void grad_splat_ots(T weight, V3<T> mu, V3<T> s, const T* q, const Camera<T>& cam, T filter, T g_w2, V2<T> g_xy, S2<T> g_cov, T* g_weight,
+void grad_splat(Formulation f, T weight, V3<T> mu, V3<T> s, const T* q, const Camera<T>& cam, T filter, T g_w2, V2<T> g_xy, S2<T> g_cov, T* g_weight,
     V3<T>* g_mu, V3<T>* g_s, T* g_q)
 {
     const V4<T> tu4 = mat4_mul_point(cam.view, mu);
@@ -909,25 +931,54 @@ void grad_splat_ots(T weight, V3<T> mu, V3<T> s, const T* q, const Camera<T>& ca
     const M3<T> W = mat3_of(cam.view);
     const M3<T> Tm = matmul(SJ, W);
     const S3<T> cov3 = compute_cov(s, q);
-    S2<T> cov2 = affine_transform_and_cut(cov3, Tm);
+    const S2<T> c = affine_transform_and_cut(cov3, Tm);
+    S2<T> cov2 = c;
     cov2.v[0] = cov2.v[0] + filter;
     cov2.v[2] = cov2.v[2] + filter;
     const T detSJ = det3(SJ);
-    const V2<T> l2 = larger2(s);
-    const T i2p = integrate_exponential2(l2);
-    const T dc = det2(cov2);
-    const T i2 = integrate_exponential_cov2(cov2);
-    // weight2d = w * detSJ * i2p / i2
-    *g_weight = *g_weight + g_w2 * detSJ * i2p / i2;
-    const T g_detSJ = g_w2 * weight * i2p / i2;
-    const T g_i2p = g_w2 * weight * detSJ / i2;
-    const T g_i2 = -g_w2 * weight * detSJ * i2p / (i2 * i2);
-    const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dc)) : T(0);
-    g_cov.v[0] = g_cov.v[0] + g_dc * cov2.v[2];
-    g_cov.v[1] = g_cov.v[1] - g_dc * T(2) * cov2.v[1];
-    g_cov.v[2] = g_cov.v[2] + g_dc * cov2.v[0];
-    const V2<T> g_l2 = { g_i2p * two_pi<T>() * l2.y, g_i2p * two_pi<T>() * l2.x };
-    *g_s = add(*g_s, grad_larger2(s, g_l2));
+    T g_detSJ = T(0);
+    if (f == Formulation::Opacity) {
+        // weight2d = w sqrt(max(eps, det c / det(c + filter)))
+        const T dcv = det2(c), dn = det2(cov2);
+        const T r = dcv / dn;
+        const T factor = dgmr_fm::sqrt_f(max_f(T(0.000025), r));
+        *g_weight = *g_weight + g_w2 * factor;
+        if (T(0.000025) < r) {
+            const T g_r = (g_w2 * weight) / (T(2) * factor);
+            const T g_dc = g_r / dn;
+            const T g_dn = -g_r * dcv / (dn * dn);
+            g_cov.v[0] = (g_cov.v[0] + g_dc * c.v[2]) + g_dn * cov2.v[2];
+            g_cov.v[1] = (g_cov.v[1] - g_dc * T(2) * c.v[1]) - g_dn * T(2) * cov2.v[1];
+            g_cov.v[2] = (g_cov.v[2] + g_dc * c.v[0]) + g_dn * cov2.v[0];
+        }
+    } else {
+        // weight2d = w detSJ A(s) / i2(cov2)
+        T A = T(1);
+        if (f == Formulation::Density)
+            A = integrate_exponential3(s);
+        else if (f == Formulation::Ots)
+            A = integrate_exponential2(larger2(s));
+        else if (f == Formulation::Ols)
+            A = integrate_exponential2(smaller2(s));
+        const T dc = det2(cov2);
+        const T i2 = integrate_exponential_cov2(cov2);
+        *g_weight = *g_weight + g_w2 * detSJ * A / i2;
+        g_detSJ = g_w2 * weight * A / i2;
+        const T g_A = g_w2 * weight * detSJ / i2;
+        const T g_i2 = -g_w2 * weight * detSJ * A / (i2 * i2);
+        const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dc)) : T(0);
+        g_cov.v[0] = g_cov.v[0] + g_dc * cov2.v[2];
+        g_cov.v[1] = g_cov.v[1] - g_dc * T(2) * cov2.v[1];
+        g_cov.v[2] = g_cov.v[2] + g_dc * cov2.v[0];
+        if (f == Formulation::Density) {
+            const T k = g_A * two_pi_pow_1_5<T>();
+            *g_s = add(*g_s, V3<T> { k * s.y * s.z, k * s.x * s.z, k * s.x * s.y });
+        } else if (f == Formulation::Ots || f == Formulation::Ols) {
+            const V2<T> l2 = f == Formulation::Ots ? larger2(s) : smaller2(s);
+            const V2<T> g_l2 = { g_A * two_pi<T>() * l2.y, g_A * two_pi<T>() * l2.x };
+            *g_s = add(*g_s, f == Formulation::Ots ? grad_larger2(s, g_l2) : grad_smaller2(s, g_l2));
+        }
+    }
     M3<T> g_SJ = cofactor3(SJ);
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
@@ -1101,7 +1152,8 @@ void splat_backward_impl(const SceneIn<T>& s, const T* rgb, const uint8_t* clamp
         T g_weight = 0;
         V3<T> g_mu = { 0, 0, 0 }, g_s = { 0, 0, 0 };
         T g_q[4] = { 0, 0, 0, 0 };
-        grad_splat_ots(s.weights[i], mu, sc, q, cam, T(0.3f), T(a[5]), V2<T> { T(a[0]), T(a[1]) }, g_cov, &g_weight, &g_mu, &g_s, g_q);
+        grad_splat(form_or(Formulation::Ots), s.weights[i], mu, sc, q, cam, T(0.3f), T(a[5]), V2<T> { T(a[0]), T(a[1]) }, g_cov, &g_weight, &g_mu, &g_s,
+            g_q);
         // colour
         const V3<T> v = sub(mu, campos);
         const T vl = dgmr_fm::sqrt_f(dot(v, v));
@@ -1203,7 +1255,7 @@ void vr_preprocess(const SceneIn<float>& s, VrCache& c)
         const float w = s.weights[i];
         const V3<float> sc = mul(load3(s.scales, size_t(i)), s.cov_scale_multiplier);
         const float* q = s.rotations + 4 * size_t(i);
-        const Gaussian2d<float> g = splat(Formulation::Ots, w, mu, sc, q, cam, 0.3f);
+        const Gaussian2d<float> g = splat(form_or(Formulation::Ots), w, mu, sc, q, cam, 0.3f);
         const S3<float> cov3 = compute_cov(sc, q);
         const float fks = length(sub(mu, campos)) * aa;
         const float fks2 = fks * fks;
@@ -1212,7 +1264,7 @@ void vr_preprocess(const SceneIn<float>& s, VrCache& c)
         filtered.v[3] = filtered.v[3] + fks2;
         filtered.v[5] = filtered.v[5] + fks2;
         // weight_to_mass<Ots> of the scales plus the squared filter size (vol_raster_forward.cu:106)
-        c.masses[i] = weight_to_mass(Formulation::Ots, w, V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 }, g.cov);
+        c.masses[i] = weight_to_mass(form_or(Formulation::Ots), w, V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 }, g.cov);
         const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
         const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
         c.rects[2 * i] = ex;
@@ -1403,6 +1455,9 @@ void orc_set_num_threads(int n)
 }
 
 uint32_t orc_higher_msb(uint32_t n) { return higher_msb(n); }
+
+// the formulation of the following calls: 0 = each renderer's default, else 1 + types.h value
+void orc_set_formulation(int f) { g_formulation = (f >= 0 && f <= 5) ? f : 0; }
 
 // the marcher's debug render mode for the following vol_marcher forwards (0 Full, 1 Bins, 2 Depth)
 void orc_set_render_mode(int mode, int bin, double max_depth)

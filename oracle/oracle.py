@@ -88,6 +88,8 @@ def _declare(L):
         f = getattr(L, f"orc_density_randomised_{sfx}")
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.orc_set_formulation.restype = None
+    L.orc_set_formulation.argtypes = [C.c_int]
     L.orc_set_render_mode.restype = None
     L.orc_set_render_mode.argtypes = [C.c_int, C.c_int, C.c_double]
     L.orc_set_const_samples.restype = None
@@ -112,7 +114,14 @@ def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
 
 
+_FORMS = {None: 0, "opacity": 1, "mass": 2, "density": 3, "ots": 4, "ols": 5}
+
+
 def _scene_args(scene, cam, dt, bg=None, cov_mult=1.0):
+    """The scene/camera arguments of every oracle entry point; also selects the
+    scene's formulation (attribute 'formulation': None = the renderer's
+    reference default, or opacity/mass/density/ots/ols) for the call."""
+    lib().orc_set_formulation(_FORMS[getattr(scene, "formulation", None)])
     sh = _c(scene.sh, dt)
     bg = np.zeros(3, dt) if bg is None else _c(bg, dt)
     return [scene.n, _c(scene.centroids, dt), sh, sh.shape[1], scene.sh_degree, _c(scene.weights, dt).reshape(-1),

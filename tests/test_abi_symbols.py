@@ -54,6 +54,25 @@ def test_bad_arguments_are_rejected_on_the_host():
     assert lib.dgmr_vm_set_const_samples(5, None) == _native.DGMR_ERR_BAD_ARG
 
 
+def test_scene_struct_layout_and_formulation_codes():
+    import ctypes as C
+    import pytest
+    # dgmr_scene: 4 int32, 5 pointers, formulation, reserved
+    assert C.sizeof(_native.Scene) == 64 and _native.Scene.formulation.offset == 56
+    assert [_native.formulation_code(f) for f in (None, "opacity", "Mass", "density", "ots", "OLS", 3)] == \
+        [0, 1, 2, 3, 4, 5, 3]
+    for bad in ("gaussian", 6, -1, True, 1.0):
+        with pytest.raises(ValueError):
+            _native.formulation_code(bad)
+    lib = _native.load()
+    scene = _native.Scene()
+    cam = _native.Camera()
+    cam.width, cam.height = 16, 16
+    scene.n_gaussians, scene.sh_stride, scene.sh_degree, scene.dtype = 0, 1, 0, 0
+    scene.formulation = 6  # out of range: rejected before any device work
+    assert lib.dgmr_splat_forward(scene, cam, None, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+
+
 def _batch_tables(n_views, scene_index=0, n_scenes=1):
     scenes = (_native.Scene * n_scenes)()
     for s in scenes:
