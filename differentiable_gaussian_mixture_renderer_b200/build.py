@@ -20,6 +20,9 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(OUT_DIR, "libdgmr_b200.so")
 SOURCES = ["dgmr_splat.cu", "dgmr_marcher.cu", "dgmr_raster.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+INCLUDE = os.path.join(HERE, "..", "include")
+VIEWER_SRC = os.path.join(HERE, "viewer", "headless_view.cpp")
+VIEWER_PATH = os.path.join(OUT_DIR, "dgmr_headless_view")
 
 
 def nvcc() -> str:
@@ -59,5 +62,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB_PATH
 
 
+def build_viewer(force: bool = False) -> str:
+    """The headless viewer (viewer/headless_view.cpp): host code over the C++
+    viewer interface, linked against libdgmr_b200.so next to it."""
+    lib = build(force=force)
+    deps = [VIEWER_SRC, lib, os.path.join(INCLUDE, "dgmr_b200_sibr.hpp"), os.path.join(INCLUDE, "dgmr_b200.h")]
+    if not force and os.path.exists(VIEWER_PATH) and all(os.path.getmtime(d) <= os.path.getmtime(VIEWER_PATH)
+                                                          for d in deps):
+        return VIEWER_PATH
+    tmp = VIEWER_PATH + ".tmp"
+    cmd = [nvcc(), *host_compiler(), "-Wno-deprecated-gpu-targets", "-std=c++17", "-O2", "-I", INCLUDE, VIEWER_SRC, "-L", OUT_DIR, "-ldgmr_b200",
+           "-Xlinker", "-rpath,$ORIGIN", "-o", tmp]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, VIEWER_PATH)
+    return VIEWER_PATH
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_viewer(force="--force" in sys.argv))
