@@ -236,13 +236,17 @@ __device__ __forceinline__ float rect_min_q(float cx, float cy, float a, float b
     return m;
 }
 
-// One 16x16 tile per block of 128 threads, two pixels per thread (rows y and
-// y + 8).  Each batch of up to 256 list entries is loaded two per thread;
-// splats whose cutoff ellipse cannot reach the tile are dropped (an exact
-// rectangle minimum with a margin, so no pixel that could pass its own cutoff
-// test loses a splat); the rest are compacted in list order into shared memory
-// as 32-byte records and evaluated by both pixels.  The block stops when every
-// pixel is saturated.
+// One 16x16 tile per block of 256 threads, one pixel per thread.  Each batch
+// of up to 256 list entries is loaded one per thread; splats whose cutoff
+// ellipse cannot reach the tile are dropped (an exact rectangle minimum with a
+// margin, so no pixel that could pass its own cutoff test loses a splat); the
+// rest are compacted in list order into shared memory as 32-byte records and
+// evaluated by every pixel.  The block stops when every pixel is saturated.
+// The kernel's duration is set by its slowest tile (a few tiles with ~2-3k
+// unsaturated entries run from the first wave to the end), so a tile's
+// pixels are spread over as many threads as it has pixels: two pixels per
+// thread made that critical path, and the launch, 12 % longer.
+
 // Where one tile's pixels live: the frame it belongs to and the tile's index
 // inside that frame's grid.  final_T / n_contrib / grad_fb point at the
 // frame's own planes.
@@ -267,13 +271,12 @@ struct SingleFrame {
 };
 
 template <class Frames>
-__global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
+__global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
     const float* __restrict__ rgb, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, const uint32_t* __restrict__ tile_order,
     const __grid_constant__ Frames frames)
 {
-    constexpr int kThreads = 128;
-    constexpr int kPer = 2; // list entries loaded per thread per batch
-    constexpr int kBatch = kThreads * kPer;
+    constexpr int kThreads = 256;
+    constexpr int kBatch = kThreads;
     constexpr int kWarps = kThreads / 32;
     __shared__ float4 s_r0[kBatch];
     __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
@@ -284,10 +287,9 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
     const unsigned px = tx * kTile + (threadIdx.x & 15u);
-    const unsigned py0 = ty * kTile + (threadIdx.x >> 4), py1 = py0 + 8;
-    PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py0 < H) };
-    PixelState p1 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py1 < H) };
-    const bool in0 = !p0.done, in1 = !p1.done;
+    const unsigned py = ty * kTile + (threadIdx.x >> 4);
+    PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py < H) };
+    const bool in0 = !p0.done;
     int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
     if (b < 0 || e < b || uint32_t(e) > cap) {
         if (threadIdx.x == 0)
@@ -295,47 +297,38 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
         b = e = 0;
     }
     const float fx0 = float(tx * kTile), fx1 = fx0 + 15.f, fy0 = float(ty * kTile), fy1 = fy0 + 15.f;
-    const float fpx = float(px), fpy0 = float(py0), fpy1 = float(py1);
+    const float fpx = float(px), fpy = float(py);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int32_t base = b; base < e; base += kBatch) {
-        const bool all_done = p0.done && p1.done;
-        if (__syncthreads_count(all_done) == kThreads)
+        if (__syncthreads_count(p0.done) == kThreads)
             break;
-        float4 r0[kPer], r1[kPer];
-        uint32_t id[kPer];
+        float4 r0, r1;
+        uint32_t id = 0xffffffffu;
         int keep = 0;
-#pragma unroll
-        for (int h = 0; h < kPer; ++h) {
-            const int32_t k = base + int(threadIdx.x) * kPer + h;
-            id[h] = 0xffffffffu;
+        {
+            const int32_t k = base + int(threadIdx.x);
             if (k < e) {
                 uint32_t g = list[k];
                 if (g >= N) {
                     flag_bounds(stats, 0x32u);
                     g = 0;
                 }
-                r0[h] = rec[2 * size_t(g)];
-                r1[h] = rec[2 * size_t(g) + 1];
-                const float qmin = rect_min_q(r0[h].x, r0[h].y, r0[h].z, 0.5f * r1[h].x, r0[h].w, fx0, fx1, fy0, fy1);
-                if (!(qmin > r1[h].z * 1.001f + 0.01f)) {
-                    id[h] = g;
-                    r1[h].w = __int_as_float(k - b + 1);
-                    ++keep;
+                r0 = rec[2 * size_t(g)];
+                r1 = rec[2 * size_t(g) + 1];
+                const float qmin = rect_min_q(r0.x, r0.y, r0.z, 0.5f * r1.x, r0.w, fx0, fx1, fy0, fy1);
+                if (!(qmin > r1.z * 1.001f + 0.01f)) {
+                    id = g;
+                    r1.w = __int_as_float(k - b + 1);
+                    keep = 1;
                 }
             }
         }
-        // order-preserving compaction: exclusive scan of the per-thread counts
-        int x = keep;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o)
-                x += y;
-        }
-        if (lane == 31)
-            s_warp_tot[warp] = x;
+        // order-preserving compaction: warp ballot, then the warps' totals in order
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0)
+            s_warp_tot[warp] = __popc(m);
         __syncthreads();
-        int slot = x - keep;
+        int slot = __popc(m & ((1u << lane) - 1u));
         int n = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
@@ -343,51 +336,37 @@ __global__ void __launch_bounds__(128) k_splat_blend(const int32_t* __restrict__
             slot += (w < warp) ? t : 0;
             n += t;
         }
-#pragma unroll
-        for (int h = 0; h < kPer; ++h) {
-            if (id[h] != 0xffffffffu) {
-                s_r0[slot] = r0[h];
-                s_r1[slot] = r1[h];
-                s_rgb[0][slot] = rgb[3 * size_t(id[h])];
-                s_rgb[1][slot] = rgb[3 * size_t(id[h]) + 1];
-                s_rgb[2][slot] = rgb[3 * size_t(id[h]) + 2];
-                ++slot;
-            }
+        if (keep) {
+            s_r0[slot] = r0;
+            s_r1[slot] = r1;
+            s_rgb[0][slot] = rgb[3 * size_t(id)];
+            s_rgb[1][slot] = rgb[3 * size_t(id) + 1];
+            s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
         }
         __syncthreads();
-        if (!all_done) {
+        if (!p0.done) {
             for (int j = 0; j < n; ++j) {
                 const float4 a0 = s_r0[j];
                 const float4 a1 = s_r1[j];
                 float dx, dy;
-                const float q0 = splat_q(a0, a1.x, fpx, fpy0, &dx, &dy);
-                const float q1 = splat_q(a0, a1.x, fpx, fpy1, &dx, &dy);
-                if ((p0.done || q0 > a1.z) && (p1.done || q1 > a1.z))
+                const float q0 = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
+                if (q0 > a1.z)
                     continue;
-                const float cr = s_rgb[0][j], cg = s_rgb[1][j], cb = s_rgb[2][j];
-                const int32_t idx = __float_as_int(a1.w);
-                blend_step(p0, q0, a1.z, a1.y, cr, cg, cb, idx);
-                blend_step(p1, q1, a1.z, a1.y, cr, cg, cb, idx);
+                blend_step(p0, q0, a1.z, a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
+                if (p0.done)
+                    break;
             }
         }
         __syncthreads();
     }
     const size_t plane = size_t(W) * H;
     if (in0) {
-        const size_t pix = size_t(py0) * W + px;
+        const size_t pix = size_t(py) * W + px;
         f.fb[pix] = p0.c0 + p0.T * f.bg0;
         f.fb[plane + pix] = p0.c1 + p0.T * f.bg1;
         f.fb[2 * plane + pix] = p0.c2 + p0.T * f.bg2;
         f.final_T[pix] = p0.T;
         f.n_contrib[pix] = p0.last;
-    }
-    if (in1) {
-        const size_t pix = size_t(py1) * W + px;
-        f.fb[pix] = p1.c0 + p1.T * f.bg0;
-        f.fb[plane + pix] = p1.c1 + p1.T * f.bg1;
-        f.fb[2 * plane + pix] = p1.c2 + p1.T * f.bg2;
-        f.final_T[pix] = p1.T;
-        f.n_contrib[pix] = p1.last;
     }
 }
 
@@ -635,7 +614,7 @@ void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb
     const int par
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
     k_tile_order<<<1, 1024, 0, s>>>(L.ranges, cam.gx * cam.gy, L.tile_order);
-    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, N, cap, st_dev, L.tile_order, single_frame(cam, fb, L));
+    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, N, cap, st_dev, L.tile_order, single_frame(cam, fb, L));
     note_launch(2);
 }
 
@@ -758,7 +737,7 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
     const CameraT<float> cam = make_camera<float>(*camera);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int par = tile_sort_parity(cam.gx * cam.gy);
-    k_splat_blend<<<cam.gx * cam.gy, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
+    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
         L.tile_order, single_frame(cam, framebuffer, L));
     note_launch();
     return launch_status();
@@ -1121,7 +1100,7 @@ dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes,
     const int par = run_binning_grids<float>(G, plan.tab.n_tiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev,
         num_sms(), s, true);
     k_tile_order<<<1, 1024, 0, s>>>(L.ranges, plan.tab.n_tiles, L.tile_order);
-    k_splat_blend<<<plan.tab.n_tiles, 128, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab);
+    k_splat_blend<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab);
     note_launch(2);
     return launch_status();
 }
