@@ -44,8 +44,13 @@ struct VmLayout {
     size_t bytes;
 };
 
+inline uint32_t frame_tiles(const dgmr_camera* camera)
+{
+    return ((uint32_t(camera->width) + kTile - 1) / kTile) * ((uint32_t(camera->height) + kTile - 1) / kTile);
+}
+
 template <class T>
-inline VmLayout<T> vm_layout(uint32_t N, uint32_t cap, void* base)
+inline VmLayout<T> vm_layout(uint32_t N, uint32_t n_tiles, uint32_t cap, void* base)
 {
     VmLayout<T> L;
     Carver c;
@@ -54,7 +59,7 @@ inline VmLayout<T> vm_layout(uint32_t N, uint32_t cap, void* base)
     L.pre_scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
     L.pre_bytes = c.off;
     L.acc = c.take<T>(size_t(N) * 10);
-    carve_binning(c, L.bin, N, cap);
+    carve_binning(c, L.bin, N, n_tiles, cap);
     L.bytes = c.off;
     return L;
 }
@@ -381,7 +386,7 @@ dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dg
     dgmr_frame_stats* stats, cudaStream_t s)
 {
     const uint32_t N = uint32_t(scene->n_gaussians);
-    const VmLayout<T> Lw = vm_layout<T>(N, 0, workspace);
+    const VmLayout<T> Lw = vm_layout<T>(N, frame_tiles(camera), 0, workspace);
     if (workspace_bytes < Lw.pre_bytes)
         return DGMR_ERR_WORKSPACE;
     const CameraT<T> cam = make_camera<T>(*camera);
@@ -407,7 +412,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     dgmr_frame_stats* stats, cudaStream_t s, const dgmr_render_options* options)
 {
     const uint32_t N = uint32_t(scene->n_gaussians), cap = uint32_t(cap64);
-    const VmLayout<T> L = vm_layout<T>(N, cap, workspace);
+    const VmLayout<T> L = vm_layout<T>(N, frame_tiles(camera), cap, workspace);
     if (workspace_bytes < L.bytes)
         return DGMR_ERR_WORKSPACE;
     const CameraT<T> cam = make_camera<T>(*camera);
@@ -448,7 +453,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     void* g_centroids, void* g_scales, void* g_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, cudaStream_t s)
 {
     const uint32_t N = uint32_t(scene->n_gaussians);
-    const VmLayout<T> L = vm_layout<T>(N, 0, workspace);
+    const VmLayout<T> L = vm_layout<T>(N, frame_tiles(camera), 0, workspace);
     if (workspace_bytes < L.bytes)
         return DGMR_ERR_WORKSPACE;
     const CameraT<T> cam = make_camera<T>(*camera);
@@ -503,8 +508,8 @@ size_t dgmr_vm_workspace_size(int32_t n_gaussians, int32_t width, int32_t height
     const uint32_t n_tiles = ((uint32_t(width) + kTile - 1) / kTile) * ((uint32_t(height) + kTile - 1) / kTile);
     const size_t masks = size_t(n_tiles) * sizeof(uint32_t); // march order
     if (dtype == DGMR_F64)
-        return align_up(vm_layout<double>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;
-    return align_up(vm_layout<float>(uint32_t(n_gaussians), uint32_t(pair_capacity), nullptr).bytes) + masks;
+        return align_up(vm_layout<double>(uint32_t(n_gaussians), n_tiles, uint32_t(pair_capacity), nullptr).bytes) + masks;
+    return align_up(vm_layout<float>(uint32_t(n_gaussians), n_tiles, uint32_t(pair_capacity), nullptr).bytes) + masks;
 }
 
 dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* cache, void* workspace, size_t workspace_bytes,

@@ -61,7 +61,7 @@ inline VrLayout vr_layout(uint32_t N, uint32_t W, uint32_t H, uint32_t cap, void
     L.point_offsets = c.take<uint32_t>(N);
     L.ranges = c.take<int32_t>(size_t(gx) * gy * 2);
     L.stats = c.take<uint32_t>(4);
-    carve_binning_gaussians(c, L.bin, N);
+    carve_binning_gaussians(c, L.bin, N, gx * gy);
     L.bytes = c.off;
     Carver cp;
     cp.base = static_cast<char*>(pair_base);

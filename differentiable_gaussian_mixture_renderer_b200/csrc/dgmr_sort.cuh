@@ -342,11 +342,12 @@ inline size_t radix_temp_bytes(uint32_t capacity)
     return (size_t(kSortBins) * (tiles + 1) + kSortBins) * sizeof(uint32_t);
 }
 
-// Stable sort of (keys, vals) by key bits [0, end_bit).  The data ping-pongs
-// between (k0, v0) and (k1, v1); returns 0 if the result is in k0/v0, 1 if in
-// k1/v1.  n comes from *n_dev (device) when non-null, else n_static.
+// Stable sort of (keys, vals) by key bits [begin_bit, end_bit).  The data
+// ping-pongs between (k0, v0) and (k1, v1); returns 0 if the result is in
+// k0/v0, 1 if in k1/v1.  n comes from *n_dev (device) when non-null, else
+// n_static.
 inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int end_bit,
-    void* temp, int n_sms, cudaStream_t stream, uint32_t* stats = nullptr)
+    void* temp, int n_sms, cudaStream_t stream, uint32_t* stats = nullptr, int begin_bit = 0)
 {
     const uint32_t tiles = (capacity + kSortTile - 1) / kSortTile;
     if (tiles == 0)
@@ -359,9 +360,9 @@ inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* 
     // fewest 8-bit-or-narrower passes, with the bits spread evenly over them
     // (e.g. 13 tile bits -> 7 + 6): fewer buckets per pass keep the runs each
     // tile writes per digit longer
-    const int n_pass = (end_bit + 7) / 8;
-    const int width = n_pass ? (end_bit + n_pass - 1) / n_pass : 8;
-    for (int shift = 0; shift < end_bit; shift += width) {
+    const int n_pass = (end_bit - begin_bit + 7) / 8;
+    const int width = n_pass ? (end_bit - begin_bit + n_pass - 1) / n_pass : 8;
+    for (int shift = begin_bit; shift < end_bit; shift += width) {
         const int bits = (end_bit - shift) < width ? (end_bit - shift) : width;
         const uint32_t mask = (1u << bits) - 1u;
         uint32_t* ki = cur ? k1 : k0;

@@ -57,7 +57,7 @@ inline SplatLayout splat_layout_n(uint32_t N, uint32_t n_tiles, size_t n_px, uin
     L.blend_rec = c.take<float4>(size_t(N) * 2);
     L.tile_order = c.take<uint32_t>(n_tiles);
     L.stats = c.take<uint32_t>(4);
-    carve_binning_gaussians(c, L.bin, N);
+    carve_binning_gaussians(c, L.bin, N, n_tiles);
     L.bytes = c.off;
     Carver cp;
     cp.base = static_cast<char*>(pair_base);
@@ -646,7 +646,7 @@ dgmr_status dgmr_splat_workspace_views(int32_t n_gaussians, int32_t width, int32
     if (frame_workspace_bytes < L.bytes || pair_workspace_bytes < L.pair_bytes)
         return DGMR_ERR_WORKSPACE;
     const uint32_t gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
-    const int par = tile_sort_parity(gx * gy);
+    const int par = tile_sort_parity(super_count(gx, gy));
     views->rects = L.rects;
     views->rgb = L.rgb;
     views->rgb_sh_clamped = L.clamped;
@@ -736,7 +736,7 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
         return DGMR_ERR_WORKSPACE;
     const CameraT<float> cam = make_camera<float>(*camera);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const int par = tile_sort_parity(cam.gx * cam.gy);
+    const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
     k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
         L.tile_order, single_frame(cam, framebuffer, L));
     note_launch();
@@ -761,7 +761,7 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
         return DGMR_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const CameraT<float> cam = make_camera<float>(*camera);
-    const int par = tile_sort_parity(cam.gx * cam.gy);
+    const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
     k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc,
         single_frame(cam, nullptr, L, grad_framebuffer));
@@ -821,9 +821,10 @@ struct BatchView {
 };
 
 struct BatchTable {
-    uint32_t n_views, n_scenes, G, n_tiles;
+    uint32_t n_views, n_scenes, G, n_tiles, n_stiles;
     uint32_t g_off[kMaxBatchViews + 1];
     uint32_t tile_off[kMaxBatchViews + 1];
+    uint32_t stile_off[kMaxBatchViews + 1]; // first super-tile of each view
     uint32_t scene_off[kMaxBatchScenes + 1];
     uint8_t view_by_scene[kMaxBatchViews];
     float* final_T;
@@ -847,7 +848,12 @@ struct BatchTable {
     __device__ __forceinline__ TileGrid grid(uint32_t g) const
     {
         const uint32_t v = owner(g_off, n_views, g);
-        return TileGrid { views[v].cam.gx, views[v].cam.gy, tile_off[v] };
+        return TileGrid { views[v].cam.gx, views[v].cam.gy, tile_off[v], stile_off[v] };
+    }
+    __device__ __forceinline__ TileGrid super_grid(uint32_t s) const
+    {
+        const uint32_t v = owner(stile_off, n_views, s);
+        return TileGrid { views[v].cam.gx, views[v].cam.gy, tile_off[v], stile_off[v] };
     }
     __device__ __forceinline__ FrameRef frame(uint32_t t) const
     {
@@ -937,7 +943,7 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
     std::memset(&t, 0, sizeof(t));
     t.n_views = uint32_t(n_views);
     t.n_scenes = uint32_t(n_scenes);
-    uint64_t G = 0, T = 0, px = 0, gs = 0;
+    uint64_t G = 0, T = 0, ST = 0, px = 0, gs = 0;
     for (int s = 0; s < n_scenes; ++s) {
         const dgmr_scene& sc = scenes[s];
         if (sc.dtype != DGMR_F32 || sc.n_gaussians < 0 || sc.sh_stride < 1 || sc.sh_stride > 16 || sc.sh_degree < 0 || sc.sh_degree > 3
@@ -995,13 +1001,18 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
         w.px_off = size_t(px);
         t.g_off[v] = uint32_t(G);
         t.tile_off[v] = uint32_t(T);
+        t.stile_off[v] = uint32_t(ST);
         G += uint64_t(scenes[bv.scene].n_gaussians);
         T += uint64_t(w.cam.gx) * w.cam.gy;
+        ST += super_count(w.cam.gx, w.cam.gy);
         px += uint64_t(c.width) * uint64_t(c.height);
     }
     t.g_off[n_views] = uint32_t(G);
     t.tile_off[n_views] = uint32_t(T);
-    if (G > 0x7fffffffull || T > (1ull << 30) || gs > 0x7fffffffull)
+    t.stile_off[n_views] = uint32_t(ST);
+    t.n_stiles = uint32_t(ST);
+    // super-tile ids share a 32-bit sort key with a 12-bit rectangle
+    if (G > 0x7fffffffull || T > (1ull << 30) || ST >= (1ull << 20) || gs > 0x7fffffffull)
         return DGMR_ERR_BAD_ARG;
     t.G = uint32_t(G);
     t.n_tiles = uint32_t(T);
@@ -1097,7 +1108,7 @@ dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes,
     uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
     const uint32_t G = plan.tab.G, cap = uint32_t(pair_capacity);
     batch_preprocess(plan, st_dev, s);
-    const int par = run_binning_grids<float>(G, plan.tab.n_tiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev,
+    const int par = run_binning_grids<float>(G, plan.tab.n_tiles, plan.tab.n_stiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev,
         num_sms(), s, true);
     k_tile_order<<<1, 1024, 0, s>>>(L.ranges, plan.tab.n_tiles, L.tile_order);
     k_splat_blend<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab);
@@ -1124,7 +1135,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     const uint32_t n_scene_gaussians = plan.tab.scene_off[n_scenes];
     if (n_scene_gaussians == 0)
         return DGMR_OK;
-    const int par = tile_sort_parity(plan.tab.n_tiles);
+    const int par = tile_sort_parity(plan.tab.n_stiles);
     cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
     k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc, plan.tab);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
