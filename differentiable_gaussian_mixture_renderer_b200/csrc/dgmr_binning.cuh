@@ -206,23 +206,30 @@ __device__ __forceinline__ TileRect super_rect(const TileRect& r)
     return TileRect { r.x0 / kSuper, r.y0 / kSuper, (r.x1 - 1) / kSuper + 1, (r.y1 - 1) / kSuper + 1 };
 }
 
-// Super-tiles touched by the j-th Gaussian in depth order.
+// Super-tiles touched by the j-th Gaussian in depth order, and its tile
+// rectangle in depth order (x0 | y0 << 16, x1 | y1 << 16), so that the
+// emission reads it contiguously.
 template <class T, class Grids>
 static __global__ void k_super_counts(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tiles_touched, const int32_t* __restrict__ rects,
-    const T* __restrict__ xy, uint32_t N, uint32_t* __restrict__ cnt_sorted, uint32_t* __restrict__ stats, const __grid_constant__ Grids grids)
+    const T* __restrict__ xy, uint32_t N, uint32_t* __restrict__ cnt_sorted, uint32_t* __restrict__ rect_lo, uint32_t* __restrict__ rect_hi,
+    uint32_t* __restrict__ stats, const __grid_constant__ Grids grids)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N)
         return;
     uint32_t g = perm[j];
     uint32_t c = 0;
+    TileRect r = { 0, 0, 0, 0 };
     if (g < N) {
-        const TileRect sr = super_rect(checked_rect(g, tiles_touched, rects, xy, grids.grid(g), stats));
+        r = checked_rect(g, tiles_touched, rects, xy, grids.grid(g), stats);
+        const TileRect sr = super_rect(r);
         c = (sr.x1 - sr.x0) * (sr.y1 - sr.y0);
     } else {
         flag_bounds(stats, 0x21u);
     }
     cnt_sorted[j] = c;
+    rect_lo[j] = r.x0 | (r.y0 << 16);
+    rect_hi[j] = r.x1 | (r.y1 << 16);
 }
 
 // n_sort[1] = super-tile entries to sort = min(total, cap)
@@ -240,10 +247,10 @@ static __global__ void k_super_total(const uint32_t* __restrict__ off_sorted, ui
 // together: in each round lane l takes slot base + l and finds its owner --
 // the first lane whose inclusive end exceeds the slot -- by a five-step
 // binary search over the lanes' ends, done with shuffles.
-template <class T, class Grids>
+template <class Grids>
 static __global__ void __launch_bounds__(256) k_emit_super(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ cnt_sorted,
-    const uint32_t* __restrict__ off_sorted, const uint32_t* __restrict__ tiles_touched, const int32_t* __restrict__ rects, const T* __restrict__ xy,
-    uint32_t N, uint32_t cap, uint32_t* __restrict__ skey, uint32_t* __restrict__ sval, uint32_t* __restrict__ stats, const __grid_constant__ Grids grids)
+    const uint32_t* __restrict__ off_sorted, const uint32_t* __restrict__ rect_lo, const uint32_t* __restrict__ rect_hi, uint32_t N, uint32_t cap,
+    uint32_t* __restrict__ skey, uint32_t* __restrict__ sval, uint32_t* __restrict__ stats, const __grid_constant__ Grids grids)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -259,7 +266,8 @@ static __global__ void __launch_bounds__(256) k_emit_super(const uint32_t* __res
             g = perm[j];
             if (g < N) {
                 tg = grids.grid(g);
-                tr = checked_rect(g, tiles_touched, rects, xy, tg, stats);
+                const uint32_t lo = rect_lo[j], hi = rect_hi[j];
+                tr = TileRect { lo & 0xffffu, lo >> 16, hi & 0xffffu, hi >> 16 };
                 sr = super_rect(tr);
                 if ((sr.x1 - sr.x0) * (sr.y1 - sr.y0) != c) {
                     flag_bounds(stats, 0x26u);
@@ -753,16 +761,18 @@ inline int run_binning_grids(uint32_t N, uint32_t n_tiles, uint32_t n_super, con
     note_launch();
     const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s, stats);
     const uint32_t* perm = dpar ? b.perm_tmp : b.perm;
+    // the pair of N-sized buffers the depth sort did not end in holds the rectangles
+    uint32_t* rect_lo = dpar ? b.depth_key : b.key_tmp;
+    uint32_t* rect_hi = dpar ? b.perm : b.perm_tmp;
     const uint32_t blocks = (N + 255) / 256;
-    k_super_counts<T, Grids><<<blocks, 256, 0, s>>>(perm, tiles_touched, rects, xy, N, b.cnt_sorted, stats, grids);
+    k_super_counts<T, Grids><<<blocks, 256, 0, s>>>(perm, tiles_touched, rects, xy, N, b.cnt_sorted, rect_lo, rect_hi, stats, grids);
     inclusive_scan_u32(b.cnt_sorted, b.off_sorted, N, b.scan_tmp, s);
     k_super_total<<<1, 1, 0, s>>>(b.off_sorted, N, cap, b.n_sort);
     note_launch(2);
     cudaMemsetAsync(b.super_ranges, 0, size_t(n_super) * 2 * sizeof(int32_t), s);
     cudaMemsetAsync(b.tile_total, 0, size_t(n_tiles) * sizeof(uint32_t), s);
     if (cap > 0) {
-        k_emit_super<T, Grids><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, tiles_touched, rects, xy, N, cap, b.pair_tile[0], b.pair_val[0], stats,
-            grids);
+        k_emit_super<Grids><<<blocks, 256, 0, s>>>(perm, b.cnt_sorted, b.off_sorted, rect_lo, rect_hi, N, cap, b.pair_tile[0], b.pair_val[0], stats, grids);
         note_launch();
         const int spar = radix_sort_pairs(b.pair_tile[0], b.pair_val[0], b.pair_tile[1], b.pair_val[1], b.n_sort + 1, 0, cap,
             kRectBits + int(higher_msb(n_super)), b.sort_tmp, n_sms, s, stats, kRectBits);
