@@ -58,10 +58,11 @@ def parse():
     ap.add_argument("--slots", type=int, default=3, help="requests in flight")
     ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving"], default="served",
+    ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving", "configs"], default="served",
                     help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
                          "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512; "
-                         "serving: 8 scenes, Poisson 200 req/s, mixed resolutions, 20%% gradient requests")
+                         "serving: 8 scenes, Poisson 200 req/s, mixed resolutions, 20%% gradient requests; "
+                         "configs: per-call GPU and oracle timings of the parity configurations")
     return ap.parse_args()
 
 
@@ -659,6 +660,102 @@ def run_serving(args):
     return 0
 
 
+def run_configs(args):
+    """The parity configurations as per-call timings: splat forward 10k at
+    256x256, splat forward + backward 200k at 1024x1024, vol_marcher forward +
+    backward 100k at 512x512 -- each on the GPU (CUDA events around the calls,
+    median over the cameras) and on the host through the oracle (a bounded
+    sample: the first camera, or for the marcher a 128x128 frame of the same
+    scene whose time is scaled by the pixel count)."""
+    torch, dev, local = _gpu_common()
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200 import splat
+    from oracle import oracle as O
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
+    out = {}
+    n_cams = args.warmup + args.steps
+
+    def timed(fn):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        mid = fn(e1)
+        e2.record()
+        e2.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2), mid
+
+    for name, n, W, H, bwd in (("c0_splat_fwd_10k_256", 10_000, 256, 256, False),
+                               ("c1_splat_fwd_bwd_200k_1024", 200_000, 1024, 1024, True)):
+        sc = S.make_scene(n, seed=0, extent=2.0 if n == 200_000 else 1.0)
+        ins = (t(sc.sh), t(sc.weights), t(sc.centroids), t(sc.scales), t(sc.rotations))
+        cams = S.random_cameras(n_cams, W, H, seed=1)
+        G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
+        fw, bw = [], []
+        for k, cam in enumerate(cams):
+            def call(e_mid):
+                fb, frame = splat.splat_forward(*ins, cam.view, cam.proj, cam.campos, (0.0, 0.0, 0.0), W, H, cam.tan_fovx,
+                                                cam.tan_fovy, 0)
+                e_mid.record()
+                if bwd:
+                    splat.splat_backward(frame, G, *ins)
+                return frame
+            a, b, _ = timed(call)
+            if k >= args.warmup:
+                fw.append(a)
+                bw.append(b)
+        r = {"gpu_fwd_ms": statistics.median(fw)}
+        if bwd:
+            r["gpu_bwd_ms"] = statistics.median(bw)
+        if not args.no_cpu:
+            c0 = time.perf_counter()
+            ref = O.splat_forward(sc, cams[0])
+            c1 = time.perf_counter()
+            r["cpu_fwd_ms"] = (c1 - c0) * 1e3
+            if bwd:
+                O.splat_backward(sc, cams[0], ref, G.cpu().numpy())
+                r["cpu_bwd_ms"] = (time.perf_counter() - c1) * 1e3
+            r["cpu_cores"] = O.num_threads()
+        out[name] = r
+
+    n, W, H = 100_000, 512, 512
+    sc = S.make_scene(n, seed=0)
+    ins = (t(sc.sh), t(sc.weights).reshape(-1, 1), t(sc.centroids), t(sc.scales), t(sc.rotations))
+    cams = S.random_cameras(n_cams, W, H, seed=1)
+    G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
+    bg = torch.zeros(3, device=dev)
+    fw, bw = [], []
+    for k, cam in enumerate(cams):
+        v, pm, c = t(cam.view), t(cam.proj), t(cam.campos)
+
+        def call(e_mid):
+            cache = cpp_binding.forward(*ins, v, pm, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0)
+            e_mid.record()
+            cpp_binding.backward(*ins, v, pm, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache)
+            return cache
+        a, b, _ = timed(call)
+        if k >= args.warmup:
+            fw.append(a)
+            bw.append(b)
+    r = {"gpu_fwd_ms": statistics.median(fw), "gpu_bwd_ms": statistics.median(bw)}
+    if not args.no_cpu:
+        small = S.make_camera(128, 128, eye=tuple(cams[0].campos.tolist()))
+        c0 = time.perf_counter()
+        cache = O.vm_forward(sc, small)
+        c1 = time.perf_counter()
+        O.vm_backward(sc, small, cache, np.zeros((3, 128, 128), np.float32) + 1.0)
+        c2 = time.perf_counter()
+        scale = (W * H) / (128 * 128)
+        r.update(cpu_fwd_ms=(c1 - c0) * 1e3 * scale, cpu_bwd_ms=(c2 - c1) * 1e3 * scale, cpu_cores=O.num_threads(),
+                 cpu_sample="one 128x128 frame of the same scene from the first camera's position, x16 for 512x512")
+    out["c2_vol_marcher_fwd_bwd_100k_512"] = r
+    line = {"metric": "per-call ms of the parity configurations", "value": out["c1_splat_fwd_bwd_200k_1024"]["gpu_fwd_ms"],
+            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": "c0 / c1 / c2 per-call timings"},
+            "configs": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -669,6 +766,8 @@ def main():
         return run_marcher(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "configs":
+        return run_configs(args)
     return run_ours(args)
 
 
