@@ -25,10 +25,14 @@ constexpr unsigned kRayWarps = 4; // rays per block
 constexpr unsigned kRayRounds = 4; // 4 x 32 lanes >= 128 borders
 constexpr unsigned kRayMaskRegs = 4; // ray masks kept in registers: 4 x 32 batches of 32 entries
 
+// A ray's section set lives in shared memory, once per warp: lane 0 inserts,
+// every lane reads it after a __syncwarp (kept per lane, the 32 identical
+// copies and the insertion's scratch went to local memory).
 template <class T>
 struct RayWarpShared {
     T borders[kSmallSteps];
     Bin<T> bins[kSmallSteps]; // forward: (r, g, b, exp(-mass)); backward: (r, g, b, mass)
+    SectionSet<kLargeSteps, T> sec;
 };
 
 template <class T>
@@ -37,6 +41,7 @@ struct RayWarpSharedBwd {
     Bin<T> bins[kSmallSteps];
     Bin<T> gbins[kSmallSteps]; // bin adjoints
     int32_t queue[32]; // pass 3: list entries waiting for a lane
+    SectionSet<kLargeSteps, T> sec;
 };
 
 // The gates of both passes (see ray_can_use) as a 32-bit mask per batch of 32
@@ -132,14 +137,17 @@ __device__ __forceinline__ WarpRayMasks warp_ray_masks(const VmMarch<T>& a, int3
 namespace dgmr {
 
 // Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
-// intersected lane-parallel, then walked in list order by every lane alike.
+// intersected lane-parallel, then walked in list order; lane 0 inserts them
+// into the warp's section set (in shared memory), which every lane reads.
 template <class T>
 __device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
     const WarpRayMasks& rm, unsigned lane)
 {
     if (a.cs.n > 0) {
-        for (int i = 0; i < a.cs.n; ++i)
-            sec.put(Section<T> { a.cs.s[i][0], a.cs.s[i][1], a.cs.s[i][2] });
+        if (lane == 0)
+            for (int i = 0; i < a.cs.n; ++i)
+                sec.put(Section<T> { a.cs.s[i][0], a.cs.s[i][1], a.cs.s[i][2] });
+        __syncwarp();
         return;
     }
     unsigned i = 0;
@@ -172,7 +180,10 @@ __device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, co
             }
             if (!((okm >> j) & 1u))
                 continue;
-            sec.put(Section<T> { __shfl_sync(0xffffffffu, s0, j), __shfl_sync(0xffffffffu, s1, j), __shfl_sync(0xffffffffu, dt, j) });
+            const Section<T> sj = { __shfl_sync(0xffffffffu, s0, j), __shfl_sync(0xffffffffu, s1, j), __shfl_sync(0xffffffffu, dt, j) };
+            if (lane == 0)
+                sec.put(sj);
+            __syncwarp();
         }
         if (stop)
             break;
@@ -297,14 +308,16 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, 
     T tr = T(1);
     T start = T(0);
     T distance = T(0); // Depth mode
-    SectionSet<kLargeSteps, T> sec;
+    SectionSet<kLargeSteps, T>& sec = sm.sec;
     for (unsigned step = 0;; ++step) {
         if (step >= kMaxLargeSteps) {
             if (lane == 0)
                 atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
             break;
         }
-        sec.reset(start);
+        if (lane == 0)
+            sec.reset(start);
+        __syncwarp();
         warp_collect(sec, a, b, e, o, d, rm, lane);
         if (lane == 0)
             sample_positions(sec, sm.borders);
@@ -462,14 +475,16 @@ __global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp_bwd(VmMarch<T>
     const T gt = (gc.x * cam.bg[0] + gc.y * cam.bg[1]) + gc.z * cam.bg[2];
     T tr = T(1);
     T start = T(0);
-    SectionSet<kLargeSteps, T> sec;
+    SectionSet<kLargeSteps, T>& sec = sm.sec;
     for (unsigned step = 0;; ++step) {
         if (step >= kMaxLargeSteps) {
             if (lane == 0)
                 atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
             break;
         }
-        sec.reset(start);
+        if (lane == 0)
+            sec.reset(start);
+        __syncwarp();
         warp_collect(sec, a, b, e, o, d, rm, lane);
         if (lane == 0)
             sample_positions(sec, sm.borders);
