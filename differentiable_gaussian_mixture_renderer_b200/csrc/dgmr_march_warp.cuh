@@ -136,6 +136,36 @@ __device__ __forceinline__ WarpRayMasks warp_ray_masks(const VmMarch<T>& a, int3
 
 namespace dgmr {
 
+// SectionSet::put_leaves_unchanged (dgmr_sections.h) with lane i (< kLargeSteps)
+// testing section i: whether inserting s would leave the warp's set exactly as
+// it is, so that the insertion (and lane 0's serial walk) can be skipped.
+template <class T>
+__device__ __forceinline__ bool warp_section_covered(const SectionSet<kLargeSteps, T>& sec, const Section<T>& s, unsigned lane)
+{
+    const T cs = max_f(sec.lo, s.start), ce = min_f(sec.hi, s.end);
+    const unsigned n = sec.n;
+    if (n == kLargeSteps && sec.e[kLargeSteps - 1].end < sec.hi)
+        return false;
+    Section<T> my = { T(0), T(0), T(0) };
+    if (lane < n)
+        my = sec.e[lane];
+    const bool ov = lane < n && my.end > cs && my.start < ce;
+    const uint32_t ovm = __ballot_sync(0xffffffffu, ov);
+    const T next_start = __shfl_down_sync(0xffffffffu, my.start, 1);
+    const T next_dt = __shfl_down_sync(0xffffffffu, my.delta_t, 1);
+    if (!ovm)
+        return false;
+    const unsigned f = unsigned(__ffs(int(ovm)) - 1), l = 31u - unsigned(__clz(int(ovm)));
+    bool bad = ov && my.delta_t > s.delta_t;
+    if (ov && lane < l && (my.end != next_start || (my.delta_t == s.delta_t && next_dt == s.delta_t)))
+        bad = true; // a gap, or two neighbours that the insertion would merge
+    if (lane == f && my.start > cs)
+        bad = true;
+    if (lane == l && my.end < ce)
+        bad = true;
+    return __ballot_sync(0xffffffffu, bad) == 0u;
+}
+
 // Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
 // intersected lane-parallel, then walked in list order; lane 0 inserts them
 // into the warp's section set (in shared memory), which every lane reads.
@@ -181,6 +211,10 @@ __device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, co
             if (!((okm >> j) & 1u))
                 continue;
             const Section<T> sj = { __shfl_sync(0xffffffffu, s0, j), __shfl_sync(0xffffffffu, s1, j), __shfl_sync(0xffffffffu, dt, j) };
+            // put() returns at once for a section outside [lo, hi) and leaves the
+            // set unchanged for a covered one: skip both without the call
+            if (sj.end <= sec.lo || sj.start >= sec.hi || warp_section_covered(sec, sj, lane))
+                continue;
             if (lane == 0)
                 sec.put(sj);
             __syncwarp();
@@ -292,7 +326,7 @@ __device__ __forceinline__ void warp_store_bins(Bin<T>* bins, const Bin<T> (&acc
 }
 
 template <class T>
-__global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_march_warp(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
 {
     __shared__ RayWarpShared<T> shared_rays[kRayWarps];
     RayWarpShared<T>& sm = shared_rays[threadIdx.x >> 5];
@@ -455,7 +489,7 @@ __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders,
 
 // vol_marcher_backward.cu:115-319 with one warp per ray
 template <class T>
-__global__ void __launch_bounds__(kRayWarps * 32) k_vm_march_warp_bwd(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_march_warp_bwd(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
 {
     __shared__ RayWarpSharedBwd<T> shared_rays[kRayWarps];
     RayWarpSharedBwd<T>& sm = shared_rays[threadIdx.x >> 5];

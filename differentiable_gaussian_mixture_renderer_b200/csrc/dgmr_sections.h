@@ -55,6 +55,39 @@ struct SectionSet {
         out[1] = { out[0].end, out[2].start, min_f(a.delta_t, b.delta_t) };
     }
 
+    // Whether put(s) would leave the set exactly as it is, for an s that
+    // reaches into [lo, hi): the sections overlapping s (clipped to [lo, hi))
+    // cover it without a gap, none has a larger step, no two consecutive ones
+    // both have s's step (put would merge those), and a full set already has
+    // hi at its last end (put would pull hi in).  Then put only splits each
+    // covering section against s and merges the pieces back into it, bit for
+    // bit.  The marcher's device code skips such insertions (a lane-parallel
+    // form of this test); tests check the claim on random insertion sequences.
+    DGMR_HD bool put_leaves_unchanged(Section<T> s) const
+    {
+        const T cs = max_f(lo, s.start), ce = min_f(hi, s.end);
+        if (n == MAX && e[MAX - 1].end < hi)
+            return false;
+        unsigned f = n, l = n;
+        for (unsigned i = 0; i < n; ++i)
+            if (e[i].end > cs && e[i].start < ce) {
+                if (f == n)
+                    f = i;
+                l = i;
+            }
+        if (f == n)
+            return false;
+        if (e[f].start > cs || e[l].end < ce)
+            return false;
+        for (unsigned i = f; i <= l; ++i) {
+            if (e[i].delta_t > s.delta_t)
+                return false;
+            if (i < l && (e[i].end != e[i + 1].start || (e[i].delta_t == s.delta_t && e[i + 1].delta_t == s.delta_t)))
+                return false;
+        }
+        return true;
+    }
+
     DGMR_HD_NOINLINE void put(Section<T> s)
     {
         if (s.end <= lo)

@@ -4,6 +4,8 @@
 // can run them on the CPU, the way the reference's own unit tests run its
 // __host__ __device__ math on the host.
 #include <cstdlib>
+#include <cstring>
+#include <random>
 #include <vector>
 
 #include "../../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_sections.h"
@@ -200,3 +202,49 @@ void kat_rbs4(float sigma, float transmission_threshold, const float* adds, int 
 }
 
 } // extern "C"
+
+namespace {
+
+// Random insertion sequences (coarse values make equal ends and steps common):
+// for every insertion that SectionSet::put_leaves_unchanged accepts, the set
+// after put must be the set before, bit for bit.  Returns the mismatches;
+// *covered counts the accepted insertions.
+template <class T>
+long check_unchanged(unsigned seed, int trials, long* covered)
+{
+    std::mt19937 rng(seed);
+    long bad = 0, cov = 0;
+    for (int trial = 0; trial < trials; ++trial) {
+        dgmr::SectionSet<16, T> sec;
+        sec.reset(T(rng() % 3) * T(0.5));
+        const int n_put = 5 + int(rng() % 60);
+        for (int k = 0; k < n_put; ++k) {
+            T c = T(std::uniform_real_distribution<double>(0.0, 10.0)(rng));
+            T w = T(0.05 + std::uniform_real_distribution<double>(0.0, 2.0)(rng));
+            if (rng() % 2) {
+                c = T(int(c * T(4))) / T(4);
+                w = T(1 + rng() % 8) / T(4);
+            }
+            const T dt = (rng() % 3 == 0) ? T(1 + rng() % 4) / T(32) : w / T(31);
+            const dgmr::Section<T> s { c - w, c + w, dt };
+            const bool reaches = !(s.end <= sec.lo || s.start >= sec.hi);
+            const bool same_claim = reaches && sec.put_leaves_unchanged(s);
+            const dgmr::SectionSet<16, T> before = sec;
+            sec.put(s);
+            if (!same_claim)
+                continue;
+            ++cov;
+            bool same = before.n == sec.n && before.lo == sec.lo && before.hi == sec.hi;
+            for (unsigned q = 0; same && q < sec.n; ++q)
+                same = std::memcmp(&before.e[q], &sec.e[q], sizeof(dgmr::Section<T>)) == 0;
+            bad += same ? 0 : 1;
+        }
+    }
+    *covered = cov;
+    return bad;
+}
+
+} // namespace
+
+extern "C" long kat_section_unchanged_f32(unsigned seed, int trials, long* covered) { return check_unchanged<float>(seed, trials, covered); }
+extern "C" long kat_section_unchanged_f64(unsigned seed, int trials, long* covered) { return check_unchanged<double>(seed, trials, covered); }

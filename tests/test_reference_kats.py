@@ -310,3 +310,19 @@ def test_deterministic_exp_log_erf_error_bounds():
     refe = np.array([math.erf(float(v)) for v in xe])
     gote = O.fmath("erf", xe).astype(np.float64)
     assert np.max(np.abs(gote - refe)) < 2.5e-7  # Abramowitz & Stegun 7.1.26 bound 1.5e-7 plus float rounding
+
+
+@pytest.mark.parametrize("suffix", ["f32", "f64"])
+def test_insertions_claimed_unchanged_leave_the_set_unchanged(shim, suffix):
+    """The volume marcher skips a section insertion that
+    SectionSet::put_leaves_unchanged accepts (its device form tests the same
+    conditions lane-parallel).  On random insertion sequences built to make
+    equal ends and equal steps common, every accepted insertion must leave the
+    set bit for bit as it was, and a good share of insertions must be accepted."""
+    f = getattr(shim, f"kat_section_unchanged_{suffix}")
+    f.restype = C.c_long
+    f.argtypes = [C.c_uint, C.c_int, C.POINTER(C.c_long)]
+    covered = C.c_long(0)
+    bad = f(11, 20000, C.byref(covered))
+    assert bad == 0
+    assert covered.value > 100000
