@@ -188,6 +188,27 @@ struct PixelState {
     bool done;
 };
 
+// blend_step after the cutoff test, given exp(-q/2) (splat_forward.cu:303-321)
+__device__ __forceinline__ void blend_alpha(PixelState& ps, float ex, float opacity, float r, float g, float b, int32_t idx)
+{
+    if (ps.done)
+        return;
+    const float alpha = min_f(0.99f, opacity * ex);
+    if (alpha < 1.0f / 255.0f)
+        return;
+    const float test_T = ps.T * (1.f - alpha);
+    if (test_T < 0.0001f) {
+        ps.done = true;
+        return;
+    }
+    const float w = alpha * ps.T;
+    ps.c0 = __fmaf_rn(r, w, ps.c0);
+    ps.c1 = __fmaf_rn(g, w, ps.c1);
+    ps.c2 = __fmaf_rn(b, w, ps.c2);
+    ps.T = test_T;
+    ps.last = idx;
+}
+
 __device__ __forceinline__ void blend_step(PixelState& ps, float q, float qcut, float opacity, float r, float g, float b, int32_t idx)
 {
     if (ps.done || q > qcut)
@@ -345,16 +366,33 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
         }
         __syncthreads();
         if (!p0.done) {
-            for (int j = 0; j < n; ++j) {
-                const float4 a0 = s_r0[j];
-                const float4 a1 = s_r1[j];
+            // two records per iteration: their quadratic forms and exps are
+            // independent and overlap; the blend steps still run in list order
+            int j = 0;
+            for (; j + 1 < n; j += 2) {
+                const float4 a0 = s_r0[j], a1 = s_r1[j];
+                const float4 b0 = s_r0[j + 1], b1 = s_r1[j + 1];
                 float dx, dy;
-                const float q0 = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
-                if (q0 > a1.z)
+                const float qa = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
+                const float qb = splat_q(b0, b1.x, fpx, fpy, &dx, &dy);
+                const bool ua = !(qa > a1.z), ub = !(qb > b1.z);
+                if (!(ua || ub))
                     continue;
-                blend_step(p0, q0, a1.z, a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
+                const float ea = ua ? dgmr_fm::exp_f_nonpos(-0.5f * qa) : 0.f;
+                const float eb = ub ? dgmr_fm::exp_f_nonpos(-0.5f * qb) : 0.f;
+                if (ua)
+                    blend_alpha(p0, ea, a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
+                if (ub)
+                    blend_alpha(p0, eb, b1.y, s_rgb[0][j + 1], s_rgb[1][j + 1], s_rgb[2][j + 1], __float_as_int(b1.w));
                 if (p0.done)
                     break;
+            }
+            if (j < n && !p0.done) {
+                const float4 a0 = s_r0[j], a1 = s_r1[j];
+                float dx, dy;
+                const float q0 = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
+                if (!(q0 > a1.z))
+                    blend_alpha(p0, dgmr_fm::exp_f_nonpos(-0.5f * q0), a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
             }
         }
         __syncthreads();

@@ -248,3 +248,26 @@ long check_unchanged(unsigned seed, int trials, long* covered)
 
 extern "C" long kat_section_unchanged_f32(unsigned seed, int trials, long* covered) { return check_unchanged<float>(seed, trials, covered); }
 extern "C" long kat_section_unchanged_f64(unsigned seed, int trials, long* covered) { return check_unchanged<double>(seed, trials, covered); }
+
+// exp_f_nonpos against exp_f, bit for bit, on every float in [lo, hi] stepped
+// by `stride` representable values, plus special values.  Returns mismatches.
+extern "C" long kat_exp_nonpos_mismatches(float lo, float hi, unsigned stride)
+{
+    long bad = 0;
+    const float special[] = { 0.0f, -0.0f, -87.0f, -87.5f, -88.0f, -104.0f, -1e30f, 1e-30f, 0.5f, 88.0f, 89.0f };
+    for (float x : special) {
+        const float a = dgmr_fm::exp_f(x), b = dgmr_fm::exp_f_nonpos(x);
+        bad += std::memcmp(&a, &b, sizeof(float)) != 0;
+    }
+    for (float x = lo; x <= hi;) {
+        const float a = dgmr_fm::exp_f(x), b = dgmr_fm::exp_f_nonpos(x);
+        bad += std::memcmp(&a, &b, sizeof(float)) != 0;
+        uint32_t u;
+        std::memcpy(&u, &x, sizeof(u));
+        u = (x < 0.0f) ? (u >= stride ? u - stride : 0u) : u + stride; // toward +inf by stride ulps
+        if (x < 0.0f && u == 0u)
+            u = 0u;
+        std::memcpy(&x, &u, sizeof(u));
+    }
+    return bad;
+}

@@ -326,3 +326,11 @@ def test_insertions_claimed_unchanged_leave_the_set_unchanged(shim, suffix):
     bad = f(11, 20000, C.byref(covered))
     assert bad == 0
     assert covered.value > 100000
+
+
+def test_range_specialised_exp_is_bit_identical(shim):
+    """The blend's exp_f_nonpos must return exp_f's bits for every input."""
+    f = shim.kat_exp_nonpos_mismatches
+    f.restype = C.c_long
+    f.argtypes = [C.c_float, C.c_float, C.c_uint]
+    assert f(-100.0, 2.0, 97) == 0
