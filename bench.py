@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--batch", type=int, default=8, help="requests per step")
-    ap.add_argument("--slots", type=int, default=3, help="requests in flight")
+    ap.add_argument("--slots", type=int, default=4, help="requests in flight")
     ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving", "configs"], default="served",
