@@ -80,7 +80,7 @@ struct BinningBuffers {
     uint32_t* cnt_sorted; // [N] super-tiles touched, in depth order
     uint32_t* off_sorted; // [N] their inclusive scan
     uint32_t* scan_tmp; // scan_temp_bytes(max(N, n_tiles))
-    uint32_t* n_sort; // [4] min(P, cap), super entries to sort, chunk count, spare
+    uint32_t* n_sort; // [8] min(P, cap), super entries to sort, chunk count, spare, depth-key min / max
     int32_t* super_ranges; // [n_tiles, 2] each super-tile's entries in the sorted list
     uint32_t* chunk_base; // [n_tiles + 1] first chunk of each super-tile
     uint32_t* tile_total; // [n_tiles] pairs per tile
@@ -117,7 +117,7 @@ inline void carve_binning_gaussians(Carver& c, BinningBuffers& b, uint32_t N, ui
     b.cnt_sorted = c.take<uint32_t>(N);
     b.off_sorted = c.take<uint32_t>(N);
     b.scan_tmp = c.take<uint32_t>(scan_temp_bytes(N > n_tiles ? N : n_tiles) / 4 + 1);
-    b.n_sort = c.take<uint32_t>(4);
+    b.n_sort = c.take<uint32_t>(8);
     b.super_ranges = c.take<int32_t>(size_t(n_tiles) * 2);
     b.chunk_base = c.take<uint32_t>(size_t(n_tiles) + 1);
     b.tile_total = c.take<uint32_t>(n_tiles);
@@ -160,6 +160,8 @@ inline int tile_sort_parity(uint32_t n_super)
 
 static __global__ void k_pair_count(const uint32_t* __restrict__ point_offsets, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, uint32_t* __restrict__ n_sort)
 {
+    n_sort[4] = 0xffffffffu; // depth-key range, filled by k_key_range
+    n_sort[5] = 0u;
     const uint32_t P = N ? point_offsets[N - 1] : 0u;
     stats[0] = P;
     if (P > cap)
@@ -759,7 +761,15 @@ inline int run_binning_grids(uint32_t N, uint32_t n_tiles, uint32_t n_super, con
         inclusive_scan_u32(tiles_touched, point_offsets, N, b.scan_tmp, s);
     k_pair_count<<<1, 1, 0, s>>>(point_offsets, N, cap, stats, b.n_sort);
     note_launch();
-    const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s, stats);
+    // the depth keys of the Gaussians that touch a tile usually span < 2^24
+    // values: rebased, the top pass only copies
+    {
+        const uint32_t want = (N + 255) / 256, limit = uint32_t(n_sms) * 8;
+        k_key_range<<<want < limit ? want : limit, 256, 0, s>>>(b.depth_key, tiles_touched, N, b.n_sort + 4);
+        note_launch();
+    }
+    const int dpar = radix_sort_pairs(b.depth_key, b.perm, b.key_tmp, b.perm_tmp, nullptr, N, N, 32, b.sort_tmp, n_sms, s, stats, 0, b.n_sort + 4,
+        tiles_touched);
     const uint32_t* perm = dpar ? b.perm_tmp : b.perm;
     // the pair of N-sized buffers the depth sort did not end in holds the rectangles
     uint32_t* rect_lo = dpar ? b.depth_key : b.key_tmp;
@@ -785,7 +795,12 @@ inline int run_binning_grids(uint32_t N, uint32_t n_tiles, uint32_t n_super, con
             stats, grids);
         k_chunk_prefix<Grids><<<n_super, kSuperTiles * kPrefixParts, 0, s>>>(b.chunk_base, n_super, rows, b.tile_total, n_tiles, stats, grids);
         note_launch(4);
-        inclusive_scan_u32(b.tile_total, b.tile_incl, n_tiles, b.scan_tmp, s);
+        if (n_tiles <= kScanSingleMax) {
+            k_scan_single<<<1, 1024, 0, s>>>(b.tile_total, n_tiles, b.tile_incl);
+            note_launch();
+        } else {
+            inclusive_scan_u32(b.tile_total, b.tile_incl, n_tiles, b.scan_tmp, s);
+        }
         k_tile_ranges_from_counts<<<(n_tiles + 255) / 256, 256, 0, s>>>(b.tile_total, b.tile_incl, n_tiles, cap, ranges);
         static bool smem_set = false; // one opt-in per instantiation, above the 48 KB default
         if (!smem_set) {

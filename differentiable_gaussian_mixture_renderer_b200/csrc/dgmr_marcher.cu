@@ -56,7 +56,7 @@ inline VmLayout<T> vm_layout(uint32_t N, uint32_t n_tiles, uint32_t cap, void* b
     Carver c;
     c.base = static_cast<char*>(base);
     L.stats = c.take<uint32_t>(4);
-    L.pre_scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 1);
+    L.pre_scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 8); // + room for k_pair_count's eight counters
     L.pre_bytes = c.off;
     L.acc = c.take<T>(size_t(N) * 10);
     carve_binning(c, L.bin, N, n_tiles, cap);

@@ -154,10 +154,65 @@ static __global__ void k_scan_apply(const uint32_t* __restrict__ in, uint32_t n,
 
 // ---------------------------------------------------------------- radix sort
 // Histogram of one digit per tile: hist[d * tile_stride + tile].
-static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask,
-    uint32_t* __restrict__ hist, uint32_t tile_stride)
+// Key rebasing for a sort whose keys span a narrow range: range = {min, max}
+// over the keys that matter (live[i] != 0), or min > max when none does.  The
+// first pass replaces every key by key - min (a dead key by max - min) before
+// counting it; any pass whose digit is then zero for every key only copies.
+// The order of the live keys is unchanged (equal keys stay equal, the stable
+// passes keep their input order), so the sorted positions of the live items
+// are those of the full 32-bit sort.
+__device__ __forceinline__ bool range_rebases(const uint32_t* range) { return range && range[0] <= range[1]; }
+__device__ __forceinline__ bool pass_is_copy(const uint32_t* range, int shift)
+{
+    return range_rebases(range) && ((range[1] - range[0]) >> shift) == 0u;
+}
+
+// min / max of the live keys into range (initialised to {~0, 0})
+static __global__ void k_key_range(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ live, uint32_t n, uint32_t* __restrict__ range)
+{
+    uint32_t lo = 0xffffffffu, hi = 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (live[i]) {
+            const uint32_t k = keys[i];
+            lo = k < lo ? k : lo;
+            hi = k > hi ? k : hi;
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    // one pair of atomics per block (per warp, they serialised on two addresses)
+    __shared__ uint32_t s_lo[32], s_hi[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = int(blockDim.x >> 5);
+    if (lane == 0) {
+        s_lo[warp] = lo;
+        s_hi[warp] = hi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        lo = lane < n_warps ? s_lo[lane] : 0xffffffffu;
+        hi = lane < n_warps ? s_hi[lane] : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0 && lo <= hi) {
+            atomicMin(&range[0], lo);
+            atomicMax(&range[1], hi);
+        }
+    }
+}
+
+static __global__ void k_radix_hist(uint32_t* __restrict__ keys, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask,
+    uint32_t* __restrict__ hist, uint32_t tile_stride, const uint32_t* __restrict__ range, const uint32_t* __restrict__ live, bool rebase)
 {
     __shared__ uint32_t h[kSortWarps][kSortBins];
+    if (pass_is_copy(range, shift))
+        return;
+    const bool rb = rebase && range_rebases(range);
+    const uint32_t kmin = rb ? range[0] : 0u, kspan = rb ? range[1] - range[0] : 0u;
     const uint32_t n = dev_count(n_dev, n_static, capacity);
     const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -170,8 +225,14 @@ static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, const uin
 #pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
             const uint32_t idx = base + r * 32 + lane;
-            if (idx < n)
-                atomicAdd(&h[warp][(keys[idx] >> shift) & mask], 1u);
+            if (idx < n) {
+                uint32_t k = keys[idx];
+                if (rb) {
+                    k = live[idx] ? k - kmin : kspan;
+                    keys[idx] = k;
+                }
+                atomicAdd(&h[warp][(k >> shift) & mask], 1u);
+            }
         }
         __syncthreads();
         uint32_t t = 0;
@@ -185,10 +246,12 @@ static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, const uin
 
 // Exclusive scan of each digit's row over tiles; row totals to digit_total.
 static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, uint32_t tile_stride,
-    uint32_t* __restrict__ digit_total)
+    uint32_t* __restrict__ digit_total, const uint32_t* __restrict__ range, int shift)
 {
     __shared__ uint32_t warp_tot[kSortWarps];
     __shared__ uint32_t carry;
+    if (pass_is_copy(range, shift))
+        return;
     const uint32_t n = dev_count(n_dev, n_static, capacity);
     const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
     uint32_t* row = hist + size_t(blockIdx.x) * tile_stride;
@@ -234,7 +297,8 @@ static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint
 // run (coalesced), instead of every lane storing into a different bucket.
 static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int shift, uint32_t mask,
-    const uint32_t* __restrict__ hist, uint32_t tile_stride, const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ stats)
+    const uint32_t* __restrict__ hist, uint32_t tile_stride, const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ stats,
+    const uint32_t* __restrict__ range)
 {
     __shared__ uint32_t wcount[kSortWarps][kSortBins];
     __shared__ uint32_t gbase[kSortBins]; // global start of this tile's run of each digit
@@ -244,6 +308,13 @@ static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __
     __shared__ uint32_t s_key[kSortTile];
     __shared__ uint32_t s_val[kSortTile];
     const uint32_t n = dev_count(n_dev, n_static, capacity);
+    if (pass_is_copy(range, shift)) {
+        // every key has digit 0 here and in every later pass: the order stays and
+        // no later pass reads the keys, so only the values move
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            vals_out[i] = vals_in[i];
+        return;
+    }
     const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -345,9 +416,12 @@ inline size_t radix_temp_bytes(uint32_t capacity)
 // Stable sort of (keys, vals) by key bits [begin_bit, end_bit).  The data
 // ping-pongs between (k0, v0) and (k1, v1); returns 0 if the result is in
 // k0/v0, 1 if in k1/v1.  n comes from *n_dev (device) when non-null, else
-// n_static.
+// n_static.  With range / live (see k_key_range) the keys are rebased in place
+// by the first pass and passes over all-zero digits copy the values only; the
+// sorted keys are then not produced (only the values' order is).
 inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, const uint32_t* n_dev, uint32_t n_static, uint32_t capacity, int end_bit,
-    void* temp, int n_sms, cudaStream_t stream, uint32_t* stats = nullptr, int begin_bit = 0)
+    void* temp, int n_sms, cudaStream_t stream, uint32_t* stats = nullptr, int begin_bit = 0, const uint32_t* range = nullptr,
+    const uint32_t* live = nullptr)
 {
     const uint32_t tiles = (capacity + kSortTile - 1) / kSortTile;
     if (tiles == 0)
@@ -369,13 +443,45 @@ inline int radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* 
         uint32_t* vi = cur ? v1 : v0;
         uint32_t* ko = cur ? k0 : k1;
         uint32_t* vo = cur ? v0 : v1;
-        k_radix_hist<<<grid, kSortThreads, 0, stream>>>(ki, n_dev, n_static, capacity, shift, mask, hist, stride);
-        k_radix_scan_rows<<<kSortBins, kSortThreads, 0, stream>>>(hist, n_dev, n_static, capacity, stride, dtotal);
-        k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal, stats);
+        k_radix_hist<<<grid, kSortThreads, 0, stream>>>(ki, n_dev, n_static, capacity, shift, mask, hist, stride, range, live, shift == begin_bit);
+        k_radix_scan_rows<<<kSortBins, kSortThreads, 0, stream>>>(hist, n_dev, n_static, capacity, stride, dtotal, range, shift);
+        k_radix_scatter<<<grid, kSortThreads, 0, stream>>>(ki, vi, ko, vo, n_dev, n_static, capacity, shift, mask, hist, stride, dtotal, stats, range);
         note_launch(3);
         cur ^= 1;
     }
     return cur;
+}
+
+// inclusive scan of n <= 32 * 1024 u32 in one block (one launch instead of
+// three for short arrays): thread t owns a contiguous run of ceil(n / 1024)
+// items, sums it, the 1024 sums are scanned once, then each run is written.
+constexpr uint32_t kScanSingleMax = 32u * 1024u;
+static __global__ void __launch_bounds__(1024) k_scan_single(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t warp_tot[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t per = (n + 1023u) / 1024u;
+    const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+    uint32_t v = 0;
+    for (uint32_t i = b; i < e; ++i)
+        v += in[i];
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        warp_tot[warp] = x;
+    __syncthreads();
+    uint32_t run = x - v;
+    for (int w = 0; w < warp; ++w)
+        run += warp_tot[w];
+    for (uint32_t i = b; i < e; ++i) {
+        run += in[i];
+        out[i] = run;
+    }
 }
 
 inline size_t scan_temp_bytes(uint32_t n) { return ((size_t(n) + kSortTile - 1) / kSortTile + 1) * sizeof(uint32_t); }
