@@ -149,7 +149,12 @@ DGMR_HD float exp_f_nonpos(float x)
     const float log2e = 1.44269504088896341f;
     const float ln2_hi = 0.693145751953125f;
     const float ln2_lo = 1.42860682030941723e-06f;
-    const float n = rint_f(x * log2e);
+    // rint by the 1.5 * 2^23 shift (ties to even, exact for |t| < 2^22), and the
+    // integer read from the shifted value's low bits: no conversion instructions
+    const float magic = 12582912.0f;
+    const float tm = x * log2e + magic;
+    const float n = tm - magic;
+    const int ni = int(float_to_bits(tm)) - int(float_to_bits(magic));
     float r = fma_f(-n, ln2_hi, x);
     r = fma_f(-n, ln2_lo, r);
     float p = 1.98412698412698413e-04f;
@@ -160,7 +165,7 @@ DGMR_HD float exp_f_nonpos(float x)
     p = fma_f(p, r, 0.5f);
     p = fma_f(p, r, 1.0f);
     p = fma_f(p, r, 1.0f);
-    return p * bits_to_float(uint32_t(int(n) + 127) << 23); // n in [-126, 0]
+    return p * bits_to_float(uint32_t(ni + 127) << 23); // n in [-126, 0]
 }
 
 DGMR_HD double exp_f(double x)

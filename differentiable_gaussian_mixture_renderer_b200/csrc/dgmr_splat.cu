@@ -421,11 +421,10 @@ __device__ __forceinline__ float warp_sum(float v)
 // summed over the warp with shuffles before one atomic per value.
 template <class Frames>
 __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
-    const float* __restrict__ xy, const float* __restrict__ conic_opacity, const float* __restrict__ rgb, float* __restrict__ acc,
-    const __grid_constant__ Frames frames)
+    const float4* __restrict__ rec, const float* __restrict__ rgb, float* __restrict__ acc, const __grid_constant__ Frames frames)
 {
-    __shared__ float2 s_xy[256];
-    __shared__ float4 s_co[256];
+    __shared__ float4 s_r0[256]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
+    __shared__ float4 s_r1[256];
     __shared__ float s_rgb[3][256];
     __shared__ uint32_t s_id[256];
     __shared__ int s_max;
@@ -465,8 +464,8 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
         if (k < hi) {
             const uint32_t id = list[b + k];
             s_id[threadIdx.x] = id;
-            s_xy[threadIdx.x] = reinterpret_cast<const float2*>(xy)[id];
-            s_co[threadIdx.x] = reinterpret_cast<const float4*>(conic_opacity)[id];
+            s_r0[threadIdx.x] = rec[2 * size_t(id)];
+            s_r1[threadIdx.x] = rec[2 * size_t(id) + 1];
             s_rgb[0][threadIdx.x] = rgb[3 * id];
             s_rgb[1][threadIdx.x] = rgb[3 * id + 1];
             s_rgb[2][threadIdx.x] = rgb[3 * id + 2];
@@ -477,11 +476,14 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
             float v[9] = { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f };
             bool any = false;
             if (kk < my_n) {
+                // the forward's cutoff: past q_cut alpha < 1/255, so exp is not needed
                 float dx, dy;
-                const float4 co = s_co[j];
-                const float g = splat_gauss(co, s_xy[j], fpx, fpy, &dx, &dy);
+                const float4 r0 = s_r0[j], r1 = s_r1[j];
+                const float q = splat_q(r0, r1.x, fpx, fpy, &dx, &dy);
+                const float4 co = make_float4(r0.z, 0.5f * r1.x, r0.w, r1.y); // conic a, b, c and opacity
+                const float g = q > r1.z ? 0.f : dgmr_fm::exp_f_nonpos(-0.5f * q);
                 const float alpha = min_f(0.99f, co.w * g);
-                if (!(alpha < 1.0f / 255.0f)) {
+                if (!(q > r1.z) && !(alpha < 1.0f / 255.0f)) {
                     any = true;
                     Tr = Tr / (1.f - alpha);
                     const float c0 = s_rgb[0][j], c1 = s_rgb[1][j], c2 = s_rgb[2][j];
@@ -801,7 +803,7 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
-    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc,
+    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc,
         single_frame(cam, nullptr, L, grad_framebuffer));
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
@@ -1175,7 +1177,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
         return DGMR_OK;
     const int par = tile_sort_parity(plan.tab.n_stiles);
     cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
-    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.xy, L.conic_opacity, L.rgb, L.grad_acc, plan.tab);
+    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, plan.tab);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
         nullptr, Formulation::Ots };
     k_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);
