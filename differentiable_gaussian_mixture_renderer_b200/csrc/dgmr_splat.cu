@@ -408,12 +408,29 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
     }
 }
 
-__device__ __forceinline__ float warp_sum(float v)
+// Sums of 9 per-lane values over a warp, scattered: halve the slots each lane
+// holds at every butterfly level (16 -> 8 -> 4 -> 2 -> 1, the upper half kept
+// by the lanes whose level bit is set), then add the partner's copy.  Lane l
+// returns the warp total of slot 8 b4 + 4 b3 + 2 b2 + b1 (b = the bits of l;
+// slots 9..15 are zero).
+__device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], int lane)
 {
+    float a[16];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+    for (int q = 0; q < 16; ++q)
+        a[q] = q < 9 ? v[q] : 0.f;
+#pragma unroll
+    for (int half = 8; half >= 1; half >>= 1) {
+        const int bit = half * 2; // the xor distance: 16, 8, 4, 2
+        const bool upper = (lane & bit) != 0;
+#pragma unroll
+        for (int q = 0; q < half; ++q) {
+            const float give = upper ? a[q] : a[q + half];
+            const float keep = upper ? a[q + half] : a[q];
+            a[q] = keep + __shfl_xor_sync(0xffffffffu, give, bit);
+        }
+    }
+    return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
 // Reverse-order blend adjoint: each pixel walks its contributors back to
@@ -507,16 +524,13 @@ __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restr
                 }
             }
             if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-                for (int q = 0; q < 9; ++q)
-                    v[q] = warp_sum(v[q]);
-                if (lane == 0) {
-                    float* dst = acc + size_t(s_id[j]) * 9;
-#pragma unroll
-                    for (int q = 0; q < 9; ++q)
-                        if (v[q] != 0.f)
-                            atomicAdd(dst + q, v[q]);
-                }
+                // reduce-scatter of the 9 partials over the warp (16 shuffles, not
+                // 9 x 5): lane l ends with the warp's sum of partial slot(l) and
+                // the lanes of slots 0..8 add them, one atomic each
+                float w = warp_reduce_scatter9(v, lane);
+                const int slot = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+                if ((lane & 1) == 0 && slot < 9 && w != 0.f)
+                    atomicAdd(acc + size_t(s_id[j]) * 9 + slot, w);
             }
         }
     }
