@@ -414,14 +414,14 @@ namespace dgmr {
 // over the bins in shared memory -- in bin order, so its sums round exactly
 // as the one-thread loop does -- then added to the per-Gaussian accumulators.
 template <class T>
-__device__ __forceinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, const Bin<T>* gbins, const T* borders, V3<T> o, V3<T> d)
+__device__ __forceinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, const Bin<T>* gbins, const T* borders, V3<T> o, V3<T> d, int live_end)
 {
     const RayEntry<T> en = load_entry(a, k);
     const V3<T> rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
     T g_mass = T(0);
     V3<T> grgb = { T(0), T(0), T(0) }, gmu = { T(0), T(0), T(0) };
     S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
-    grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ);
+    grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ, live_end);
     T* dst = a.acc + size_t(en.id) * 10;
     const T v[10] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5] };
 #pragma unroll
@@ -442,9 +442,12 @@ __device__ __forceinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, 
 // however sparse the ray's entries are in the tile list.  (Each Gaussian's
 // adjoint is independent of the others'; only the atomic additions of
 // different pixels meet, in no fixed order, as in the one-thread kernel.)
+// live_end: the bins from there on have zero adjoints (the ray stopped before
+// them), so a Gaussian whose live bins all lie there adds nothing and is not
+// queued (its atomics would all be skipped as zeros).
 template <class T>
 __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders, int32_t* queue, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
-    const WarpRayMasks& rm, unsigned lane)
+    const WarpRayMasks& rm, unsigned lane, int live_end)
 {
     unsigned i = 0, fill = 0;
     for (int32_t base = b; base < e; base += 32, ++i) {
@@ -457,6 +460,11 @@ __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders,
             Gauss1d<T> g;
             T sd, inv_sd, mor;
             ok = warp_entry_on_bins(en, o, d, borders, &g, &sd, &inv_sd, &mor);
+            if (ok && live_end < int(kBins)) {
+                int k0, k1;
+                live_bins(borders, g.centre, inv_sd, &k0, &k1);
+                ok = k0 < live_end;
+            }
         }
         const uint32_t okm = __ballot_sync(0xffffffffu, ok);
         const unsigned n_ok = unsigned(__popc(okm));
@@ -467,7 +475,7 @@ __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders,
         }
         __syncwarp();
         if (fill + n_ok >= 32) {
-            lane_grad_entry(a, queue[lane], gbins, borders, o, d);
+            lane_grad_entry(a, queue[lane], gbins, borders, o, d, live_end);
             __syncwarp();
             // the entries that did not fit go to the front of the emptied queue
             const unsigned left = fill + n_ok - 32;
@@ -483,7 +491,7 @@ __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders,
         }
     }
     if (lane < fill)
-        lane_grad_entry(a, queue[lane], gbins, borders, o, d);
+        lane_grad_entry(a, queue[lane], gbins, borders, o, d, live_end);
     __syncwarp();
 }
 
@@ -549,11 +557,12 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
                 break;
             }
         }
+        const int live_end = int(k);
         for (; k < kBins; ++k)
             if (lane == 0)
                 sm.gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
         __syncwarp();
-        warp_grad(sm.gbins, sm.borders, sm.queue, a, b, e, o, d, rm, lane);
+        warp_grad(sm.gbins, sm.borders, sm.queue, a, b, e, o, d, rm, lane, live_end);
         const bool done = sec.n == 0 || tr < T(1.f / 255.f);
         start = sm.borders[kSmallSteps - 1];
         __syncwarp();

@@ -99,7 +99,7 @@ __device__ __forceinline__ void live_bins(const T* borders, T c, T inv_sd, int* 
 // grad/math.h:559-620; accumulates into the outputs
 template <class T>
 __device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V3<T> o, V3<T> d, T mass, V3<T> rgb, const T* borders, const Bin<T>* gbins,
-    T* g_mass, V3<T>* g_rgb, V3<T>* g_mu, S3<T>* g_Q)
+    T* g_mass, V3<T>* g_rgb, V3<T>* g_mu, S3<T>* g_Q, int live_end = int(kBins))
 {
     const Gauss1d<T> g = intersect_with_ray_inv_C(mu, Q, o, d);
     T sd, mor;
@@ -114,6 +114,9 @@ __device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V
     V3<T> grgb = { 0, 0, 0 };
     int k0, k1;
     live_bins(borders, centre, inv_sd, &k0, &k1);
+    // bins from live_end on have zero adjoints (the ray stopped before them):
+    // they would add exact zeros
+    k1 = k1 < live_end - 1 ? k1 : live_end - 1;
     T cdf_start = cdf_inv_SD(centre, inv_sd, borders[k0]);
     for (int k = k0; k <= k1; ++k) {
         const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
