@@ -156,7 +156,7 @@ __device__ __forceinline__ void preprocess_one(const SplatPre& p, const CameraT<
     p.blend_rec[2 * o + 1] = make_float4(2.f * con.v[1], g.weight, q_cut, 0.f);
 }
 
-__global__ void __launch_bounds__(256) k_splat_preprocess(SplatPre p, CameraT<float> cam)
+__global__ void __launch_bounds__(256, 6) k_splat_preprocess(SplatPre p, CameraT<float> cam)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < p.N)
