@@ -572,7 +572,10 @@ static __global__ void k_tile_ranges_from_counts(const uint32_t* __restrict__ ti
 // (earlier lanes).  A round's pairs (typically ~1.5-2k) are first staged in
 // shared memory grouped by tile, then copied out run by run, so that
 // consecutive threads store consecutive addresses of one tile's run; a round
-// with more pairs than the stage holds writes them directly.
+// with more pairs than the stage holds writes them directly.  Three barriers
+// per round: after the ballots (which also ends the previous copy-out, so warp
+// 0 then advances the tile positions by the previous round's counts), after
+// the offsets, and after the staging.
 constexpr unsigned kEmitStage = 4096;
 template <class Grids>
 static __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval, uint32_t N,
@@ -612,8 +615,12 @@ static __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(const uint3
             const uint32_t b_hi = warp_bit_transpose(uint32_t(m >> 32), lane);
             bal[warp][lane] = b_lo;
             bal[warp][lane + 32] = b_hi;
-            __syncthreads();
+            __syncthreads(); // also ends the previous round's copy-out
             if (warp == 0) {
+                if (r0 != ch.a) { // the previous round's pairs advance each tile's position
+                    base[lane] += roff[lane + 1] - roff[lane];
+                    base[lane + 32] += roff[lane + 33] - roff[lane + 32];
+                }
                 // per tile: prefix over warps, then the exclusive scan over the 64 tiles
                 uint32_t run_lo = 0, run_hi = 0;
 #pragma unroll
@@ -634,6 +641,7 @@ static __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(const uint3
                     }
                 }
                 const uint32_t lo_total = __shfl_sync(0xffffffffu, x, 31);
+                __syncwarp(); // the base update above read the old offsets
                 roff[lane + 1] = x;
                 roff[lane + 33] = lo_total + y;
                 if (lane == 0)
@@ -673,11 +681,8 @@ static __global__ void __launch_bounds__(kChunkThreads) k_chunk_emit(const uint3
                     out_val[pos] = stage_val[i];
                 }
             }
-            __syncthreads();
-            if (threadIdx.x < kSuperTiles)
-                base[threadIdx.x] += roff[threadIdx.x + 1] - roff[threadIdx.x];
-            __syncthreads();
         }
+        __syncthreads(); // the last copy-out reads base and tile_id
     }
 }
 
