@@ -414,7 +414,7 @@ namespace dgmr {
 // over the bins in shared memory -- in bin order, so its sums round exactly
 // as the one-thread loop does -- then added to the per-Gaussian accumulators.
 template <class T>
-__device__ __forceinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, const Bin<T>* gbins, const T* borders, V3<T> o, V3<T> d, int live_end)
+__device__ __noinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, const Bin<T>* gbins, const T* borders, V3<T> o, V3<T> d, int live_end)
 {
     const RayEntry<T> en = load_entry(a, k);
     const V3<T> rgb = { a.rgb[3 * size_t(en.id)], a.rgb[3 * size_t(en.id) + 1], a.rgb[3 * size_t(en.id) + 2] };
