@@ -188,3 +188,24 @@ def test_vol_marcher_backward_matches_oracle(cuda, dtype):
     for name, g in zip(("sh", "weights", "centroids", "scales", "rotations"), grads):
         e = grad_err(g.cpu().numpy().reshape(gref[name].shape), gref[name])
         assert e <= GRAD_TOL, (name, e)
+
+
+def test_splat_large_frame_bit_exact(cuda):
+    """A 4096x2304 frame: 36,864 tiles (the three-launch tile scan, above the
+    one-block limit) and 576 super-tiles (two radix passes over the super-tile
+    entries instead of one) -- the point list, its tile ids, the ranges and
+    the image against the oracle."""
+    sc = S.make_scene(200_000, seed=9, extent=1.0)
+    cam = S.make_camera(4096, 2304, eye=(0.2, -0.1, -2.6))
+    ref = O.splat_forward(sc, cam)
+    fb, frame, _ = run_splat(sc, cam, cuda)
+    v = {k: t.cpu().numpy() for k, t in frame.views().items()}
+    P = ref["n_pairs"]
+    st = [int(x) for x in frame.stats.tolist()]
+    assert st[0] == P and st[1] == 0, f"stats {st}, oracle pairs {P}"
+    np.testing.assert_array_equal(v["i_ranges"], ref["i_ranges"])
+    np.testing.assert_array_equal(v["point_list"][:P].astype(np.uint32), ref["point_list"])
+    depth_bits = v["depths"].view(np.uint32)[v["point_list"][:P]]
+    keys = (v["point_list_tiles"][:P].astype(np.uint64) << np.uint64(32)) | depth_bits.astype(np.uint64)
+    np.testing.assert_array_equal(keys, ref["keys"])
+    assert np.abs(fb.cpu().numpy() - ref["fb"]).max() <= IMAGE_TOL
