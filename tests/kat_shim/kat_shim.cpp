@@ -271,3 +271,42 @@ extern "C" long kat_exp_nonpos_mismatches(float lo, float hi, unsigned stride)
     }
     return bad;
 }
+
+// Random insertion sequences into a set sitting in front of a guard region:
+// returns how many insertions left more than 16 sections or wrote past the
+// set.  (The marcher keeps one set per warp in shared memory, next to other
+// warps' data.)
+extern "C" long kat_section_overflows(unsigned seed, int trials)
+{
+    struct Guarded {
+        dgmr::SectionSet<16, float> s;
+        float guard[64];
+    };
+    std::mt19937 rng(seed);
+    long bad = 0;
+    for (int trial = 0; trial < trials; ++trial) {
+        Guarded g;
+        for (float& x : g.guard)
+            x = 12345.f;
+        g.s.reset(float(rng() % 3) * 0.5f);
+        const int n_put = 5 + int(rng() % 80);
+        for (int k = 0; k < n_put; ++k) {
+            float c = std::uniform_real_distribution<float>(0.f, 10.f)(rng);
+            float w = 0.02f + std::uniform_real_distribution<float>(0.f, 2.f)(rng);
+            if (rng() % 2) {
+                c = float(int(c * 4)) / 4;
+                w = float(1 + rng() % 8) / 4;
+            }
+            const float dt = (rng() % 3 == 0) ? float(1 + rng() % 4) / 32 : w / 31.f;
+            g.s.put({ c - w, c + w, dt });
+            bool hit = g.s.n > 16;
+            for (float x : g.guard)
+                hit = hit || x != 12345.f;
+            if (hit) {
+                ++bad;
+                break;
+            }
+        }
+    }
+    return bad;
+}

@@ -334,3 +334,13 @@ def test_range_specialised_exp_is_bit_identical(shim):
     f.restype = C.c_long
     f.argtypes = [C.c_float, C.c_float, C.c_uint]
     assert f(-100.0, 2.0, 97) == 0
+
+
+def test_insertions_never_overflow_the_set(shim):
+    """A section set holds at most 16 sections whatever is inserted: no
+    insertion leaves more, or writes past the set (the marcher keeps one set
+    per warp in shared memory, next to the other warps' data)."""
+    f = shim.kat_section_overflows
+    f.restype = C.c_long
+    f.argtypes = [C.c_uint, C.c_int]
+    assert f(3, 40000) == 0
