@@ -489,10 +489,15 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     return launch_status();
 }
 
-inline bool cache_ok(const dgmr_vm_cache* c, bool need_list)
+// The per-pixel and per-tile arrays are always needed; the per-Gaussian ones
+// only when there are Gaussians (an empty tensor may have no address).
+inline bool cache_ok(const dgmr_vm_cache* c, bool need_list, int32_t n_gaussians)
 {
-    return c && c->framebuffer && c->rects && c->rgb && c->rgb_sh_clamped && c->depths && c->points_xy_image && c->inverse_filtered_cov3d
-        && c->filtered_masses && c->tiles_touched && c->point_offsets && c->i_ranges && c->remaining_transparency && (!need_list || c->b_point_list);
+    if (!c || !c->framebuffer || !c->i_ranges || !c->remaining_transparency || (need_list && !c->b_point_list))
+        return false;
+    return n_gaussians == 0
+        || (c->rects && c->rgb && c->rgb_sh_clamped && c->depths && c->points_xy_image && c->inverse_filtered_cov3d && c->filtered_masses
+            && c->tiles_touched && c->point_offsets);
 }
 
 } // namespace dgmr
@@ -518,7 +523,7 @@ dgmr_status dgmr_vm_forward_preprocess(const dgmr_scene* scene, const dgmr_camer
     dgmr_status st = check_scene(scene, camera, -1);
     if (st != DGMR_OK)
         return st;
-    if (!cache_ok(cache, false) || !workspace)
+    if (!cache_ok(cache, false, scene->n_gaussians) || !workspace)
         return DGMR_ERR_BAD_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (scene->dtype == DGMR_F64)
@@ -532,7 +537,7 @@ dgmr_status dgmr_vm_forward_render_options(const dgmr_scene* scene, const dgmr_c
     dgmr_status st = check_scene(scene, camera, -1);
     if (st != DGMR_OK)
         return st;
-    if (!cache_ok(cache, pair_capacity > 0) || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+    if (!cache_ok(cache, pair_capacity > 0, scene->n_gaussians) || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
         return DGMR_ERR_BAD_ARG;
     if (options && options->render_mode != DGMR_RENDER_FULL && options->render_mode != DGMR_RENDER_BINS && options->render_mode != DGMR_RENDER_DEPTH)
         return DGMR_ERR_BAD_ARG;
@@ -555,7 +560,8 @@ dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera,
     dgmr_status st = check_scene(scene, camera, -1);
     if (st != DGMR_OK)
         return st;
-    if (!cache_ok(cache, false) || !workspace || !grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations)
+    const bool grads_ok = scene->n_gaussians == 0 || (grad_sh && grad_weights && grad_centroids && grad_scales && grad_rotations);
+    if (!cache_ok(cache, false, scene->n_gaussians) || !workspace || !grad_framebuffer || !grads_ok)
         return DGMR_ERR_BAD_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (scene->dtype == DGMR_F64)
