@@ -804,8 +804,10 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     dgmr_status st = check_scene(scene, camera, DGMR_F32);
     if (st != DGMR_OK)
         return st;
-    if (!grad_framebuffer || !grad_sh || !grad_weights || !grad_centroids || !grad_scales || !grad_rotations || !frame_workspace || pair_capacity < 0
-        || pair_capacity > int64_t(0x7fffffff) || (pair_capacity > 0 && !pair_workspace))
+    // per-Gaussian outputs may have no address when there are no Gaussians
+    const bool grads_ok = scene->n_gaussians == 0 || (grad_sh && grad_weights && grad_centroids && grad_scales && grad_rotations);
+    if (!grad_framebuffer || !grads_ok || !frame_workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff)
+        || (pair_capacity > 0 && !pair_workspace))
         return DGMR_ERR_BAD_ARG;
     const uint32_t N = uint32_t(scene->n_gaussians);
     const SplatLayout L = splat_layout(N, uint32_t(camera->width), uint32_t(camera->height), uint32_t(pair_capacity), frame_workspace, pair_workspace);

@@ -40,6 +40,12 @@ def test_empty_scene_draws_the_background(cuda):
     want = np.broadcast_to(np.array(BG, np.float32)[:, None, None], (3, cam.height, cam.width))
     np.testing.assert_array_equal(fb.cpu().numpy(), want)
     assert int(frame.stats[0].item()) == 0
+    grads = splat.splat_backward(frame, torch.ones(3, cam.height, cam.width, device=cuda), shs, w.reshape(-1), mu, s, q)
+    torch.cuda.synchronize()
+    assert [tuple(g.shape) for g in grads] == [(0, 1, 3), (0,), (0, 3), (0, 3), (0, 4)]
+    from differentiable_gaussian_mixture_renderer_b200 import vol_raster
+    fr = vol_raster.forward(shs, w, mu, s, q, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx, cam.tan_fovy, 0)
+    np.testing.assert_array_equal(fr.cpu().numpy(), want)
     cache = cpp_binding.forward(shs, w, mu, s, q, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx,
                                 cam.tan_fovy, 0)
     torch.cuda.synchronize()
