@@ -174,59 +174,33 @@ __device__ __forceinline__ float splat_q(float4 r0, float b2, float px, float py
     return __fmaf_rn(__fmaf_rn(r0.z, dx, b2 * dy), dx, (r0.w * dy) * dy);
 }
 
-__device__ __forceinline__ float splat_gauss(float4 co, float2 xy, float px, float py, float* dx_o, float* dy_o)
-{
-    const float4 r0 = make_float4(xy.x, xy.y, co.x, co.z);
-    return dgmr_fm::exp_f(-0.5f * splat_q(r0, 2.f * co.y, px, py, dx_o, dy_o));
-}
-
-// Per-pixel blend step shared by both pixels a thread owns
-// (splat_forward.cu:299-321).
+// Per-pixel blend state of the pixel a thread owns (splat_forward.cu:299-321).
 struct PixelState {
     float T, c0, c1, c2;
     int32_t last;
     bool done;
 };
 
-// blend_step after the cutoff test, given exp(-q/2) (splat_forward.cu:303-321)
-__device__ __forceinline__ void blend_alpha(PixelState& ps, float ex, float opacity, float r, float g, float b, int32_t idx)
+// One blend step after the cutoff test, given exp(-q/2)
+// (splat_forward.cu:303-321): alpha = min(0.99, opacity * exp), skipped below
+// 1/255; the pixel saturates (and keeps its state) once T * (1 - alpha) would
+// drop below 1e-4.  Written as selects so that a warp can run it for every
+// lane, whether or not the lane uses the record (`use`): the arithmetic and
+// its order are the reference's, applied only where `use` holds.
+__device__ __forceinline__ void blend_alpha_select(PixelState& ps, bool use, float ex, float opacity, float r, float g, float b, int32_t idx)
 {
-    if (ps.done)
-        return;
     const float alpha = min_f(0.99f, opacity * ex);
-    if (alpha < 1.0f / 255.0f)
-        return;
     const float test_T = ps.T * (1.f - alpha);
-    if (test_T < 0.0001f) {
-        ps.done = true;
-        return;
-    }
+    const bool live = use && !ps.done && !(alpha < 1.0f / 255.0f);
+    const bool stop = live && test_T < 0.0001f;
+    const bool take = live && !stop;
     const float w = alpha * ps.T;
-    ps.c0 = __fmaf_rn(r, w, ps.c0);
-    ps.c1 = __fmaf_rn(g, w, ps.c1);
-    ps.c2 = __fmaf_rn(b, w, ps.c2);
-    ps.T = test_T;
-    ps.last = idx;
-}
-
-__device__ __forceinline__ void blend_step(PixelState& ps, float q, float qcut, float opacity, float r, float g, float b, int32_t idx)
-{
-    if (ps.done || q > qcut)
-        return;
-    const float alpha = min_f(0.99f, opacity * dgmr_fm::exp_f(-0.5f * q));
-    if (alpha < 1.0f / 255.0f)
-        return;
-    const float test_T = ps.T * (1.f - alpha);
-    if (test_T < 0.0001f) {
-        ps.done = true;
-        return;
-    }
-    const float w = alpha * ps.T;
-    ps.c0 = __fmaf_rn(r, w, ps.c0);
-    ps.c1 = __fmaf_rn(g, w, ps.c1);
-    ps.c2 = __fmaf_rn(b, w, ps.c2);
-    ps.T = test_T;
-    ps.last = idx;
+    ps.c0 = take ? __fmaf_rn(r, w, ps.c0) : ps.c0;
+    ps.c1 = take ? __fmaf_rn(g, w, ps.c1) : ps.c1;
+    ps.c2 = take ? __fmaf_rn(b, w, ps.c2) : ps.c2;
+    ps.T = take ? test_T : ps.T;
+    ps.last = take ? idx : ps.last;
+    ps.done = ps.done || stop;
 }
 
 // Minimum of d'Qd over the tile's pixel rectangle [x0,x1] x [y0,y1] for a
@@ -299,6 +273,8 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
     constexpr int kThreads = 256;
     constexpr int kBatch = kThreads;
     constexpr int kWarps = kThreads / 32;
+    constexpr int kGroup = 4;
+    static_assert(kBatch % kGroup == 0, "a group never reads past the batch");
     __shared__ float4 s_r0[kBatch];
     __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
     __shared__ float s_rgb[3][kBatch];
@@ -365,34 +341,38 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
             s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
         }
         __syncthreads();
-        if (!p0.done) {
-            // two records per iteration: their quadratic forms and exps are
-            // independent and overlap; the blend steps still run in list order
-            int j = 0;
-            for (; j + 1 < n; j += 2) {
-                const float4 a0 = s_r0[j], a1 = s_r1[j];
-                const float4 b0 = s_r0[j + 1], b1 = s_r1[j + 1];
-                float dx, dy;
-                const float qa = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
-                const float qb = splat_q(b0, b1.x, fpx, fpy, &dx, &dy);
-                const bool ua = !(qa > a1.z), ub = !(qb > b1.z);
-                if (!(ua || ub))
+        if (!__all_sync(0xffffffffu, p0.done)) {
+            // kGroup records at a time, in three steps whose control flow is
+            // uniform over the warp: the quadratic forms (independent, so their
+            // shared-memory loads and multiply-adds overlap), the exps of the
+            // records inside some lane's cutoff (again independent), then the
+            // blend steps in list order as selects.  A group no lane needs is
+            // skipped whole; the warp leaves once all its pixels are saturated.
+            for (int j = 0; j < n; j += kGroup) {
+                float q[kGroup];
+                bool u[kGroup];
+                bool any = false;
+#pragma unroll
+                for (int i = 0; i < kGroup; ++i) {
+                    const float4 a0 = s_r0[j + i], a1 = s_r1[j + i]; // j + i < kBatch (kBatch % kGroup == 0)
+                    float dx, dy;
+                    q[i] = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
+                    u[i] = j + i < n && !(q[i] > a1.z) && !p0.done;
+                    any = any || u[i];
+                }
+                if (!__any_sync(0xffffffffu, any))
                     continue;
-                const float ea = ua ? dgmr_fm::exp_f_nonpos(-0.5f * qa) : 0.f;
-                const float eb = ub ? dgmr_fm::exp_f_nonpos(-0.5f * qb) : 0.f;
-                if (ua)
-                    blend_alpha(p0, ea, a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
-                if (ub)
-                    blend_alpha(p0, eb, b1.y, s_rgb[0][j + 1], s_rgb[1][j + 1], s_rgb[2][j + 1], __float_as_int(b1.w));
-                if (p0.done)
+                float ex[kGroup];
+#pragma unroll
+                for (int i = 0; i < kGroup; ++i)
+                    ex[i] = u[i] ? dgmr_fm::exp_f_nonpos(-0.5f * q[i]) : 0.f;
+#pragma unroll
+                for (int i = 0; i < kGroup; ++i) {
+                    const float4 a1 = s_r1[j + i];
+                    blend_alpha_select(p0, u[i], ex[i], a1.y, s_rgb[0][j + i], s_rgb[1][j + i], s_rgb[2][j + i], __float_as_int(a1.w));
+                }
+                if (__all_sync(0xffffffffu, p0.done))
                     break;
-            }
-            if (j < n && !p0.done) {
-                const float4 a0 = s_r0[j], a1 = s_r1[j];
-                float dx, dy;
-                const float q0 = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
-                if (!(q0 > a1.z))
-                    blend_alpha(p0, dgmr_fm::exp_f_nonpos(-0.5f * q0), a1.y, s_rgb[0][j], s_rgb[1][j], s_rgb[2][j], __float_as_int(a1.w));
             }
         }
         __syncthreads();
