@@ -80,7 +80,8 @@ struct BinningBuffers {
     uint32_t* cnt_sorted; // [N] super-tiles touched, in depth order
     uint32_t* off_sorted; // [N] their inclusive scan
     uint32_t* scan_tmp; // scan_temp_bytes(max(N, n_tiles))
-    uint32_t* n_sort; // [8] min(P, cap), super entries to sort, chunk count, spare, depth-key min / max
+    uint32_t* n_sort; // [8] min(P, cap), super entries to sort, chunk count, spare, depth-key min / max,
+                      // blocks done in the blend's tile-order kernel, spare
     int32_t* super_ranges; // [n_tiles, 2] each super-tile's entries in the sorted list
     uint32_t* chunk_base; // [n_tiles + 1] first chunk of each super-tile
     uint32_t* tile_total; // [n_tiles] pairs per tile
@@ -162,6 +163,7 @@ static __global__ void k_pair_count(const uint32_t* __restrict__ point_offsets, 
 {
     n_sort[4] = 0xffffffffu; // depth-key range, filled by k_key_range
     n_sort[5] = 0u;
+    n_sort[6] = 0u; // counter of the blend's tile-order kernel (k_blend_tile_order)
     const uint32_t P = N ? point_offsets[N - 1] : 0u;
     stats[0] = P;
     if (P > cap)
@@ -759,7 +761,7 @@ inline int run_binning_grids(uint32_t N, uint32_t n_tiles, uint32_t n_super, con
     const int par = tile_sort_parity(n_super);
     if (N == 0) {
         cudaMemsetAsync(ranges, 0, size_t(n_tiles) * 2 * sizeof(int32_t), s);
-        cudaMemsetAsync(b.n_sort, 0, 4 * sizeof(uint32_t), s);
+        cudaMemsetAsync(b.n_sort, 0, 8 * sizeof(uint32_t), s);
         return par;
     }
     if (!offsets_ready)
