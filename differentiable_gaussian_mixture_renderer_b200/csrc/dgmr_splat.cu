@@ -344,12 +344,13 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
         }
         __syncthreads();
         if (!__all_sync(0xffffffffu, p0.done)) {
-            // kGroup records at a time, in three steps whose control flow is
-            // uniform over the warp: the quadratic forms (independent, so their
-            // shared-memory loads and multiply-adds overlap), the exps of the
-            // records inside some lane's cutoff (again independent), then the
-            // blend steps in list order as selects.  A group no lane needs is
-            // skipped whole; the warp leaves once all its pixels are saturated.
+            // kGroup records at a time, with control flow that is uniform over
+            // the warp: the group's quadratic forms (independent, so their
+            // shared-memory loads and multiply-adds overlap), then, in list
+            // order, the exp and the blend step (as selects) of each record
+            // that some lane's cutoff admits; a record no lane needs costs a
+            // vote, a group no lane needs is skipped whole, and the warp leaves
+            // once all its pixels are saturated.
             for (int j = 0; j < n; j += kGroup) {
                 float q[kGroup];
                 bool u[kGroup];
@@ -364,14 +365,13 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
                 }
                 if (!__any_sync(0xffffffffu, any))
                     continue;
-                float ex[kGroup];
-#pragma unroll
-                for (int i = 0; i < kGroup; ++i)
-                    ex[i] = u[i] ? dgmr_fm::exp_f_nonpos(-0.5f * q[i]) : 0.f;
 #pragma unroll
                 for (int i = 0; i < kGroup; ++i) {
+                    if (!__any_sync(0xffffffffu, u[i]))
+                        continue;
+                    const float ex = u[i] ? dgmr_fm::exp_f_nonpos(-0.5f * q[i]) : 0.f;
                     const float4 a1 = s_r1[j + i];
-                    blend_alpha_select(p0, u[i], ex[i], a1.y, s_rgb[0][j + i], s_rgb[1][j + i], s_rgb[2][j + i], __float_as_int(a1.w));
+                    blend_alpha_select(p0, u[i], ex, a1.y, s_rgb[0][j + i], s_rgb[1][j + i], s_rgb[2][j + i], __float_as_int(a1.w));
                 }
                 if (__all_sync(0xffffffffu, p0.done))
                     break;
