@@ -417,17 +417,21 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], int l
 
 // Reverse-order blend adjoint: each pixel walks its contributors back to
 // front, recovering T_i = T_{i+1} / (1 - alpha_i); per-splat gradients are
-// summed over the warp with shuffles before one atomic per value.
+// summed over the warp with shuffles before one atomic per value.  Tiles run
+// in the forward's launch order (heaviest predicted walk first): a tile's
+// backward walks the same list up to its last contributor.
 template <class Frames>
 __global__ void __launch_bounds__(256) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
-    const float4* __restrict__ rec, const float* __restrict__ rgb, float* __restrict__ acc, const __grid_constant__ Frames frames)
+    const float4* __restrict__ rec, const float* __restrict__ rgb, float* __restrict__ acc, const uint32_t* __restrict__ tile_order,
+    const __grid_constant__ Frames frames)
 {
     __shared__ float4 s_r0[256]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
     __shared__ float4 s_r1[256];
     __shared__ float s_rgb[3][256];
     __shared__ uint32_t s_id[256];
     __shared__ int s_max;
-    const unsigned tile = blockIdx.x;
+    const unsigned ordered = tile_order ? tile_order[blockIdx.x] : blockIdx.x;
+    const unsigned tile = ordered < gridDim.x ? ordered : blockIdx.x; // the order is a permutation of the tiles
     const FrameRef f = frames.frame(tile);
     if (!f.grad_fb) // a view without an image gradient (batched renders that only asked for the image)
         return;
@@ -957,7 +961,7 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
-    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc,
+    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order,
         single_frame(cam, nullptr, L, grad_framebuffer));
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
@@ -1331,7 +1335,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
         return DGMR_OK;
     const int par = tile_sort_parity(plan.tab.n_stiles);
     cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
-    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, plan.tab);
+    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order, plan.tab);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
         nullptr, Formulation::Ots };
     k_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);
