@@ -308,13 +308,13 @@ __global__ void __launch_bounds__(kVrThreads) k_vr_render(VrRender a, CameraT<fl
                 const float weight = g.weight * sh.mass[j];
                 if (variance <= 0.f || dgmr_fm::isnan_f(variance) || dgmr_fm::isnan_f(weight) || weight > 100000.f)
                     continue;
-                if (weight * (cdf_inv_SD(centre, inv_sd, max_distance) - cdf_inv_SD(centre, inv_sd, 0.f)) <= 0.001f)
+                if (weight * (cdf_inv_SD_inline(centre, inv_sd, max_distance) - cdf_inv_SD_inline(centre, inv_sd, 0.f)) <= 0.001f)
                     continue;
                 const uint32_t id = sh.id[j];
                 const V3<float> rgb = { a.rgb[3 * size_t(id)], a.rgb[3 * size_t(id) + 1], a.rgb[3 * size_t(id) + 2] };
-                float cdf_start = cdf_inv_SD(centre, inv_sd, 0.f);
+                float cdf_start = cdf_inv_SD_inline(centre, inv_sd, 0.f);
                 for (unsigned q = 0; q < kVrBins; ++q) {
-                    const float cdf_end = cdf_inv_SD(centre, inv_sd, sizer.end_of(q));
+                    const float cdf_end = cdf_inv_SD_inline(centre, inv_sd, sizer.end_of(q));
                     const float mass = (cdf_end - cdf_start) * weight;
                     cdf_start = cdf_end;
                     if (mass < 0.0001f)
