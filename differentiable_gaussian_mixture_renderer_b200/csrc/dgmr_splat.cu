@@ -342,6 +342,12 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
             s_rgb[1][slot] = rgb[3 * size_t(id) + 1];
             s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
         }
+        // the slots after the last record up to the group boundary: a cutoff below
+        // every quadratic form (q = 0 here), so no lane ever uses them
+        if (int(threadIdx.x) < kGroup - 1 && n + int(threadIdx.x) < kBatch) {
+            s_r0[n + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s_r1[n + threadIdx.x] = make_float4(0.f, 0.f, -1.f, 0.f);
+        }
         __syncthreads();
         if (!__all_sync(0xffffffffu, p0.done)) {
             // kGroup records at a time, with control flow that is uniform over
@@ -349,22 +355,17 @@ __global__ void __launch_bounds__(256) k_splat_blend(const int32_t* __restrict__
             // shared-memory loads and multiply-adds overlap), then, in list
             // order, the exp and the blend step (as selects) of each record
             // that some lane's cutoff admits; a record no lane needs costs a
-            // vote, a group no lane needs is skipped whole, and the warp leaves
-            // once all its pixels are saturated.
+            // vote, and the warp leaves once all its pixels are saturated.
             for (int j = 0; j < n; j += kGroup) {
                 float q[kGroup];
                 bool u[kGroup];
-                bool any = false;
 #pragma unroll
                 for (int i = 0; i < kGroup; ++i) {
                     const float4 a0 = s_r0[j + i], a1 = s_r1[j + i]; // j + i < kBatch (kBatch % kGroup == 0)
                     float dx, dy;
                     q[i] = splat_q(a0, a1.x, fpx, fpy, &dx, &dy);
-                    u[i] = j + i < n && !(q[i] > a1.z) && !p0.done;
-                    any = any || u[i];
+                    u[i] = !(q[i] > a1.z) && !p0.done;
                 }
-                if (!__any_sync(0xffffffffu, any))
-                    continue;
 #pragma unroll
                 for (int i = 0; i < kGroup; ++i) {
                     if (!__any_sync(0xffffffffu, u[i]))
