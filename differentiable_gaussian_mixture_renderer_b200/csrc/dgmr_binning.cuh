@@ -719,10 +719,12 @@ static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, 
     }
 }
 
-// Launch order for the per-tile kernels: tiles bucketed by floor(log2(list
-// length + 1)), longest first, so the heaviest tiles start at the head of the
-// grid instead of stretching its tail.  One block; order inside a bucket is
-// arbitrary (it only affects scheduling, never results).
+// Launch order for the marcher's per-tile kernels: tiles bucketed by
+// floor(log2(list length + 1)), longest first, so the heaviest tiles start at
+// the head of the grid instead of stretching its tail.  One block; order
+// inside a bucket is arbitrary (it only affects scheduling, never results).
+// The splat blend orders its tiles by a predicted cost instead
+// (k_blend_tile_order): there the longest lists saturate early.
 static __global__ void __launch_bounds__(1024) k_tile_order(const int32_t* __restrict__ ranges, uint32_t n_tiles, uint32_t* __restrict__ order)
 {
     __shared__ uint32_t count[33];
