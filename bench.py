@@ -257,11 +257,22 @@ def run_ours(args):
         server.estimate_capacity("scene", cam)
 
     # ---------------------------------------------------------------- value leg
+    def release_done(upto: list):
+        # each result is read (kept in HBM / pinned memory) and handed back, so the
+        # server cycles through a fixed set of leased buffers
+        while upto[0] < len(server.completed):
+            server.completed[upto[0]].release()
+            upto[0] += 1
+
     def served_leg(cam_list, to_host: bool):
+        done = [0]
         for i in range(args.warmup * args.batch):
             server.submit(Request("scene", cam_list[i], to_host=to_host))
+            release_done(done)
         server.drain()
+        release_done(done)
         server.completed.clear()
+        done = [0]
         barrier()
         launches0 = lib.dgmr_launch_count()
         start = torch.cuda.Event(enable_timing=True)
@@ -271,7 +282,9 @@ def run_ours(args):
         t_wall = time.perf_counter()
         for i in range(args.steps * args.batch):
             server.submit(Request("scene", cam_list[args.warmup * args.batch + i], to_host=to_host))
+            release_done(done)
         server.drain()
+        release_done(done)
         s0 = server.slots[0].stream
         for sl in server.slots[1:]:
             s0.wait_stream(sl.stream)

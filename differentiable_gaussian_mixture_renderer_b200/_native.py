@@ -13,6 +13,7 @@ import torch
 from . import build as _build
 
 DGMR_OK, DGMR_ERR_BAD_ARG, DGMR_ERR_WORKSPACE, DGMR_ERR_CUDA, DGMR_ERR_STATIC_SCRATCH = 0, 1, 2, 3, 4
+DGMR_ERR_PAIR_OVERFLOW = 5
 DGMR_F32, DGMR_F64 = 0, 1
 FLAG_PAIR_OVERFLOW, FLAG_STEP_LIMIT = 1, 2
 

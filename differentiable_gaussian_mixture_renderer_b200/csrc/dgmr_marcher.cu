@@ -595,6 +595,8 @@ const char* dgmr_status_string(dgmr_status status)
         return "CUDA launch error";
     case DGMR_ERR_STATIC_SCRATCH:
         return "frame exceeds the 64 MiB static scratch of the no-allocation entry point";
+    case DGMR_ERR_PAIR_OVERFLOW:
+        return "pair capacity too small for the frame (rendered incompletely)";
     }
     return "unknown status";
 }

@@ -1427,5 +1427,14 @@ extern "C" dgmr_status dgmr_splat_forward_noalloc(const dgmr_scene* scene, const
     uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
     launch_preprocess(scene, cam, L, st_dev, s);
     launch_render(scene, cam, framebuffer, L, cap, st_dev, s);
-    return launch_status();
+    st = launch_status();
+    if (st != DGMR_OK || stats)
+        return st;
+    // No caller-visible statistics: the overflow flag sits in the static
+    // array, so wait for the frame and report it as the call's status.
+    uint32_t flags = 0;
+    if (cudaMemcpyAsync(&flags, L.stats + 1, sizeof(flags), cudaMemcpyDeviceToHost, s) != cudaSuccess
+        || cudaStreamSynchronize(s) != cudaSuccess)
+        return DGMR_ERR_CUDA;
+    return (flags & DGMR_FLAG_PAIR_OVERFLOW) ? DGMR_ERR_PAIR_OVERFLOW : DGMR_OK;
 }

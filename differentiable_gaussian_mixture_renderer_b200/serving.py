@@ -2,14 +2,19 @@
 CUDA streams, no host synchronisation per request.
 
 A request is (scene, camera).  Each of ``n_slots`` slots owns a stream, a
-frame workspace, a pair workspace, a device framebuffer and a pinned host
-image; a new request takes the least recently used slot once its previous
-request has finished, so up to ``n_slots`` frames overlap on the GPU
-(preprocess and sort of one with the blend of another, device-to-host copies
-with compute).  The pair capacity of each (scene, resolution) is learnt from
-the frames rendered so far; a frame that overflowed its capacity is rendered
-again with the exact count before its result is handed out, so every result
-equals the plain per-call render.
+frame workspace and a pair workspace; a new request takes the least recently
+used slot once its previous request has finished, so up to ``n_slots`` frames
+overlap on the GPU (preprocess and sort of one with the blend of another,
+device-to-host copies with compute).  The pair capacity of each (scene,
+resolution) is learnt from the frames rendered so far; a frame that
+overflowed its capacity is rendered again with the exact count before its
+result is handed out, so every result equals the plain per-call render.
+
+Every request owns its result: its framebuffer (and pinned host image) are
+leased from a pool of the server's and stay the request's until the caller
+hands them back with ``Request.release()``; a result the caller keeps is never
+written by a later request.  A caller that releases each result once it has
+read it lets the server run on a fixed set of buffers.
 """
 from __future__ import annotations
 
@@ -66,8 +71,6 @@ class _Slot:
     frame_ws: torch.Tensor | None = None
     pair_ws: torch.Tensor | None = None
     cap: int = 0
-    fb: torch.Tensor | None = None
-    host: torch.Tensor | None = None
     stats: torch.Tensor | None = None
     stats_host: torch.Tensor | None = None
     done: torch.cuda.Event | None = None
@@ -87,6 +90,16 @@ class Request:
     rerendered: bool = False
     slot: int = -1
     meta: dict = field(default_factory=dict)
+    _release: object = None  # set by the server that leased the result buffers
+
+    def release(self) -> None:
+        """Hands the result buffers back to the server that rendered them; the
+        request's ``image`` is gone afterwards.  Without this call the request
+        simply keeps them."""
+        if self._release is not None:
+            self._release(self)
+            self._release = None
+        self.image = None
 
 
 class RenderServer:
@@ -102,6 +115,24 @@ class RenderServer:
         self.completed: list[Request] = []
         self.ref_event = None
         self.t0 = 0.0
+        self._pool: dict = {}  # (pinned, H, W) -> result buffers no request holds
+
+    # ------------------------------------------------------------ result buffers
+    def _lease(self, pinned: bool, H: int, W: int) -> torch.Tensor:
+        free = self._pool.get((pinned, H, W))
+        if free:
+            return free.pop()
+        if pinned:
+            return torch.empty((3, H, W), dtype=torch.float32, pin_memory=True)
+        return torch.empty((3, H, W), dtype=torch.float32, device=self.device)
+
+    def _give_back(self, buf: torch.Tensor | None, pinned: bool) -> None:
+        if buf is not None:
+            self._pool.setdefault((pinned, int(buf.shape[1]), int(buf.shape[2])), []).append(buf)
+
+    def _release_request(self, req: Request) -> None:
+        self._give_back(req.meta.pop("_fb", None), False)
+        self._give_back(req.meta.pop("_host", None), True)
 
     # ------------------------------------------------------------ buffers
     def _ensure(self, slot: _Slot, scene: GaussianScene, W: int, H: int, cap: int, to_host: bool):
@@ -113,11 +144,6 @@ class RenderServer:
         pbytes = max(1, lib.dgmr_splat_pair_workspace_size(scene.n, cap))
         if slot.pair_ws is None or slot.pair_ws.numel() < pbytes:
             slot.pair_ws = torch.empty(pbytes, dtype=torch.uint8, device=dev)
-        if slot.fb is None or tuple(slot.fb.shape) != (3, H, W):
-            slot.fb = torch.empty((3, H, W), dtype=torch.float32, device=dev)
-            slot.host = None
-        if to_host and slot.host is None:
-            slot.host = torch.empty((3, H, W), dtype=torch.float32, pin_memory=True)
         if slot.stats is None:
             slot.stats = torch.zeros(4, dtype=torch.int32, device=dev)
             slot.stats_host = torch.zeros(4, dtype=torch.int32, pin_memory=True)
@@ -150,13 +176,20 @@ class RenderServer:
         cam = req.camera
         self._ensure(slot, scene, cam.width, cam.height, cap, req.to_host)
         s = slot.stream
-        N.check(self.lib.dgmr_splat_forward(scene.c_scene(), camera_struct(cam, req.background), N.ptr(slot.fb),
+        # the request's own result buffers (kept on a re-render)
+        if "_fb" not in req.meta:
+            req.meta["_fb"] = self._lease(False, cam.height, cam.width)
+            if req.to_host:
+                req.meta["_host"] = self._lease(True, cam.height, cam.width)
+            req._release = self._release_request
+        fb = req.meta["_fb"]
+        N.check(self.lib.dgmr_splat_forward(scene.c_scene(), camera_struct(cam, req.background), N.ptr(fb),
                                             N.ptr(slot.frame_ws), slot.frame_ws.numel(), N.ptr(slot.pair_ws),
                                             slot.pair_ws.numel(), cap, N.ptr(slot.stats), s.cuda_stream),
                 "splat forward")
         slot.stats_host.copy_(slot.stats, non_blocking=True)
         if req.to_host:
-            slot.host.copy_(slot.fb, non_blocking=True)
+            req.meta["_host"].copy_(fb, non_blocking=True)
 
     def submit(self, req: Request) -> Request:
         idx = self.next_slot
@@ -195,7 +228,12 @@ class RenderServer:
             req.t_done = self.t0 + self.ref_event.elapsed_time(slot.done) * 1e-3
         else:
             req.t_done = time.perf_counter()
-        req.image = slot.host if req.to_host else slot.fb
+        if req.to_host:
+            # the copy to the host has finished: the device framebuffer is free again
+            self._give_back(req.meta.pop("_fb"), False)
+            req.image = req.meta["_host"]
+        else:
+            req.image = req.meta["_fb"]
         req.meta["n_pairs"] = n_pairs
         self.completed.append(req)
         slot.request = None

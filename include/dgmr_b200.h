@@ -30,6 +30,7 @@ typedef enum dgmr_status {
     DGMR_ERR_WORKSPACE = 2, /* workspace smaller than the query returned */
     DGMR_ERR_CUDA = 3, /* a launch failed; cudaGetLastError() holds the cause */
     DGMR_ERR_STATIC_SCRATCH = 4, /* frame too large for dgmr_splat_forward_noalloc's 64 MiB scratch */
+    DGMR_ERR_PAIR_OVERFLOW = 5, /* dgmr_splat_forward_noalloc without stats: the frame had more pairs than pair_capacity */
 } dgmr_status;
 
 /* Device-side frame statistics (caller-owned, 16 bytes, written by the calls
@@ -155,7 +156,12 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
  * the array's device address (make that first call before any stream
  * capture).  All calls on a device share the array: calls that overlap on the
  * GPU race and corrupt each other; calls ordered on one stream are fine.
- * Results equal dgmr_splat_forward's; the workspace views are not available. */
+ * Results equal dgmr_splat_forward's; the workspace views are not available.
+ * With a device `stats` the call is asynchronous and the caller reads
+ * DGMR_FLAG_PAIR_OVERFLOW there.  With stats == NULL the frame's statistics
+ * stay in the static array, which the caller cannot read, so the call waits
+ * for the stream and returns DGMR_ERR_PAIR_OVERFLOW when pair_capacity was too
+ * small (the image is then incomplete) instead of dropping pairs silently. */
 dgmr_status dgmr_splat_forward_noalloc(const dgmr_scene* scene, const dgmr_camera* camera, float* framebuffer, int64_t pair_capacity,
     dgmr_frame_stats* stats, dgmr_stream stream);
 

@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -29,7 +30,7 @@
 #endif
 
 #include "dgmr_oracle_marching.h"
-#include "../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_volume_fit.h"
+#include "dgmr_oracle_volume_fit.h"
 
 using namespace orc;
 
@@ -261,7 +262,12 @@ inline T splat_alpha(const T* co, const T* xy, T px, T py, T* g_out = nullptr, T
     const T dx = px - xy[0];
     const T dy = py - xy[1];
     const T q = std::fma(std::fma(co[0], dx, (T(2) * co[1]) * dy), dx, (co[2] * dy) * dy);
-    const T g = dgmr_fm::exp_f(T(-0.5f) * q);
+    const T g = ofm::exp_f(T(-0.5f) * q);
+    if (std::is_same<T, float>::value && audit().on.load(std::memory_order_relaxed)) {
+        const T gl = std::exp(T(-0.5f) * q);
+        const T al = min_f(T(0.99f), co[3] * g);
+        audit_note(AUDIT_ALPHA, !(al < T(1.0f / 255.0f)), !(min_f(T(0.99f), co[3] * gl) < T(1.0f / 255.0f)), double(al), double(T(1.0f / 255.0f)));
+    }
     if (g_out) {
         *g_out = g;
         *dx_out = dx;
@@ -390,13 +396,24 @@ void vm_preprocess(const SceneIn<T>& s, VmCache<T>& c)
             continue;
         const Gaussian2d<T> g = splat(form_or(Formulation::Opacity), w, mu, sc, q, cam, T(FILTER_SD * FILTER_SD));
         const auto iso = [](T wt, T var, T isoline) {
-            const T sv = T(-2) * dgmr_fm::log_f(isoline / wt);
+            const T sv = T(-2) * ofm::log_f(isoline / wt);
             if (sv <= T(0))
                 return T(0);
             return dgmr_fm::sqrt_f(sv * var);
         };
         const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[0], T(1.f / 255.f))));
         const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[2], T(1.f / 255.f))));
+        if (std::is_same<T, float>::value && audit().on.load(std::memory_order_relaxed)) {
+            const auto iso_l = [](T wt, T var, T isoline) {
+                const T sv = T(-2) * std::log(isoline / wt);
+                return sv <= T(0) ? T(0) : dgmr_fm::sqrt_f(sv * var);
+            };
+            const int exl = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso_l(g.weight, g.cov.v[0], T(1.f / 255.f))));
+            const int eyl = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso_l(g.weight, g.cov.v[2], T(1.f / 255.f))));
+            const T rx = iso(g.weight, g.cov.v[0], T(1.f / 255.f)), ry = iso(g.weight, g.cov.v[2], T(1.f / 255.f));
+            audit_note(AUDIT_RECT, true, ex == exl, double(rx), std::round(double(rx)));
+            audit_note(AUDIT_RECT, true, ey == eyl, double(ry), std::round(double(ry)));
+        }
         c.rects[2 * i] = ex;
         c.rects[2 * i + 1] = ey;
         const URect r = get_rect(float(g.centroid.x), float(g.centroid.y), ex, ey, gx, gy);
@@ -494,6 +511,11 @@ void collect_sections(DensityArray<N_LARGE, T>& sections, const Ray<T>& ray, con
         if (sections.end() < depths[id])
             break;
         const T mor = g.weight * masses[id];
+        if (std::is_same<T, float>::value && audit().on.load(std::memory_order_relaxed)) {
+            const T mor_l = intersect_weight_libm(mu, Q, ray) * masses[id];
+            audit_note(AUDIT_SECTION_MASS, !(mor <= T(1.0f / 255.f) || mor > T(1000)), !(mor_l <= T(1.0f / 255.f) || mor_l > T(1000)), double(mor),
+                double(T(1.0f / 255.f)));
+        }
         if (mor <= T(1.0f / 255.f) || mor > T(1000))
             continue;
         if (g.C <= T(0))
@@ -571,7 +593,7 @@ void vm_march(const SceneIn<T>& s, const int32_t* list, VmCache<T>& c, int32_t* 
                         Tr = T(0);
                     } else if (g_render_mode.mode == 2) { // vol_marcher_forward.cu:466-481
                         for (unsigned k = 0; k < N_SMALL - 1; ++k)
-                            Tr = Tr * dgmr_fm::exp_f(-bins[k].m);
+                            Tr = Tr * ofm::exp_f(-bins[k].m);
                         distance = max_f(sections.end(), distance);
                         const T dd = distance / T(g_render_mode.max_depth);
                         colour = { dd, dd, dd };
@@ -1298,7 +1320,7 @@ void vr_preprocess(const SceneIn<float>& s, VrCache& c)
 inline float eval_exponential_1d(float c, float var, float x)
 {
     const float dx = x - c;
-    return dgmr_fm::exp_f((-0.5f * (dx * dx)) / var);
+    return ofm::exp_f((-0.5f * (dx * dx)) / var);
 }
 
 // Ray through the pixel corner at NDC z = -1 (vol_raster_forward.cu:263-268)
@@ -1337,8 +1359,8 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                 if (px >= W || py >= H)
                     continue;
                 const Ray<float> ray = vr_pixel_ray(inv_proj, campos, px, py, W, H);
-                dgmr::RasterBinSizer<VR_BINS> sizer;
-                sizer.init(VR_RELEVANCE_SIGMA, VR_TRANSMISSION);
+                oracle_vf::DepthBins<VR_BINS> sizer;
+                sizer.reset(VR_RELEVANCE_SIGMA, VR_TRANSMISSION);
                 for (int32_t k = b; k < e; ++k) { // pass A: bin sizes
                     const uint32_t id = list[k];
                     S3<float> Q;
@@ -1350,11 +1372,11 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                         continue;
                     if (g.C + 0.f <= 0.f)
                         continue;
-                    sizer.add_gaussian(mor, g.centre, dgmr_fm::sqrt_f(g.C + 0.f));
-                    if (sizer.is_full())
+                    sizer.add(mor, g.centre, dgmr_fm::sqrt_f(g.C + 0.f));
+                    if (sizer.saturated())
                         break;
                 }
-                sizer.finalise();
+                sizer.close();
                 float bin_mass[VR_BINS][4] = {};
                 float bin_eval[VR_BINS + 1][4] = {};
                 for (int32_t k = b; k < e; ++k) { // pass B: masses and border values per bin
@@ -1370,12 +1392,12 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                     const float weight = g.weight * c.masses[id];
                     if (variance <= 0.f || dgmr_fm::isnan_f(variance) || dgmr_fm::isnan_f(weight) || weight > 100000.f)
                         continue;
-                    if (weight * integrate_normalised_inv_SD(centre, inv_sd, 0.f, sizer.end_of(VR_BINS - 1)) <= 0.001f)
+                    if (weight * integrate_normalised_inv_SD(centre, inv_sd, 0.f, sizer.upper(VR_BINS - 1)) <= 0.001f)
                         continue;
                     const V3<float> rgb = load3(c.rgb, id);
                     float cdf_start = cdf_inv_SD(centre, inv_sd, 0.f);
                     for (unsigned q = 0; q < VR_BINS; ++q) {
-                        const float cdf_end = cdf_inv_SD(centre, inv_sd, sizer.end_of(q));
+                        const float cdf_end = cdf_inv_SD(centre, inv_sd, sizer.upper(q));
                         const float mass = (cdf_end - cdf_start) * weight;
                         cdf_start = cdf_end;
                         if (mass < 0.0001f)
@@ -1384,13 +1406,13 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                         bin_mass[q][1] = bin_mass[q][1] + rgb.y * mass;
                         bin_mass[q][2] = bin_mass[q][2] + rgb.z * mass;
                         bin_mass[q][3] = bin_mass[q][3] + mass;
-                        const float ev = weight * eval_exponential_1d(centre, variance, sizer.begin_of(q));
+                        const float ev = weight * eval_exponential_1d(centre, variance, sizer.lower(q));
                         bin_eval[q][0] = bin_eval[q][0] + rgb.x * ev;
                         bin_eval[q][1] = bin_eval[q][1] + rgb.y * ev;
                         bin_eval[q][2] = bin_eval[q][2] + rgb.z * ev;
                         bin_eval[q][3] = bin_eval[q][3] + ev;
                     }
-                    const float ev = weight * eval_exponential_1d(centre, variance, sizer.end_of(VR_BINS - 1));
+                    const float ev = weight * eval_exponential_1d(centre, variance, sizer.upper(VR_BINS - 1));
                     bin_eval[VR_BINS][0] = bin_eval[VR_BINS][0] + rgb.x * ev;
                     bin_eval[VR_BINS][1] = bin_eval[VR_BINS][1] + rgb.y * ev;
                     bin_eval[VR_BINS][2] = bin_eval[VR_BINS][2] + rgb.z * ev;
@@ -1400,22 +1422,14 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                 // evaluates to 0.5 for every bin and channel (vol_raster_forward.cu:473).
                 float res[3] = { 0.f, 0.f, 0.f };
                 float transparency = 1.f;
-                const float half[4] = { 0.5f, 0.5f, 0.5f, 0.5f };
                 for (unsigned q = 0; q < VR_BINS; ++q) {
-                    const float t_right = sizer.end_of(q) - sizer.begin_of(q);
+                    const float t_right = sizer.upper(q) - sizer.lower(q);
                     if (t_right <= 0.f)
                         continue;
-                    const dgmr::FunctionGroup<float> f = dgmr::create_approximation(half, bin_mass[q], bin_eval[q], bin_eval[q + 1], t_right);
-                    const float dt = f.t_right / float(VR_STEPS_PER_BIN);
-                    float t = dt / 2.f;
-                    for (unsigned i = 0; i < VR_STEPS_PER_BIN; ++i) {
-                        const float e0 = f.sample(0, t), e1 = f.sample(1, t), e2 = f.sample(2, t), e3 = f.sample(3, t);
-                        res[0] = res[0] + (e0 * transparency) * dt;
-                        res[1] = res[1] + (e1 * transparency) * dt;
-                        res[2] = res[2] + (e2 * transparency) * dt;
-                        transparency = transparency * dgmr_fm::max_f(0.f, 1.f - e3 * dt);
-                        t = t + dt;
-                    }
+                    oracle_vf::BinChannel ch[4];
+                    for (int k = 0; k < 4; ++k)
+                        ch[k] = oracle_vf::fit_channel(0.5f, bin_mass[q][k], bin_eval[q][k], bin_eval[q + 1][k], t_right);
+                    oracle_vf::integrate_bin(ch, t_right, VR_STEPS_PER_BIN, res, transparency);
                 }
                 // final colour C + T * background with T = 1 in this mode (vol_raster_forward.cu:509-513)
                 const size_t pix = size_t(py) * W + px;
@@ -1746,7 +1760,35 @@ int orc_density_randomised_f64(int iters, int puts, int probes) { return da_rand
 void orc_fmath_f32(int which, const float* x, float* y, int n)
 {
     for (int i = 0; i < n; ++i)
-        y[i] = which == 0 ? dgmr_fm::exp_f(x[i]) : (which == 1 ? dgmr_fm::log_f(x[i]) : dgmr_fm::erf_f(x[i]));
+        switch (which) { // 0-2: the shared fixed-sequence routines; 3-5: the host libm
+        case 0: y[i] = dgmr_fm::exp_f(x[i]); break;
+        case 1: y[i] = dgmr_fm::log_f(x[i]); break;
+        case 2: y[i] = dgmr_fm::erf_f(x[i]); break;
+        case 3: y[i] = std::exp(x[i]); break;
+        case 4: y[i] = std::log(x[i]); break;
+        default: y[i] = std::erf(x[i]); break;
+        }
+}
+
+// Decision audit: on = 1 resets the counters and starts counting, 0 stops;
+// out9 = (seen, flipped, near threshold) of alpha, section-mass and rect decisions.
+void orc_audit(int on, long* out9)
+{
+    DecisionAudit& a = audit();
+    if (on) {
+        for (int k = 0; k < AUDIT_KINDS; ++k) {
+            a.seen[k] = 0;
+            a.flipped[k] = 0;
+            a.near[k] = 0;
+        }
+    }
+    a.on = on;
+    if (out9)
+        for (int k = 0; k < AUDIT_KINDS; ++k) {
+            out9[3 * k] = a.seen[k].load();
+            out9[3 * k + 1] = a.flipped[k].load();
+            out9[3 * k + 2] = a.near[k].load();
+        }
 }
 
 } // extern "C"

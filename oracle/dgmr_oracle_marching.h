@@ -204,7 +204,7 @@ template <class T, unsigned NB>
 inline void integrate_bins(V3<T>& colour, T& transparency, const Bin4<T>* bins)
 {
     for (unsigned k = 0; k < NB; ++k) {
-        const T tk = dgmr_fm::exp_f(-bins[k].m);
+        const T tk = ofm::exp_f(-bins[k].m);
         colour.x = colour.x + bins[k].r * transparency;
         colour.y = colour.y + bins[k].g * transparency;
         colour.z = colour.z + bins[k].b * transparency;
@@ -225,7 +225,7 @@ inline void grad_integrate_bins(V3<T>& colour, T& transparency, T final_transpar
         g_bins[k].r = g_bins[k].r + transparency * g_colour.x;
         g_bins[k].g = g_bins[k].g + transparency * g_colour.y;
         g_bins[k].b = g_bins[k].b + transparency * g_colour.z;
-        const T tk = dgmr_fm::exp_f(-bins[k].m);
+        const T tk = ofm::exp_f(-bins[k].m);
         const T inv_tk = min_f(T(255), T(1) / tk);
         colour.x = (colour.x - bins[k].r) * inv_tk;
         colour.y = (colour.y - bins[k].g) * inv_tk;
@@ -243,7 +243,7 @@ template <class T>
 inline void grad_cdf_inv_SD(T c, T inv_sd, T x, T g, T* g_c, T* g_inv_sd)
 {
     const T u = (x - c) * inv_sd;
-    const T pdf = T(0.39894228040143267794) * dgmr_fm::exp_f(T(-0.5) * (u * u));
+    const T pdf = T(0.39894228040143267794) * ofm::exp_f(T(-0.5) * (u * u));
     *g_c = *g_c - g * inv_sd * pdf;
     *g_inv_sd = *g_inv_sd + g * (x - c) * pdf;
 }
@@ -265,7 +265,7 @@ inline void grad_intersect_with_ray_inv_C(V3<T> mu, const S3<T>& Q, const Ray<T>
     const T detQ = det_sym3(Q);
     const T r = detQ / a;
     const T sr = dgmr_fm::sqrt_f(r);
-    const T weight = (sr * T(0.15915494309189533577)) * dgmr_fm::exp_f(T(-0.5) * e);
+    const T weight = (sr * T(0.15915494309189533577)) * ofm::exp_f(T(-0.5) * e);
 
     const T g_e = g_weight * (T(-0.5) * weight);
     const T g_r = (r > T(0)) ? g_weight * weight / (T(2) * r) : T(0);

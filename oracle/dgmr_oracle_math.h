@@ -17,13 +17,67 @@
 // FMA contraction; transcendental functions come from dgmr_fmath.h).
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 
 #include "../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_fmath.h"
 
+// The oracle's exp / log / erf.  By default the fixed-sequence routines of
+// dgmr_fmath.h, which the CUDA kernels use too, so that every threshold
+// decision (alpha >= 1/255, section mass >= 1/255, the ceil of a
+// log-derived radius) comes out the same on both sides.  Built with
+// -DDGMR_ORACLE_LIBM, the host C library's expf / logf / erff instead: the
+// nearest stand-in here for the CUDA expf / erff the reference calls, used
+// only to measure how far that choice moves images and decisions.
+namespace ofm {
+#if defined(DGMR_ORACLE_LIBM)
+inline float exp_f(float x) { return std::exp(x); }
+inline float log_f(float x) { return std::log(x); }
+inline float erf_f(float x) { return std::erf(x); }
+inline double exp_f(double x) { return std::exp(x); }
+inline double log_f(double x) { return std::log(x); }
+inline double erf_f(double x) { return std::erf(x); }
+#else
+using dgmr_fm::erf_f;
+using dgmr_fm::exp_f;
+using dgmr_fm::log_f;
+#endif
+using dgmr_fm::sqrt_f;
+} // namespace ofm
+
 namespace orc {
+
+// Decision audit.  With audit().on set, the threshold decisions that depend
+// on a transcendental -- a splat's alpha >= 1/255 (exp), a ray section's mass
+// >= 1/255 (exp), a marcher rectangle's ceil of the 1/255 isoline radius
+// (log) -- are also taken with the host libm's function on the same argument,
+// and disagreements are counted; so are the decisions whose compared value
+// lies within a relative 16 * 2^-23 of the threshold (16 float ulps), the
+// only ones an implementation of exp / log within 16 ulps of ours could take
+// the other way.  Float only; off by default.
+enum AuditKind { AUDIT_ALPHA = 0, AUDIT_SECTION_MASS = 1, AUDIT_RECT = 2, AUDIT_KINDS = 3 };
+struct DecisionAudit {
+    std::atomic<int> on { 0 };
+    std::atomic<long> seen[AUDIT_KINDS] = {};
+    std::atomic<long> flipped[AUDIT_KINDS] = {};
+    std::atomic<long> near[AUDIT_KINDS] = {};
+};
+inline DecisionAudit& audit()
+{
+    static DecisionAudit a;
+    return a;
+}
+inline void audit_note(AuditKind k, bool shared, bool libm, double value, double threshold)
+{
+    DecisionAudit& a = audit();
+    a.seen[k].fetch_add(1, std::memory_order_relaxed);
+    if (shared != libm)
+        a.flipped[k].fetch_add(1, std::memory_order_relaxed);
+    if (std::fabs(value - threshold) <= std::fabs(value) * (16.0 / 8388608.0))
+        a.near[k].fetch_add(1, std::memory_order_relaxed);
+}
 
 using dgmr_fm::clamp_f;
 using dgmr_fm::max_f;
@@ -593,8 +647,24 @@ inline Gauss1d<T> intersect_with_ray_inv_C(V3<T> mu, const S3<T>& Q, const Ray<T
     g.C = T(1) / a;
     g.centre = b / a;
     const T e = k - b * g.centre;
-    g.weight = (dgmr_fm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * dgmr_fm::exp_f(T(-0.5) * e);
+    g.weight = (dgmr_fm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * ofm::exp_f(T(-0.5) * e);
     return g;
+}
+
+// intersect_with_ray_inv_C's weight with the host libm's exp (decision audit only)
+template <class T>
+inline T intersect_weight_libm(V3<T> mu, const S3<T>& Q, const Ray<T>& ray)
+{
+    const V3<T> c = sub(mu, ray.o);
+    const V3<T> d = ray.d;
+    const V3<T> Qd = { (Q.v[0] * d.x + Q.v[1] * d.y) + Q.v[2] * d.z, (Q.v[1] * d.x + Q.v[3] * d.y) + Q.v[4] * d.z, (Q.v[2] * d.x + Q.v[4] * d.y) + Q.v[5] * d.z };
+    const V3<T> Qc = { (Q.v[0] * c.x + Q.v[1] * c.y) + Q.v[2] * c.z, (Q.v[1] * c.x + Q.v[3] * c.y) + Q.v[4] * c.z, (Q.v[2] * c.x + Q.v[4] * c.y) + Q.v[5] * c.z };
+    const T a = dot(d, Qd);
+    const T b = dot(c, Qd);
+    const T k = dot(c, Qc);
+    const T centre = b / a;
+    const T e = k - b * centre;
+    return (dgmr_fm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * std::exp(T(-0.5) * e);
 }
 
 // cdf of N(c, 1/inv_sd^2) at x
@@ -602,7 +672,7 @@ template <class T>
 inline T cdf_inv_SD(T c, T inv_sd, T x)
 {
     const T z = ((x - c) * inv_sd) * T(0.70710678118654752440);
-    return T(0.5) * (T(1) + dgmr_fm::erf_f(z));
+    return T(0.5) * (T(1) + ofm::erf_f(z));
 }
 template <class T>
 inline T integrate_normalised_inv_SD(T c, T inv_sd, T a, T b) { return cdf_inv_SD(c, inv_sd, b) - cdf_inv_SD(c, inv_sd, a); }

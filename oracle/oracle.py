@@ -6,6 +6,7 @@ arrays in the reference's layouts and returns numpy arrays.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -14,7 +15,10 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libdgmr_oracle.so")
-_lib = None
+# the same restatement with the host libm's expf / logf / erff (see libm_transcendentals)
+_LIBM_PATH = os.path.join(_HERE, "_build", "libdgmr_oracle_libm.so")
+_libs: dict = {}
+_variant = _LIB_PATH
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -30,13 +34,29 @@ def build() -> str:
 
 
 def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+    if _variant not in _libs:
+        if not os.path.exists(_variant):
             build()
-        _lib = C.CDLL(_LIB_PATH)
-        _declare(_lib)
-    return _lib
+        L = C.CDLL(_variant)
+        _declare(L)
+        _libs[_variant] = L
+    return _libs[_variant]
+
+
+@contextlib.contextmanager
+def libm_transcendentals():
+    """Inside this block every oracle call runs the build whose exp / log /
+    erf are the host C library's (correctly rounded or nearly so) instead of
+    the fixed-sequence routines the CUDA kernels share with the default
+    build: the closest stand-in available here for the CUDA expf / erff the
+    reference calls.  Used to measure what sharing those routines hides."""
+    global _variant
+    old = _variant
+    _variant = _LIBM_PATH
+    try:
+        yield
+    finally:
+        _variant = old
 
 
 def _scene_types(fp):
@@ -46,6 +66,8 @@ def _scene_types(fp):
 
 
 def _declare(L):
+    L.orc_audit.argtypes = [C.c_int, C.POINTER(C.c_long)]
+    L.orc_audit.restype = None
     L.orc_num_threads.restype = C.c_int
     L.orc_set_num_threads.argtypes = [C.c_int]
     L.orc_higher_msb.restype = C.c_uint32
@@ -300,11 +322,34 @@ def density_sample(capacity, start, puts, n_samples, dtype=np.float32):
     return out
 
 
-def fmath(which: str, x):
+def fmath(which: str, x, libm: bool = False):
+    """The shared fixed-sequence exp / log / erf (float) on x, or with
+    ``libm`` the host C library's."""
     x = _c(x, np.float32)
     y = np.zeros_like(x)
-    lib().orc_fmath_f32({"exp": 0, "log": 1, "erf": 2}[which], x, y, x.size)
+    lib().orc_fmath_f32({"exp": 0, "log": 1, "erf": 2}[which] + (3 if libm else 0), x, y, x.size)
     return y
+
+
+@contextlib.contextmanager
+def decision_audit():
+    """Counts, inside the block, the float threshold decisions that depend on
+    exp or log (splat alpha >= 1/255, ray-section mass >= 1/255, marcher
+    rectangle radius) and how many of them the host libm's function would
+    have taken the other way, and how many lie within 16 float ulps of the
+    threshold (the only ones any exp / log within 16 ulps of the shared
+    routines could flip).  Yields a dict filled on exit:
+    {kind: (seen, flipped, near)}."""
+    L = lib()
+    out = np.zeros(9, np.int64)
+    L.orc_audit(1, out.ctypes.data_as(C.POINTER(C.c_long)))
+    res: dict = {}
+    try:
+        yield res
+    finally:
+        L.orc_audit(0, out.ctypes.data_as(C.POINTER(C.c_long)))
+        for k, name in enumerate(("alpha", "section_mass", "rect")):
+            res[name] = (int(out[3 * k]), int(out[3 * k + 1]), int(out[3 * k + 2]))
 
 
 def set_const_samples(sections) -> None:

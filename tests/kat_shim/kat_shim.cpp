@@ -2,7 +2,10 @@
 // (differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_sections.h and
 // dgmr_volume_fit.h) through a C ABI so the reference's known-answer tests
 // can run them on the CPU, the way the reference's own unit tests run its
-// __host__ __device__ math on the host.
+// __host__ __device__ math on the host.  The oracle's separate restatement
+// of the bin sizer and bin fit (oracle/dgmr_oracle_volume_fit.h) is exposed
+// beside them, so the same tests pin both and a randomised comparison checks
+// that the two codings agree bit for bit.
 #include <cstdlib>
 #include <cstring>
 #include <random>
@@ -10,6 +13,7 @@
 
 #include "../../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_sections.h"
 #include "../../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_volume_fit.h"
+#include "../../oracle/dgmr_oracle_volume_fit.h"
 
 namespace {
 
@@ -201,7 +205,124 @@ void kat_rbs4(float sigma, float transmission_threshold, const float* adds, int 
     }
 }
 
+// the oracle's restatement, same packing and calls as above (float inside)
+void kat_pl_create_oracle(const double* mpl, const double* mt, const double* el, const double* er, double t_right, double* packed_out)
+{
+    for (int i = 0; i < 4; ++i) {
+        const oracle_vf::BinChannel c = oracle_vf::fit_channel(float(mpl[i]), float(mt[i]), float(el[i]), float(er[i]), float(t_right));
+        packed_out[i] = c.d0;
+        packed_out[4 + i] = c.k0;
+        packed_out[8 + i] = c.t1;
+        packed_out[12 + i] = c.t2;
+        packed_out[16 + i] = c.k2;
+    }
+    packed_out[20] = t_right;
+}
+
+void kat_pl_volume_integrate_oracle(const double* packed, int n, int steps, double* out3)
+{
+    float rgb[3] = { 0.f, 0.f, 0.f };
+    float tr = 1.f;
+    for (int g = 0; g < n; ++g) {
+        const double* p = packed + 21 * g;
+        oracle_vf::BinChannel ch[4];
+        for (int i = 0; i < 4; ++i)
+            ch[i] = oracle_vf::BinChannel { float(p[i]), float(p[4 + i]), float(p[8 + i]), float(p[12 + i]), float(p[16 + i]) };
+        oracle_vf::integrate_bin(ch, float(p[20]), unsigned(steps), rgb, tr);
+    }
+    for (int i = 0; i < 3; ++i)
+        out3[i] = rgb[i];
+}
+
+void kat_rbs4_oracle(float sigma, float transmission_threshold, const float* adds, int n, int* full_after_add, int* full_after_finalise, float* begin4,
+    float* end4)
+{
+    oracle_vf::DepthBins<4> s;
+    s.reset(sigma, transmission_threshold);
+    for (int i = 0; i < n; ++i) {
+        s.add(adds[3 * i], adds[3 * i + 1], adds[3 * i + 2]);
+        full_after_add[i] = s.saturated() ? 1 : 0;
+    }
+    s.close();
+    *full_after_finalise = s.saturated() ? 1 : 0;
+    for (unsigned i = 0; i < 4; ++i) {
+        begin4[i] = s.lower(i);
+        end4[i] = s.upper(i);
+    }
+}
+
 } // extern "C"
+
+namespace {
+
+bool same_bits(float a, float b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+// Random add sequences (masses, centres and sds spread as along real rays,
+// with repeated centres for ties) through the product's RasterBinSizer<NB>
+// and the oracle's DepthBins<NB>; counts sequences whose saturation flags or
+// final borders differ in any bit.
+template <unsigned NB>
+long compare_sizers(unsigned seed, int trials)
+{
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    long bad = 0;
+    for (int t = 0; t < trials; ++t) {
+        dgmr::RasterBinSizer<NB> a;
+        oracle_vf::DepthBins<NB> b;
+        a.init(3.f, 0.005f);
+        b.reset(3.f, 0.005f);
+        const int n = 1 + int(u(rng) * 80.f);
+        bool ok = true;
+        float prev_centre = 2.f;
+        for (int i = 0; i < n && ok; ++i) {
+            const float mass = u(rng) < 0.1f ? 0.00005f : 0.0002f + 0.6f * u(rng) * u(rng);
+            const float centre = u(rng) < 0.1f ? prev_centre : 2.f + 3.f * u(rng);
+            prev_centre = centre;
+            const float sd = 0.005f + 0.1f * u(rng);
+            a.add_gaussian(mass, centre, sd);
+            b.add(mass, centre, sd);
+            ok = a.is_full() == b.saturated();
+        }
+        a.finalise();
+        b.close();
+        for (unsigned i = 0; i < NB && ok; ++i)
+            ok = same_bits(a.begin_of(i), b.lower(i)) && same_bits(a.end_of(i), b.upper(i));
+        bad += ok ? 0 : 1;
+    }
+    return bad;
+}
+
+} // namespace
+
+extern "C" long kat_compare_sizers(unsigned seed, int trials) { return compare_sizers<32>(seed, trials) + compare_sizers<4>(seed + 1, trials); }
+
+// Random bin fits (float) through the product's create_approximation and the
+// oracle's fit_channel: counts channels whose five parameters differ in any bit.
+extern "C" long kat_compare_fits(unsigned seed, int trials)
+{
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    long bad = 0;
+    for (int t = 0; t < trials; ++t) {
+        float mpl[4], mt[4], el[4], er[4];
+        for (int i = 0; i < 4; ++i) {
+            mpl[i] = u(rng) < 0.3f ? 0.5f : u(rng);
+            mt[i] = u(rng) < 0.1f ? 0.0000005f : 2.f * u(rng) * u(rng);
+            el[i] = 0.001f + 2.f * u(rng);
+            er[i] = 0.001f + 2.f * u(rng);
+        }
+        const float tr = 0.001f + 3.f * u(rng);
+        const dgmr::FunctionGroup<float> f = dgmr::create_approximation<float>(mpl, mt, el, er, tr);
+        for (int i = 0; i < 4; ++i) {
+            const oracle_vf::BinChannel c = oracle_vf::fit_channel(mpl[i], mt[i], el[i], er[i], tr);
+            const bool ok = same_bits(f.d0[i], c.d0) && same_bits(f.k0[i], c.k0) && same_bits(f.t1[i], c.t1) && same_bits(f.t2[i], c.t2)
+                && same_bits(f.k2[i], c.k2);
+            bad += ok ? 0 : 1;
+        }
+    }
+    return bad;
+}
 
 namespace {
 

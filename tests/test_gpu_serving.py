@@ -110,3 +110,33 @@ def test_overflowing_capacity_is_rerendered(cuda):
     torch.cuda.synchronize()
     assert server.rerenders > 0 and all(r.rerendered for r in reqs)
     _check(scenes, reqs)
+
+
+@pytest.mark.parametrize("to_host", [False, True])
+def test_render_server_results_are_not_reused(cuda, to_host):
+    """RenderServer: 8 results kept from 4 slots -- each still equals its frame
+    rendered alone after later requests reused the slots; released buffers are
+    handed to later requests instead of new ones."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import RenderServer, Request
+    scenes = _scenes(cuda)
+    server = RenderServer(scenes, cuda, n_slots=4)
+    reqs = []
+    for k in range(8):
+        w, h = RES[k % 2]
+        reqs.append(server.submit(Request("ab"[k % 2], S.random_cameras(1, w, h, seed=300 + k)[0], to_host=to_host)))
+    server.drain()
+    for k, req in enumerate(reqs):
+        fb, _ = _alone(scenes[req.scene_id], req)
+        img = req.image.to(cuda) if to_host else req.image
+        assert img.is_pinned() if to_host else img.is_cuda
+        assert torch.equal(img, fb), f"request {k}: image was overwritten by a later request"
+    held = {r.image.data_ptr() for r in reqs}
+    assert len(held) == 8
+    for r in reqs:
+        r.release()
+        assert r.image is None
+    again = server.submit(Request("a", S.random_cameras(1, *RES[0], seed=400)[0], to_host=to_host))
+    server.drain()
+    assert again.image.data_ptr() in held
+    fb, _ = _alone(scenes["a"], again)
+    assert torch.equal(again.image.to(cuda) if to_host else again.image, fb)

@@ -42,7 +42,23 @@ def shim():
     lib.kat_pl_create.argtypes = [f64p, f64p, f64p, f64p, C.c_double, f64p]
     lib.kat_pl_volume_integrate.argtypes = [f64p, C.c_int, C.c_int, f64p]
     lib.kat_rbs4.argtypes = [C.c_float, C.c_float, f32p, C.c_int, i32p, i32p, f32p, f32p]
+    lib.kat_pl_create_oracle.argtypes = lib.kat_pl_create.argtypes
+    lib.kat_pl_volume_integrate_oracle.argtypes = lib.kat_pl_volume_integrate.argtypes
+    lib.kat_rbs4_oracle.argtypes = lib.kat_rbs4.argtypes
+    lib.kat_compare_sizers.argtypes = [C.c_uint, C.c_int]
+    lib.kat_compare_sizers.restype = C.c_long
+    lib.kat_compare_fits.argtypes = [C.c_uint, C.c_int]
+    lib.kat_compare_fits.restype = C.c_long
     return lib
+
+
+# the bin fit and bin sizer exist twice: the product's device header (csrc/dgmr_volume_fit.h)
+# and the oracle's own restatement (oracle/dgmr_oracle_volume_fit.h); the KATs pin both
+VF_IMPLS = ["product", "oracle"]
+
+
+def vf(shim, name, impl):
+    return getattr(shim, name if impl == "product" else name + "_oracle")
 
 
 def value(lit: str, dtype):
@@ -184,10 +200,11 @@ def test_piecewise_linear_function_group(shim):
     dict(mpl=(0.5, 0.5, 0.5, 0.5), mt=(0.8, 0.8, 0.8, 0.0), el=(0.0, 0.0, 0.2, 0.0), er=(0.0, 0.1, 0.0, 0.0), tr=0.8, td=0.000001,
          rounding=0.5),
 ])
-def test_piecewise_linear_fit_conserves_mass(shim, case):
+@pytest.mark.parametrize("impl", VF_IMPLS)
+def test_piecewise_linear_fit_conserves_mass(shim, case, impl):
     f = np.zeros(21)
     a = lambda v: np.asarray(v, np.float64)
-    shim.kat_pl_create(a(case["mpl"]), a(case["mt"]), a(case["el"]), a(case["er"]), case["tr"], f)
+    vf(shim, "kat_pl_create", impl)(a(case["mpl"]), a(case["mt"]), a(case["el"]), a(case["er"]), case["tr"], f)
     assert shim.kat_pl_valid(f) == 1
     out = np.zeros(4)
     shim.kat_pl_sample(f, 0.0, out)
@@ -205,7 +222,8 @@ def test_piecewise_linear_fit_conserves_mass(shim, case):
                           (a(case["mt"]) * 1000 + case["rounding"]).astype(np.int32)), mass
 
 
-def test_piecewise_linear_volume_integral(shim):
+@pytest.mark.parametrize("impl", VF_IMPLS)
+def test_piecewise_linear_volume_integral(shim, impl):
     rows = [
         ((0.0, 0.0, 0.0, 0.0), (0.3, 0.6, 0.3, 0.6), (0.0, 0.0, 0.0, 0.0), (0.2, 0.1, 0.0, 0.1), 0.8),
         ((0.8, 0.4, 0.5, 0.3), (0.5, 0.4, 0.8, 0.2), (0.2, 0.1, 0.0, 0.1), (0.4, 0.7, 0.2, 0.9), 0.5),
@@ -220,11 +238,11 @@ def test_piecewise_linear_volume_integral(shim):
     groups = []
     for mpl, mt, el, er, tr in rows:
         f = np.zeros(21)
-        shim.kat_pl_create(a(mpl), a(mt), a(el), a(er), tr, f)
+        vf(shim, "kat_pl_create", impl)(a(mpl), a(mt), a(el), a(er), tr, f)
         groups.append(f)
     packed = np.ascontiguousarray(np.concatenate(groups))
     out = np.zeros(3)
-    shim.kat_pl_volume_integrate(packed, 8, 256, out)
+    vf(shim, "kat_pl_volume_integrate", impl)(packed, 8, 256, out)
     # numeric reference (Eq. 15 of the reference test): 1e6 steps over all bins
     n_ref = 1_000_000
     max_t = sum(r[4] for r in rows)
@@ -269,8 +287,9 @@ RBS_FULL = {
 }
 
 
+@pytest.mark.parametrize("impl", VF_IMPLS)
 @pytest.mark.parametrize("name", list(RBS_CASES))
-def test_raster_bin_sizer(shim, name):
+def test_raster_bin_sizer(shim, name, impl):
     adds = np.asarray(RBS_CASES[name], np.float32).reshape(-1)
     n = len(RBS_CASES[name])
     full = np.zeros(max(n, 1), np.int32)
@@ -278,7 +297,8 @@ def test_raster_bin_sizer(shim, name):
     b = np.zeros(4, np.float32)
     e = np.zeros(4, np.float32)
     # test configuration of unittests/raster_bin_sizer.cpp:29-33: 4 bins, threshold 0.1, relevance 1 sigma
-    shim.kat_rbs4(np.float32(1.0), np.float32(0.1), adds if n else np.zeros(3, np.float32), n, full, full_fin, b, e)
+    vf(shim, "kat_rbs4", impl)(np.float32(1.0), np.float32(0.1), adds if n else np.zeros(3, np.float32), n, full, full_fin,
+                               b, e)
     assert b[0] == pytest.approx(0.0)
     for i in range(3):
         assert e[i] == pytest.approx(b[i + 1])
@@ -291,6 +311,18 @@ def test_raster_bin_sizer(shim, name):
         assert [bool(x) for x in full[:n]] == exp_adds
         if exp_fin is not None:
             assert bool(full_fin[0]) == exp_fin
+
+
+def test_oracle_and_product_bin_sizers_agree(shim):
+    """20k random add sequences (32 and 4 bins): saturation after every add
+    and the final borders, bit for bit."""
+    assert shim.kat_compare_sizers(7, 10000) == 0
+
+
+def test_oracle_and_product_bin_fits_agree(shim):
+    """200k random four-channel bin fits: all five parameters of every
+    channel, bit for bit."""
+    assert shim.kat_compare_fits(11, 200000) == 0
 
 
 # ---------------------------------------------------------------- elementary functions

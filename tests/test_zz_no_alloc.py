@@ -67,3 +67,26 @@ def test_noalloc_rejects_frames_beyond_the_static_scratch(cuda):
                                         torch.cuda.current_stream().cuda_stream)
     assert st == N.DGMR_ERR_STATIC_SCRATCH
     assert b"static scratch" in lib.dgmr_status_string(st)
+
+
+def test_noalloc_reports_a_too_small_pair_capacity(cuda):
+    """With a device stats block the call stays asynchronous and flags the
+    overflow there; without one it waits for the frame and returns
+    DGMR_ERR_PAIR_OVERFLOW, so an incomplete image never passes as DGMR_OK."""
+    lib = N.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    tensors, scene, camera = _frame(10000, 256, 256, 0, cuda)
+    fb = torch.empty((3, 256, 256), dtype=torch.float32, device=cuda)
+    stats = torch.zeros(4, dtype=torch.int32, device=cuda)
+    assert lib.dgmr_splat_forward_noalloc(scene, camera, fb.data_ptr(), 100, stats.data_ptr(), stream) == N.DGMR_OK
+    torch.cuda.synchronize()
+    assert int(stats[1]) & 1 and int(stats[0]) > 100
+    st = lib.dgmr_splat_forward_noalloc(scene, camera, fb.data_ptr(), 100, None, stream)
+    assert st == N.DGMR_ERR_PAIR_OVERFLOW
+    assert b"pair capacity" in lib.dgmr_status_string(st)
+    # a sufficient capacity after the overflow: status OK and the full image
+    cap = int(stats[0])
+    ref, _ = _with_workspaces(lib, scene, camera, cap, cuda)
+    assert lib.dgmr_splat_forward_noalloc(scene, camera, fb.data_ptr(), cap, None, stream) == N.DGMR_OK
+    torch.cuda.synchronize()
+    assert float((fb - ref).abs().max()) <= IMAGE_TOL
