@@ -56,8 +56,10 @@ def parse():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--batch", type=int, default=8, help="requests per step")
     ap.add_argument("--slots", type=int, default=4, help="requests in flight")
-    ap.add_argument("--plain", type=int, default=16, help="plain per-call requests")
+    ap.add_argument("--plain", type=int, default=64, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the short vol_marcher (100k, 512x512) and serving (8 scenes) runs of the headline line")
     ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving", "configs"], default="served",
                     help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
                          "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512; "
@@ -139,16 +141,32 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name: str):
-    """dram bytes per launch of a kernel from a committed ncu summary, if any."""
+def profiled_value(name: str, key: str):
+    """A per-launch figure ("key: value" line) from a committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].split()[0])
-    except OSError:
+    except (OSError, ValueError):
         pass
     return None
+
+
+SMS = 148  # B200
+
+
+def issue_roof(warp_inst, ms, clocks):
+    """Warp instructions issued per second against the issue roof: one warp
+    instruction per cycle on each of the 4 schedulers of the 148 SMs, at the
+    median SM clock sampled during the run (the maximum if none was read)."""
+    if not warp_inst or not ms:
+        return None
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    achieved = warp_inst / (ms * 1e-3)
+    peak = SMS * 4 * mhz * 1e6
+    return {"achieved": achieved, "peak": peak, "unit": "warp inst/s", "frac": achieved / peak,
+            "warp_instructions_per_launch": warp_inst, "sm_mhz": mhz}
 
 
 def cpu_baseline(args, cams):
@@ -220,6 +238,7 @@ def run_ours(args):
     from differentiable_gaussian_mixture_renderer_b200 import _native as N
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
     from differentiable_gaussian_mixture_renderer_b200 import splat
+    from differentiable_gaussian_mixture_renderer_b200 import serving
     from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene, RenderServer, Request
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -304,22 +323,31 @@ def run_ours(args):
     ms_e2e, _, e2e_value = replica_totals(ms_e2e, local_renders, world, max_over_ranks, sum_over_ranks)
 
     # ---------------------------------------------------------------- plain per-call leg
+    # one request at a time on one stream, the reference's pattern: preprocess, the pair count
+    # read back, binning + blend, the image copied to pinned host memory and waited for; the
+    # workspaces grow once and are kept (no per-call allocation), as the C++ viewer interface does
     plain_cams = cams[2 * n_req:2 * n_req + args.plain]
+    ctx = splat.SplatContext(dev)
+    fb_plain = torch.empty((3, args.height, args.width), dtype=torch.float32, device=dev)
+    host_plain = torch.empty((3, args.height, args.width), dtype=torch.float32, pin_memory=True)
+
+    def plain_call(cam):
+        ctx.forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations,
+                    serving.camera_struct(cam), fb_plain, scene.sh_degree)
+        with torch.cuda.stream(ctx.stream):
+            host_plain.copy_(fb_plain, non_blocking=True)
+        ctx.stream.synchronize()
+
+    for cam in cams[:max(args.warmup, 3)]:  # grows the workspaces to their steady size
+        plain_call(cam)
     lat_plain = []
-    for cam in cams[:args.warmup]:  # warm the allocator and the path
-        fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations,
-                                    cam.view, cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height,
-                                    cam.tan_fovx, cam.tan_fovy, scene.sh_degree)
-        fb.cpu()
-    for i, cam in enumerate(plain_cams):
-        barrier()
+    barrier()
+    for cam in plain_cams:
         t = time.perf_counter()
-        fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations,
-                                    cam.view, cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height,
-                                    cam.tan_fovx, cam.tan_fovy, scene.sh_degree)
-        img = fb.cpu()
+        plain_call(cam)
         lat_plain.append((time.perf_counter() - t) * 1e3)
     plain_rps = len(lat_plain) / (sum(lat_plain) * 1e-3) * world if lat_plain else None
+    plain_rps_p50 = 1e3 / pct(lat_plain, 50) * world if lat_plain else None
 
     # ---------------------------------------------------------------- roofline of the blend
     cam = cams[0]
@@ -346,14 +374,28 @@ def run_ours(args):
     del flush
     tiles = ((args.width + 15) // 16) * ((args.height + 15) // 16)
     px = args.width * args.height
-    # per pair: list id 4 B + 32-byte splat record + rgb 12 B; per tile: range 8 B;
-    # per pixel: colour 12 B + transmittance 4 B + contributor count 4 B
-    blend_bytes = 48 * n_pairs + 8 * tiles + 20 * px
+    # algorithmic bytes of one blend launch: per pair its 32-byte record and 8-byte list entry,
+    # per tile its range (8 B), per pixel its colour (12 B)
+    blend_bytes = 40 * n_pairs + 8 * tiles + 12 * px
+    # the same with everything the kernel touches: 4 B list id + 32 B record + 12 B rgb per pair,
+    # and per pixel the final transmittance and contributor count the backward reads
+    blend_bytes_touched = 48 * n_pairs + 8 * tiles + 20 * px
     peak, peak_kind = peaks()
     achieved = blend_bytes / (blend_ms * 1e-3) / 1e9
     # the committed ncu capture is of this frame at the default workload only
     default_workload = (args.gaussians, args.width, args.height) == (1_000_000, 1920, 1080)
-    traffic = profiled_traffic("splat_blend_1080p_1M.txt") if default_workload else None
+    blend_profile = "splat_blend_1080p_1M.txt"
+    traffic = profiled_value(blend_profile, "dram_bytes_per_launch") if default_workload else None
+    warp_inst = profiled_value(blend_profile, "warp_instructions_per_launch") if default_workload else None
+
+    # ---------------------------------------------------------------- the other workloads, short runs
+    extras = {}
+    if world == 1 and not args.no_extras:
+        del fb, frame, ctx, fb_plain, host_plain
+        server.release_buffers()
+        extras["vol_marcher_c2"] = measure_marcher(dev, n_cams=3)
+        extras["batched_c3"] = measure_batched(dev, steps=3, warmup=2)
+        extras["serving_c4"] = measure_serving(dev, n_req=200, warmup=1)
 
     # ---------------------------------------------------------------- CPU baseline
     cpu = None
@@ -369,10 +411,15 @@ def run_ours(args):
             "config": dict(workload(args), parallelism=f"replicas x{world}"),
             "latency_ms": {"p50": pct(lat_value, 50), "p99": pct(lat_value, 99),
                            "note": f"submit-to-done per request with {args.slots} requests in flight"},
-            "plain_per_call": {"value": plain_rps, "unit": UNIT, "p50_ms": pct(lat_plain, 50),
-                               "p99_ms": pct(lat_plain, 99), "requests": len(lat_plain),
-                               "note": "one request at a time: preprocess, pair count read back, render, image to host"},
+            "plain_per_call": {"value": plain_rps, "unit": UNIT, "value_at_p50": plain_rps_p50,
+                               "p50_ms": pct(lat_plain, 50), "p99_ms": pct(lat_plain, 99), "requests": len(lat_plain),
+                               "note": "one request at a time on one stream: preprocess, pair count read back, "
+                                       "binning + blend, image copied to pinned host memory and waited for; "
+                                       "workspaces kept between calls"},
             "served_over_plain": (e2e_value / plain_rps) if plain_rps else None,
+            "served_over_plain_p50": (e2e_value / plain_rps_p50) if plain_rps_p50 else None,
+            "served_over_plain_note": "e2e (served, every image copied to host) over the plain per-call leg with "
+                                      "the same copy; _p50 uses the plain leg's median latency",
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": args.batch * 8 * (16 + 16 + 3 + 3 + 3 + 1),
                     "d2h_bytes_per_step": args.batch * 3 * args.width * args.height * 4,
@@ -380,14 +427,20 @@ def run_ours(args):
             "roofline": {"kernel": "k_splat_blend", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "ms_per_launch": blend_ms, "n_pairs": n_pairs, "algorithmic_bytes": blend_bytes,
+                         "bytes_formula": "40 P + 8 T + 12 px",
+                         "frac_all_touched_bytes": blend_bytes_touched / (blend_ms * 1e-3) / 1e9 / peak,
+                         "issue": issue_roof(warp_inst, blend_ms, clocks),
                          "l2": "flushed (256 MB write) before each timed launch",
-                         "note": "blend is FP32/issue-bound by construction; algorithmic bytes = 48 P + 8 T + 20 px; "
-                                 "traffic = ncu dram read+write of the same frame (profiles/splat_blend_1080p_1M.txt)"},
+                         "note": "the blend is bound by instruction issue, not HBM (see issue); frac_all_touched_bytes "
+                                 "counts 48 P + 8 T + 20 px; traffic and warp instructions from the ncu capture of "
+                                 "the same frame (profiles/splat_blend_1080p_1M.txt)"},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),
             "rerenders": int(rerenders),
         }
+        if extras:
+            line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -401,17 +454,16 @@ def _gpu_common():
     return torch, torch.device("cuda", local), local
 
 
-def run_batched(args):
+def measure_batched(dev, steps: int = 5, warmup: int = 3):
     """3 resident scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras each,
     resolutions cycling 256x256 / 800x600 / 1920x1080, forward + backward of
     all 48 views per step: autotuned batch depth under CUDA graphs, against the
     plain per-view calls (forward, pair count read back, backward)."""
-    torch, dev, local = _gpu_common()
-    from differentiable_gaussian_mixture_renderer_b200 import _native as N
+    import torch
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
     from differentiable_gaussian_mixture_renderer_b200 import splat
     from differentiable_gaussian_mixture_renderer_b200.batch import BatchRenderer, autotune, chunks
-    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene, camera_struct
     sizes = {"s50k": 50_000, "s300k": 300_000, "s1500k": 1_500_000}
     res = [(256, 256), (800, 600), (1920, 1080)]
     scenes = {k: GaussianScene.from_numpy(S.make_scene(n, seed=i), dev) for i, (k, n) in enumerate(sizes.items())}
@@ -438,117 +490,149 @@ def run_batched(args):
         for p in plans:
             s0.wait_stream(p.stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s0)
-        for _ in range(args.steps):
-            step()
-        e1.record(s0)
-        e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s0)
+    for _ in range(steps):
+        step()
+    e1.record(s0)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
     overflow = any(p.overflowed() for p in plans)
-    # plain per-view calls, the reference's pattern (one view per call, P read back)
+    # plain per-view calls, the reference's pattern (one view per call, P read back), workspaces kept
+    ctx = splat.SplatContext(dev)
     lat = []
-    for k, (sid, cam) in enumerate(views):
-        sc = scenes[sid]
-        torch.cuda.synchronize(dev)
-        e0.record(s0)
-        fb, frame = splat.splat_forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, cam.view, cam.proj,
-                                        cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
-                                        cam.tan_fovy, sc.sh_degree)
-        splat.splat_backward(frame, plans[0].grad_framebuffers[0].new_ones(fb.shape), sc.shs, sc.weights,
-                             sc.centroids, sc.scales, sc.rotations)
-        e1.record(s0)
-        e1.synchronize()
-        lat.append(e0.elapsed_time(e1))
-        del fb, frame
+    for rep in range(2):  # the first pass grows the context's workspaces
+        lat = []
+        for k, (sid, cam) in enumerate(views):
+            sc = scenes[sid]
+            fb = plans[0].grad_framebuffers[0].new_empty((3, cam.height, cam.width))
+            gfb = torch.ones_like(fb)
+            torch.cuda.synchronize(dev)
+            e0.record(s0)
+            ctx.forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, camera_struct(cam), fb, sc.sh_degree)
+            splat.splat_backward(ctx.frame(), gfb, sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations)
+            e1.record(s0)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
     plain_ms = sum(lat)
+    return {"workload": "3 scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras (r=2.5-4), resolutions cycling "
+                        "256x256 / 800x600 / 1920x1080, forward + backward",
+            "views": len(views), "megapixels_per_step": px / 1e6, "batch_depth": best, "ms_per_step": ms,
+            "views_per_s": len(views) / (ms * 1e-3), "mpix_per_s": px / 1e6 / (ms * 1e-3), "autotune_ms": timings,
+            "plain_per_view": {"views_per_s": len(views) / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                               "note": "one view per call: forward (pair count read back) + backward, workspaces kept"},
+            "batched_over_plain": plain_ms / ms, "pair_overflow": overflow, "graph_replays": steps * len(plans)}
+
+
+def run_batched(args):
+    """The batched workload (measure_batched) as its own JSON line."""
+    torch, dev, local = _gpu_common()
+    with ClockSampler(local) as clk:
+        r = measure_batched(dev, steps=args.steps, warmup=args.warmup)
     line = {"metric": "batched views/s, forward+backward, 3 scenes x 16 views, mixed resolutions",
-            "value": len(views) / (ms * 1e-3), "unit": "views/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "value": r["views_per_s"], "unit": "views/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "3 scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras (r=2.5-4), "
-                                   "resolutions cycling 256x256 / 800x600 / 1920x1080, forward + backward",
-                       "views": len(views), "megapixels_per_step": px / 1e6, "batch_depth": best,
+            "config": {"workload": r.pop("workload"), "views": r["views"], "batch_depth": r["batch_depth"],
                        "l2": "working set of one step (~30M view-Gaussian slots) far above the 126 MB L2"},
-            "mpix_per_s": px / 1e6 / (ms * 1e-3), "autotune_ms": timings,
-            "plain_per_view": {"value": len(views) / (plain_ms * 1e-3), "unit": "views/s", "ms_per_step": plain_ms},
-            "batched_over_plain": plain_ms / ms, "pair_overflow": overflow,
-            "clocks": clk.summary(), "graph_replays": args.steps * len(plans)}
+            **r, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
+
+
+MARCHER_PROFILE = "vol_marcher_c2_100k_512.txt"
+
+
+def measure_marcher(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int = 512, seed_cams: int = 1):
+    """vol_marcher forward + backward through the reference-facing binding
+    (cpp_binding.forward / backward) at 100k Gaussians, 512x512, float32, one
+    warm-up camera then ``n_cams`` timed ones; the forward also counts the
+    march's work unit (bin fills, each 128 CDF evaluations) on the device."""
+    import torch
+    from differentiable_gaussian_mixture_renderer_b200 import _native as N
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    sc = S.make_scene(n, seed=0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
+    ins = (t(sc.sh), t(sc.weights).reshape(-1, 1), t(sc.centroids), t(sc.scales), t(sc.rotations))
+    cams = S.random_cameras(n_cams + 1, W, H, seed=seed_cams)
+    G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
+    bg = torch.zeros(3, device=dev)
+    counter = torch.zeros(1, dtype=torch.int64, device=dev)
+    fwd, bwd, fills = [], [], []
+    l0 = N.lib().dgmr_launch_count()
+    for k, cam in enumerate(cams):
+        v, p, c = t(cam.view), t(cam.proj), t(cam.campos)
+        counter.zero_()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        cache = cpp_binding.forward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, work_counter=counter)
+        e1.record()
+        cpp_binding.backward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache)
+        e2.record()
+        e2.synchronize()
+        if k == 0:
+            l0 = N.lib().dgmr_launch_count()
+            continue
+        fwd.append(e0.elapsed_time(e1))
+        bwd.append(e1.elapsed_time(e2))
+        fills.append(int(counter.item()))
+    launches = N.lib().dgmr_launch_count() - l0
+    fills_per_s = sum(fills) / (sum(fwd) * 1e-3)
+    out = {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+           "backward_over_forward": statistics.median(bwd) / statistics.median(fwd),
+           "bin_fills_per_frame": statistics.median(fills), "cdf_evaluations_per_s": 128 * fills_per_s,
+           "gpu_launches": int(launches), "frames": len(fwd),
+           "workload": f"vol_marcher forward + backward, {n} Gaussians (config-0 distribution), {W}x{H}, random "
+                       "cameras r=2.5-4, through cpp_binding.forward/backward"}
+    # FP32 roof of the forward: 148 SMs x 128 FP32 lanes per cycle, over the FP32 thread
+    # instructions one bin fill takes (ncu count of the same frame / its fills)
+    per_fill = profiled_value(MARCHER_PROFILE, "fp32_thread_inst_per_fill")
+    if per_fill:
+        peak = SMS * 128 * 1965e6 / per_fill
+        out["roofline"] = {"kernel": "k_vm_march_warp", "bound": "fp32", "unit": "bin fills/s", "achieved": fills_per_s,
+                           "peak": peak, "frac": fills_per_s / peak, "fp32_thread_inst_per_fill": per_fill,
+                           "note": "forward call time (preprocess and binning included, < 2 % of it); peak at the "
+                                   "1965 MHz maximum clock; FP32 instructions per fill from "
+                                   f"profiles/{MARCHER_PROFILE}"}
+    return out
 
 
 def run_marcher(args):
     """vol_marcher forward + backward through the reference-facing binding
     (cpp_binding.forward / backward): 100k Gaussians, 512x512, fp32."""
     torch, dev, local = _gpu_common()
-    from differentiable_gaussian_mixture_renderer_b200 import _native as N
-    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
-    from differentiable_gaussian_mixture_renderer_b200 import scene as S
-    n, W, H = 100_000, 512, 512
-    sc = S.make_scene(n, seed=0)
-    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
-    ins = (t(sc.sh), t(sc.weights).reshape(-1, 1), t(sc.centroids), t(sc.scales), t(sc.rotations))
-    cams = S.random_cameras(args.warmup + args.steps, W, H, seed=1)
-    G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
-    bg = torch.zeros(3, device=dev)
-
-    def step(cam):
-        v, p, c = t(cam.view), t(cam.proj), t(cam.campos)
-        cache = cpp_binding.forward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0)
-        e_mid.record()
-        cpp_binding.backward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache)
-        return cache
-
-    e_mid = torch.cuda.Event(enable_timing=True)
-    for cam in cams[:args.warmup]:
-        step(cam)
-    torch.cuda.synchronize(dev)
-    fwd, bwd = [], []
     with ClockSampler(local) as clk:
-        l0 = N.lib().dgmr_launch_count()
-        for cam in cams[args.warmup:]:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            step(cam)
-            e1.record()
-            e1.synchronize()
-            fwd.append(e0.elapsed_time(e_mid))
-            bwd.append(e_mid.elapsed_time(e1))
-        launches = N.lib().dgmr_launch_count() - l0
-    ms = (sum(fwd) + sum(bwd)) / len(fwd)
+        r = measure_marcher(dev, n_cams=max(args.steps, 1))
+    ms = r["forward_ms"] + r["backward_ms"]
     line = {"metric": "vol_marcher forward+backward ms/frame, 100k Gaussians, 512x512", "value": ms, "unit": "ms",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "vol_marcher forward + backward, 100000 Gaussians (config-0 distribution), "
-                                   "512x512, random cameras r=2.5-4, through cpp_binding.forward/backward"},
-            "forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
-            "clocks": clk.summary(), "gpu_launches": int(launches)}
+            "config": {"workload": r.pop("workload")}, **r, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_serving(args):
+def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0):
     """8 resident scenes (100k-3M Gaussians, log-uniform), a Poisson request
-    stream at 200 req/s, resolutions drawn from 256^2 / 512^2 / 1280x720 /
+    stream at ``rate`` req/s, resolutions drawn from 256^2 / 512^2 / 1280x720 /
     1920x1080, 20 % of requests also asking for the gradient against an N(0,1)
-    image gradient.  The continuous-batching server against a serial server
-    that makes the plain per-request calls (preprocess, pair count read back,
-    render, backward) on the same arrival times."""
-    torch, dev, local = _gpu_common()
+    image gradient.  The continuous-batching server, saturated (all requests
+    queued at once) and on the Poisson arrivals, against a serial server that
+    makes the plain per-request calls (preprocess, pair count read back,
+    render, backward; workspaces kept) on the same arrival times."""
+    import torch
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
     from differentiable_gaussian_mixture_renderer_b200 import splat
-    from differentiable_gaussian_mixture_renderer_b200.serving import ContinuousServer, GaussianScene, ServeRequest
+    from differentiable_gaussian_mixture_renderer_b200.serving import (ContinuousServer, GaussianScene, ServeRequest,
+                                                                         camera_struct)
     rng = np.random.default_rng(7)
     counts = np.exp(rng.uniform(np.log(1e5), np.log(3e6), size=8)).astype(int)
     scenes = {f"s{i}": GaussianScene.from_numpy(S.make_scene(int(n), seed=20 + i), dev) for i, n in enumerate(counts)}
     res = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
-    n_req = max(args.steps, 1) * 40
-    rate = 200.0
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     gen = torch.Generator(device=dev).manual_seed(3)
 
@@ -578,7 +662,7 @@ def run_serving(args):
     rw = np.random.default_rng(5)
     for r in warm:
         r.camera = S.random_cameras(1, r.camera.width, r.camera.height, seed=int(rw.integers(1 << 30)))[0]
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         for r in warm:
             server.submit(r)
         server.drain()
@@ -608,67 +692,76 @@ def run_serving(args):
             return {}
         inflight = [x[3] * 1e3 for x in lg]
         gpu = [x[4] for x in lg]
-        worst = sorted(lg, key=lambda x: -x[3])[:3]
         return {"batches": len(lg), "mean_requests": float(np.mean([x[0] for x in lg])),
                 "gpu_ms_p50": pct(gpu, 50), "gpu_ms_p99": pct(gpu, 99),
-                "worst": [{"requests": x[0], "in_flight_ms": x[3] * 1e3, "gpu_ms": x[4], "gradient": x[5],
-                           "rerendered": x[6]} for x in worst],
-                "pairs_over_capacity_max": float(max(x[2] / max(x[1], 1) for x in lg)),
-                "capacity_over_pairs_mean": float(np.mean([x[1] / max(x[2], 1) for x in lg])),
                 "in_flight_ms_p50": pct(inflight, 50), "in_flight_ms_p99": pct(inflight, 99)}
 
     server.log = []
-    with ClockSampler(local) as clk:
-        reqs = make_requests()
-        r0, a0 = server.rerenders, server.reallocs
-        thr_poisson, lat_poisson = serve(reqs, True)
-        batch_sizes = [r.batch_size for r in reqs]
-        log_poisson = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
-        reqs = make_requests()
-        r0, a0 = server.rerenders, server.reallocs
-        thr_sat, lat_sat = serve(reqs, False)
-        log_sat = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+    reqs = make_requests()
+    r0, a0 = server.rerenders, server.reallocs
+    thr_poisson, lat_poisson = serve(reqs, True)
+    batch_sizes = [r.batch_size for r in reqs]
+    log_poisson = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+    reqs = make_requests()
+    r0, a0 = server.rerenders, server.reallocs
+    thr_sat, lat_sat = serve(reqs, False)
+    log_sat = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+    budget_gb, peak_gb = server.budget.budget / 1e9, server.budget.peak / 1e9
+    server.drain()
+    del server
     # plain per-request calls, one at a time, on the same arrival times
     reqs = make_requests()
+    ctx = splat.SplatContext(dev)
+    for r in reqs[:8]:  # grows the context's workspaces
+        sc = scenes[r.scene_id]
+        ctx.forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, camera_struct(r.camera), r.image,
+                    sc.sh_degree)
     t_free = 0.0
     lat_plain, service = [], []
     for r in reqs:
         sc = scenes[r.scene_id]
-        cam = r.camera
         torch.cuda.synchronize(dev)
         t = time.perf_counter()
-        fb, frame = splat.splat_forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, cam.view, cam.proj,
-                                        cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
-                                        cam.tan_fovy, sc.sh_degree)
+        ctx.forward(sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations, camera_struct(r.camera), r.image,
+                    sc.sh_degree)
         if r.backward:
-            splat.splat_backward(frame, r.grad_image, sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations)
+            splat.splat_backward(ctx.frame(), r.grad_image, sc.shs, sc.weights, sc.centroids, sc.scales, sc.rotations)
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t
         service.append(dt)
         start = max(r.arrival, t_free)
         t_free = start + dt
         lat_plain.append((t_free - r.arrival) * 1e3)
-        del fb, frame
     plain_thr = len(reqs) / sum(service)
-    line = {"metric": "served requests/s + p50/p99 ms, continuous batching, 8 scenes, Poisson 200 req/s",
-            "value": thr_sat, "unit": "requests/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * n_req / thr_sat / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "8 scenes (100k-3M Gaussians, log-uniform, config-0 distribution), random cameras "
-                                   "r=2.5-4, resolutions from 256x256 / 512x512 / 1280x720 / 1920x1080, 20% gradient "
-                                   "requests (N(0,1) image gradient)", "scene_gaussians": [int(n) for n in counts],
-                       "requests": n_req, "slots": 4, "max_batch": 8},
+    return {"workload": "8 scenes (100k-3M Gaussians, log-uniform, config-0 distribution), random cameras r=2.5-4, "
+                        "resolutions from 256x256 / 512x512 / 1280x720 / 1920x1080, 20% gradient requests (N(0,1) "
+                        "image gradient)",
+            "scene_gaussians": [int(n) for n in counts], "requests": n_req, "slots": 4, "max_batch": 8,
             "saturation": {"requests_per_s": thr_sat, "p50_ms": pct(lat_sat, 50), "p99_ms": pct(lat_sat, 99),
                            "note": "all requests queued at t=0", "batches": log_sat},
-            "poisson_200": {"requests_per_s": thr_poisson, "p50_ms": pct(lat_poisson, 50),
-                            "p99_ms": pct(lat_poisson, 99), "mean_batch": float(np.mean(batch_sizes)),
-                            "batches": log_poisson},
+            f"poisson_{int(rate)}": {"requests_per_s": thr_poisson, "p50_ms": pct(lat_poisson, 50),
+                                     "p99_ms": pct(lat_poisson, 99), "mean_batch": float(np.mean(batch_sizes)),
+                                     "batches": log_poisson},
             "plain_per_request": {"requests_per_s": plain_thr, "p50_ms": pct(lat_plain, 50),
                                   "p99_ms": pct(lat_plain, 99),
-                                  "note": "serial per-request calls on the same Poisson arrivals"},
-            "served_over_plain": thr_sat / plain_thr, "rerenders": server.rerenders,
-            "hbm_budget_gb": server.budget.budget / 1e9, "hbm_peak_gb": server.budget.peak / 1e9,
-            "clocks": clk.summary()}
+                                  "note": "serial per-request calls (workspaces kept) on the same Poisson arrivals"},
+            "served_over_plain": thr_sat / plain_thr, "hbm_budget_gb": budget_gb, "hbm_peak_gb": peak_gb}
+
+
+def run_serving(args):
+    """The serving workload (measure_serving) as its own JSON line."""
+    torch, dev, local = _gpu_common()
+    n_req = max(args.steps, 1) * 40
+    with ClockSampler(local) as clk:
+        r = measure_serving(dev, n_req=n_req, warmup=args.warmup)
+    thr = r["saturation"]["requests_per_s"]
+    line = {"metric": "served requests/s + p50/p99 ms, continuous batching, 8 scenes, Poisson 200 req/s",
+            "value": thr, "unit": "requests/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * n_req / thr / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": r.pop("workload"), "scene_gaussians": r.pop("scene_gaussians"),
+                       "requests": n_req, "slots": 4, "max_batch": 8},
+            **r, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -86,11 +86,36 @@ class SceneGrads(C.Structure):
                 ("rotations", C.c_void_p)]
 
 
+SERVE_SPLAT, SERVE_MARCH = 0, 1
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("n_slots", C.c_int32), ("max_views", C.c_int32), ("reserved", C.c_int32),
+                ("hbm_budget_bytes", C.c_size_t), ("capacity_margin", C.c_double)]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("scene", C.c_int32), ("camera", Camera), ("framebuffer", C.c_void_p),
+                ("grad_image", C.c_void_p), ("grads", SceneGrads), ("host_image", C.c_void_p), ("tag", C.c_uint64)]
+
+
+class ServerCompletion(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int), ("n_pairs", C.c_uint32), ("batch_size", C.c_int32),
+                ("rerendered", C.c_int32), ("submit_s", C.c_double), ("launch_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("batches", C.c_int64), ("rerenders", C.c_int64), ("deferred", C.c_int64),
+                ("reallocs", C.c_int32), ("reserved", C.c_int32), ("hbm_budget_bytes", C.c_size_t),
+                ("hbm_in_use_bytes", C.c_size_t), ("hbm_peak_bytes", C.c_size_t)]
+
+
 RENDER_FULL, RENDER_BINS, RENDER_DEPTH = 0, 1, 2
 
 
 class RenderOptions(C.Structure):
-    _fields_ = [("render_mode", C.c_int32), ("debug_bin", C.c_int32), ("max_depth", C.c_double)]
+    _fields_ = [("render_mode", C.c_int32), ("debug_bin", C.c_int32), ("max_depth", C.c_double),
+                ("work_counter", C.c_void_p)]
 
 
 # every symbol include/dgmr_b200.h declares, with its ctypes signature
@@ -138,6 +163,14 @@ _SIGNATURES = {
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                    C.c_void_p, C.c_void_p]),
     "dgmr_vm_set_const_samples": (C.c_int, [C.c_int32, C.c_void_p]),
+    "dgmr_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "dgmr_server_add_scene": (C.c_int, [C.c_void_p, C.POINTER(Scene), C.POINTER(C.c_int32)]),
+    "dgmr_server_submit": (C.c_int, [C.c_void_p, C.POINTER(ServerRequest)]),
+    "dgmr_server_poll": (C.c_int32, [C.c_void_p, C.POINTER(ServerCompletion), C.c_int32]),
+    "dgmr_server_wait": (C.c_int32, [C.c_void_p, C.POINTER(ServerCompletion), C.c_int32]),
+    "dgmr_server_pending": (C.c_int64, [C.c_void_p]),
+    "dgmr_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "dgmr_server_destroy": (C.c_int, [C.c_void_p]),
     "dgmr_status_string": (C.c_char_p, [C.c_int]),
     "dgmr_version": (C.c_char_p, []),
     "dgmr_launch_count": (C.c_uint64, []),

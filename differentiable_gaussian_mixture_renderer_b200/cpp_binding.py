@@ -55,13 +55,15 @@ _MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
 def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
             background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
             render_mode: str = "full", debug_render_bin: int = -1, max_depth: float = 20.0,
-            formulation: str | None = None):
+            formulation: str | None = None, work_counter: torch.Tensor | None = None):
     """``render_mode`` / ``debug_render_bin`` / ``max_depth`` are
     vol_marcher::ForwardData's debug fields (vol_marcher.h:48-56), which the
     reference's Python binding leaves at their defaults (Full, -1, 20).
     ``formulation`` (opacity, mass, density, ots, ols) replaces the compile-time
     vol_marcher::config::gaussian_mixture_formulation (vol_marcher.h:66); None
-    keeps its Opacity.  backward must be given the same one."""
+    keeps its Opacity.  backward must be given the same one.
+    ``work_counter`` (an int64 device tensor of one element, not in the
+    reference): the march adds its (ray, Gaussian, large step) bin fills to it."""
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -102,7 +104,8 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
         ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, n_pairs, dcode), dtype=torch.uint8, **opt)
         if render_mode not in _MODES:
             raise ValueError(f"render_mode must be one of {sorted(_MODES)}")
-        opts = N.RenderOptions(_MODES[render_mode], int(debug_render_bin), float(max_depth))
+        opts = N.RenderOptions(_MODES[render_mode], int(debug_render_bin), float(max_depth),
+                               N.ptr(work_counter) if work_counter is not None else None)
         N.check(lib.dgmr_vm_forward_render_options(scene, cam, opts, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
                 "vol_marcher forward render")
     return cache

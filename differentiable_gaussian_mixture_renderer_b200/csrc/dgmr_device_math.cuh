@@ -592,11 +592,19 @@ __device__ __noinline__ T cdf_inv_SD(T c, T inv_sd, T x)
     return cdf_inv_SD_inline(c, inv_sd, x);
 }
 
+// The adjoint of cdf_inv_SD at x is the normal pdf there times (-inv_sd,
+// x - c); the pdf is a call of its own so that the bin-adjoint loop, which
+// needs it at both borders of every bin, evaluates it once per border.
 template <class T>
-__device__ __noinline__ void grad_cdf_inv_SD(T c, T inv_sd, T x, T g, T* g_c, T* g_inv_sd)
+__device__ __noinline__ T pdf_inv_SD(T c, T inv_sd, T x)
 {
     const T u = (x - c) * inv_sd;
-    const T pdf = T(0.39894228040143267794) * dgmr_fm::exp_f(T(-0.5) * (u * u));
+    return T(0.39894228040143267794) * dgmr_fm::exp_f(T(-0.5) * (u * u));
+}
+
+template <class T>
+__device__ __forceinline__ void grad_cdf_inv_SD(T c, T inv_sd, T x, T g, T pdf, T* g_c, T* g_inv_sd)
+{
     *g_c = *g_c - g * inv_sd * pdf;
     *g_inv_sd = *g_inv_sd + g * (x - c) * pdf;
 }

@@ -276,15 +276,16 @@ __device__ __forceinline__ bool warp_entry_on_bins(const RayEntry<T>& en, V3<T> 
     return true;
 }
 
-// Pass 2 (vol_marcher_forward.cu:405-437): Gaussians in list order, bins spread over the lanes
+// Pass 2 (vol_marcher_forward.cu:405-437): Gaussians in list order, bins spread
+// over the lanes; returns how many Gaussians filled the bins (the same on every lane)
 template <class T>
-__device__ __forceinline__ void warp_fill(Bin<T> (&acc)[kRayRounds], const T* borders, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
+__device__ __forceinline__ unsigned warp_fill(Bin<T> (&acc)[kRayRounds], const T* borders, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
     const WarpRayMasks& rm, unsigned lane)
 {
 #pragma unroll
     for (unsigned r = 0; r < kRayRounds; ++r)
         acc[r] = Bin<T> { T(0), T(0), T(0), T(0) };
-    unsigned i = 0;
+    unsigned i = 0, fills = 0;
     for (int32_t base = b; base < e; base += 32, ++i) {
         const uint32_t m = rm.get(i) & lanes_below(e - base);
         if (!m)
@@ -303,6 +304,7 @@ __device__ __forceinline__ void warp_fill(Bin<T> (&acc)[kRayRounds], const T* bo
             }
         }
         uint32_t okm = __ballot_sync(0xffffffffu, ok);
+        fills += unsigned(__popc(okm));
         while (okm) {
             const int j = __ffs(int(okm)) - 1;
             okm &= okm - 1u;
@@ -310,6 +312,7 @@ __device__ __forceinline__ void warp_fill(Bin<T> (&acc)[kRayRounds], const T* bo
             warp_bins(acc, borders, __shfl_sync(0xffffffffu, centre, j), __shfl_sync(0xffffffffu, inv_sd, j), __shfl_sync(0xffffffffu, mor, j), c, lane);
         }
     }
+    return fills;
 }
 
 // bins to shared memory in order (.m = exp(-mass) for the blend, the mass itself for the peel)
@@ -343,6 +346,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
     T start = T(0);
     T distance = T(0); // Depth mode
     SectionSet<kLargeSteps, T>& sec = sm.sec;
+    unsigned long long fills = 0;
     for (unsigned step = 0;; ++step) {
         if (step >= kMaxLargeSteps) {
             if (lane == 0)
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
             sample_positions(sec, sm.borders);
         __syncwarp();
         Bin<T> acc[kRayRounds];
-        warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
+        fills += warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
         warp_store_bins(sm.bins, acc, lane, a.mode != DGMR_RENDER_BINS);
         if (a.mode == DGMR_RENDER_FULL) {
             // math.h:412-428, identical on every lane
@@ -397,6 +401,8 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
             break;
     }
     if (lane == 0) {
+        if (a.work)
+            atomicAdd(a.work, fills);
         const size_t pix = size_t(py) * cam.W + px;
         const size_t plane = size_t(cam.W) * cam.H;
         a.fb[pix] = colour.x + tr * cam.bg[0];
@@ -422,19 +428,15 @@ __device__ __noinline__ void lane_grad_entry(const VmMarch<T>& a, int32_t k, con
     V3<T> grgb = { T(0), T(0), T(0) }, gmu = { T(0), T(0), T(0) };
     S3<T> gQ = { { T(0), T(0), T(0), T(0), T(0), T(0) } };
     grad_sample_gaussian(en.mu, en.Q, o, d, en.mass, rgb, borders, gbins, &g_mass, &grgb, &gmu, &gQ, live_end);
-    T* dst = a.acc + size_t(en.id) * 10;
-    const T v[10] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5] };
+    // summed in double: a Gaussian's 13 totals collect terms from every ray and
+    // large step that reaches it, in no fixed order, and many cancel; float
+    // sums of that kind drift by far more than the gradients' 1e-3 tolerance
+    double* dst = a.acc + size_t(en.id) * kVmAcc;
+    const T v[kVmAcc] = { g_mass, grgb.x, grgb.y, grgb.z, gQ.v[0], gQ.v[1], gQ.v[2], gQ.v[3], gQ.v[4], gQ.v[5], gmu.x, gmu.y, gmu.z };
 #pragma unroll
-    for (int q = 0; q < 10; ++q)
+    for (int q = 0; q < int(kVmAcc); ++q)
         if (v[q] != T(0))
-            atomicAdd(dst + q, v[q]);
-    T* gm = a.g_centroids + size_t(en.id) * 3;
-    if (gmu.x != T(0))
-        atomicAdd(gm, gmu.x);
-    if (gmu.y != T(0))
-        atomicAdd(gm + 1, gmu.y);
-    if (gmu.z != T(0))
-        atomicAdd(gm + 2, gmu.z);
+            atomicAdd(dst + q, double(v[q]));
 }
 
 // Pass 3: the ray's Gaussians that reach the bins are gathered, in list

@@ -12,6 +12,9 @@
 
 namespace dgmr {
 
+// per-Gaussian backward accumulators (double): mass, rgb(3), inverse covariance(6), centroid(3)
+constexpr unsigned kVmAcc = 13;
+
 template <class T>
 struct ConstSamplesT {
     int n;
@@ -38,7 +41,7 @@ template <class T>
 struct VmLayout {
     uint32_t* stats;
     uint32_t* pre_scan_tmp;
-    T* acc; // [N,10]: mass, rgb(3), inverse covariance(6)
+    double* acc; // backward, [N,13]: mass, rgb(3), inverse covariance(6), centroid(3)
     BinningBuffers bin;
     size_t pre_bytes;
     size_t bytes;
@@ -58,7 +61,7 @@ inline VmLayout<T> vm_layout(uint32_t N, uint32_t n_tiles, uint32_t cap, void* b
     L.stats = c.take<uint32_t>(4);
     L.pre_scan_tmp = c.take<uint32_t>(scan_temp_bytes(N) / 4 + 8); // + room for k_pair_count's eight counters
     L.pre_bytes = c.off;
-    L.acc = c.take<T>(size_t(N) * 10);
+    L.acc = c.take<double>(size_t(N) * kVmAcc);
     carve_binning(c, L.bin, N, n_tiles, cap);
     L.bytes = c.off;
     return L;
@@ -208,13 +211,13 @@ struct VmMarch {
     T* fb;
     T* remaining_T;
     const T* grad_fb; // backward only
-    T* acc; // backward only: [N,10]
-    T* g_centroids; // backward only: [N,3]
+    double* acc; // backward only: [N,13] (kVmAcc)
     uint32_t* stats;
     ConstSamplesT<T> cs;
     int mode; // dgmr_render_mode (forward)
     int debug_bin;
     T max_depth;
+    unsigned long long* work; // forward, optional: (ray, Gaussian, large step) bin fills
 };
 
 // Which Gaussians of the tile list a ray can use.  Both passes of every large
@@ -255,10 +258,10 @@ struct VmBwdGauss {
     const T* rotations;
     const uint8_t* clamped;
     const int32_t* tiles_touched;
-    const T* acc;
+    const double* acc;
     T* g_sh;
     T* g_weights;
-    T* g_centroids; // accumulated onto the march's contribution
+    T* g_centroids; // the march's contribution plus the chain rule's
     T* g_scales;
     T* g_rotations;
     T aa;
@@ -272,6 +275,10 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.N)
         return;
+    const double* a = p.acc + size_t(i) * kVmAcc;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        p.g_centroids[3 * i + k] = T(a[10 + k]);
     for (int k = 0; k < p.sh_stride * 3; ++k)
         p.g_sh[size_t(i) * p.sh_stride * 3 + k] = T(0);
     p.g_weights[i] = T(0);
@@ -306,17 +313,16 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     if (mass <= T(0))
         return;
     const V3<T> dir = { delta.x / dist, delta.y / dist, delta.z / dist };
-    const T* a = p.acc + size_t(i) * 10;
-    const V3<T> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<T> { a[1], a[2], a[3] }, p.clamped + 3 * size_t(i), T(1), p.g_sh);
+    const V3<T> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<T> { T(a[1]), T(a[2]), T(a[3]) }, p.clamped + 3 * size_t(i), T(1), p.g_sh);
     V3<T> g_mu = mul3(g_dir, T(1) / dist);
     T g_dist = -dot3(g_dir, delta) / (dist * dist);
     S3<T> g_inv;
 #pragma unroll
     for (int k = 0; k < 6; ++k)
-        g_inv.v[k] = a[4 + k];
+        g_inv.v[k] = T(a[4 + k]);
     const S3<T> g_filtered = grad_inverse_sym3(filtered, g_inv);
     // adjoint of weight_to_mass (math.h:298-320)
-    const T g_mass = a[0];
+    const T g_mass = T(a[0]);
     T g_w = T(0);
     S2<T> g_cov2d = { { T(0), T(0), T(0) } };
     V3<T> g_s = { T(0), T(0), T(0) };
@@ -442,6 +448,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.mode = options ? options->render_mode : DGMR_RENDER_FULL;
     a.debug_bin = options ? options->debug_bin : -1;
     a.max_depth = options ? T(options->max_depth) : T(20);
+    a.work = options ? options->work_counter : nullptr;
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
     k_vm_march_warp<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
     note_launch();
@@ -460,8 +467,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
     if (N == 0)
         return DGMR_OK;
-    cudaMemsetAsync(L.acc, 0, size_t(N) * 10 * sizeof(T), s);
-    cudaMemsetAsync(g_centroids, 0, size_t(N) * 3 * sizeof(T), s);
+    cudaMemsetAsync(L.acc, 0, size_t(N) * kVmAcc * sizeof(double), s);
     VmMarch<T> a {};
     a.ranges = c->i_ranges;
     a.list = c->b_point_list;
@@ -474,7 +480,6 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     a.remaining_T = static_cast<T*>(c->remaining_transparency);
     a.grad_fb = static_cast<const T*>(grad_fb);
     a.acc = L.acc;
-    a.g_centroids = static_cast<T*>(g_centroids);
     a.stats = st_dev;
     a.cs = const_samples<T>();
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);

@@ -118,6 +118,9 @@ __device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V
     // they would add exact zeros
     k1 = k1 < live_end - 1 ? k1 : live_end - 1;
     T cdf_start = cdf_inv_SD(centre, inv_sd, borders[k0]);
+    // the pdf at a bin's right border is its successor's left one: kept for it
+    int pdf_border = -1;
+    T pdf_right = T(0);
     for (int k = k0; k <= k1; ++k) {
         const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);
         const T delta = cdf_end - cdf_start;
@@ -134,8 +137,11 @@ __device__ __forceinline__ void grad_sample_gaussian(V3<T> mu, const S3<T>& Q, V
             continue;
         g_mor = g_mor + g_m * delta;
         const T g_delta = g_m * mor;
-        grad_cdf_inv_SD(centre, inv_sd, borders[k], -g_delta, &g_centre, &g_inv_sd);
-        grad_cdf_inv_SD(centre, inv_sd, borders[k + 1], g_delta, &g_centre, &g_inv_sd);
+        const T pdf_left = pdf_border == k ? pdf_right : pdf_inv_SD(centre, inv_sd, borders[k]);
+        pdf_right = pdf_inv_SD(centre, inv_sd, borders[k + 1]);
+        pdf_border = k + 1;
+        grad_cdf_inv_SD(centre, inv_sd, borders[k], -g_delta, pdf_left, &g_centre, &g_inv_sd);
+        grad_cdf_inv_SD(centre, inv_sd, borders[k + 1], g_delta, pdf_right, &g_centre, &g_inv_sd);
     }
     const T g_w1d = g_mor * mass;
     *g_mass = *g_mass + g_mor * g.weight;

@@ -243,6 +243,14 @@ class RenderServer:
             if slot.request is not None:
                 self._finish(slot)
 
+    def release_buffers(self):
+        """Finishes what is in flight and drops the slots' workspaces and the
+        pooled result buffers (results still held by requests stay theirs)."""
+        self.drain()
+        self._pool.clear()
+        for slot in self.slots:
+            slot.frame_ws = slot.pair_ws = None
+
     def start_clock(self):
         """Anchor device completion times to the host clock (streams idle)."""
         torch.cuda.synchronize(self.device)
@@ -334,6 +342,9 @@ class ServeRequest:
     grads: tuple | None = None  # (sh, weights, centroids, scales, rotations)
     batch_size: int = 0
     rerendered: bool = False
+    kind: str = "splat"  # "splat", or "march" (vol_marcher; NativeServer only)
+    host_image: torch.Tensor | None = None  # optional pinned [3,H,W]: NativeServer copies the image there too
+    status: int = 0
 
 
 @dataclass
@@ -551,3 +562,120 @@ class ContinuousServer:
                 if slot.batch:
                     slot.done.synchronize()
                     break
+
+
+# ---------------------------------------------------------------------------
+# The same server in native code: the queue, the batch cutting, the HBM
+# admission, the capacity learning and the re-render of overflowed batches run
+# in C++ behind dgmr_server_* (csrc/dgmr_server.cpp); Python only hands it
+# device pointers and reads completions.  It also serves vol_marcher requests
+# (kind="march"), forward and backward, one per batch.
+
+
+class NativeServer:
+    """Continuous batching of splat and vol_marcher requests by the library's
+    C++ server.  Requests are ServeRequest objects as for ContinuousServer;
+    each owns its outputs (image, gradients, optional pinned host copy), and a
+    completed request's results equal the plain call's."""
+
+    def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3):
+        self.device = torch.device(device or "cuda")
+        self.lib = N.lib()
+        cfg = N.ServerConfig(self.device.index if self.device.index is not None else torch.cuda.current_device(),
+                             n_slots, max_batch, 0, int(hbm_budget_bytes or 0), capacity_margin)
+        handle = C.c_void_p()
+        N.check(self.lib.dgmr_server_create(C.byref(cfg), C.byref(handle)), "server create")
+        self._h = handle
+        self._t0 = time.perf_counter()
+        self.scenes = scenes
+        self._index = {}
+        self._c_scenes = {}
+        for sid, sc in scenes.items():
+            self._c_scenes[sid] = sc.c_scene()
+            idx = C.c_int32()
+            N.check(self.lib.dgmr_server_add_scene(self._h, C.byref(self._c_scenes[sid]), C.byref(idx)), "server scene")
+            self._index[sid] = idx.value
+        self._inflight: dict = {}
+        self._next_tag = 1
+        self._buf = (N.ServerCompletion * 64)()
+        self.completed: list = []
+
+    def submit(self, req: ServeRequest) -> ServeRequest:
+        sc = self.scenes[req.scene_id]
+        H, W = req.camera.height, req.camera.width
+        if req.kind not in ("splat", "march"):
+            raise ValueError("kind must be 'splat' or 'march'")
+        if req.backward and (req.grad_image is None or tuple(req.grad_image.shape) != (3, H, W)
+                             or req.grad_image.dtype != torch.float32 or not req.grad_image.is_contiguous()):
+            raise ValueError("a gradient request needs a contiguous float32 grad_image [3, H, W]")
+        if req.image is None:
+            req.image = torch.empty((3, H, W), dtype=torch.float32, device=self.device)
+        if req.backward and req.grads is None:
+            req.grads = (torch.empty_like(sc.shs), torch.empty_like(sc.weights), torch.empty_like(sc.centroids),
+                         torch.empty_like(sc.scales), torch.empty_like(sc.rotations))
+        r = N.ServerRequest()
+        r.kind = N.SERVE_MARCH if req.kind == "march" else N.SERVE_SPLAT
+        r.scene = self._index[req.scene_id]
+        r.camera = camera_struct(req.camera)
+        r.framebuffer = req.image.data_ptr()
+        if req.backward:
+            r.grad_image = req.grad_image.data_ptr()
+            g = req.grads
+            r.grads = N.SceneGrads(g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(), g[3].data_ptr(), g[4].data_ptr())
+        if req.host_image is not None:
+            if not req.host_image.is_pinned() or tuple(req.host_image.shape) != (3, H, W):
+                raise ValueError("host_image must be pinned float32 [3, H, W]")
+            r.host_image = req.host_image.data_ptr()
+        r.tag = self._next_tag
+        self._next_tag += 1
+        # work queued on torch's stream that produced the inputs must be done before the server's streams read them
+        torch.cuda.current_stream(self.device).synchronize()
+        N.check(self.lib.dgmr_server_submit(self._h, C.byref(r)), "server submit")
+        self._inflight[r.tag] = req
+        return req
+
+    def _collect(self, n: int) -> None:
+        failed = None
+        for k in range(n):
+            c = self._buf[k]
+            req = self._inflight.pop(c.tag)
+            req.t_launch = self._t0 + c.launch_s
+            req.t_done = self._t0 + c.done_s
+            req.batch_size = c.batch_size
+            req.rerendered = bool(c.rerendered)
+            req.status = c.status
+            self.completed.append(req)
+            if c.status != N.DGMR_OK and failed is None:
+                failed = c.status
+        if failed is not None:
+            N.check(failed, "served request")
+
+    def poll(self) -> int:
+        """Completes finished batches, launches new ones; returns the number of
+        requests still queued or in flight."""
+        self._collect(self.lib.dgmr_server_poll(self._h, self._buf, len(self._buf)))
+        return len(self._inflight)
+
+    def drain(self) -> None:
+        while self._inflight:
+            self._collect(self.lib.dgmr_server_wait(self._h, self._buf, len(self._buf)))
+
+    def stats(self) -> dict:
+        st = N.ServerStats()
+        N.check(self.lib.dgmr_server_get_stats(self._h, C.byref(st)), "server stats")
+        return {f: getattr(st, f) for f, _ in N.ServerStats._fields_ if f != "reserved"}
+
+    def close(self) -> None:
+        if self._h:
+            self.drain()
+            self.lib.dgmr_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self.lib.dgmr_server_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass

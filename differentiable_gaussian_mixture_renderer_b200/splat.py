@@ -154,3 +154,59 @@ class SplatRender(torch.autograd.Function):
 
 
 render = SplatRender.apply
+
+
+class SplatContext:
+    """The plain per-call splat path with its workspaces kept between calls.
+
+    Each ``forward`` is the reference's calling pattern
+    (splat_forward.cu:41-338): preprocess, one read back of the pair count
+    (its ``.item()`` at :204), binning and blend, one frame at a time on one
+    stream.  The frame and pair workspaces grow when a frame needs more (with
+    25 % headroom) and are never freed in between, as the C++ viewer
+    interface's Context does, so steady calls allocate nothing."""
+
+    def __init__(self, device=None, stream: torch.cuda.Stream | None = None, headroom: float = 1.25):
+        self.device = torch.device(device or "cuda")
+        self.stream = stream or torch.cuda.current_stream(self.device)
+        self.headroom = headroom
+        self.frame_ws = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self.pair_ws = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self.stats = torch.zeros(4, dtype=torch.int32, device=self.device)
+        self.stats_host = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+
+    def _grow(self, buf: torch.Tensor, nbytes: int) -> torch.Tensor:
+        if buf.numel() >= nbytes:
+            return buf
+        with torch.cuda.stream(self.stream):
+            return torch.empty(int(nbytes * self.headroom) + 256, dtype=torch.uint8, device=self.device)
+
+    def forward(self, shs, opacity, means3D, scales, rotations, camera: N.Camera, framebuffer: torch.Tensor,
+                sh_degree: int, formulation: str | None = None) -> int:
+        """Renders into ``framebuffer`` (float32 [3, H, W] on the device) and
+        returns the frame's pair count; the call returns once the pair count
+        is known, the image is complete when the stream reaches it."""
+        shs, opacity, means3D, scales, rotations = _prepare(shs, opacity, means3D, scales, rotations)
+        lib = N.lib()
+        n, W, H = int(means3D.shape[0]), int(camera.width), int(camera.height)
+        scene = N.make_scene(shs, opacity, means3D, scales, rotations, sh_degree, formulation)
+        s = self.stream.cuda_stream
+        self.frame_ws = self._grow(self.frame_ws, lib.dgmr_splat_frame_workspace_size(n, W, H))
+        N.check(lib.dgmr_splat_preprocess(scene, camera, N.ptr(self.frame_ws), self.frame_ws.numel(), N.ptr(self.stats),
+                                          s), "splat preprocess")
+        with torch.cuda.stream(self.stream):
+            self.stats_host.copy_(self.stats, non_blocking=True)
+        self.stream.synchronize()
+        pairs = int(self.stats_host[0])
+        self.pair_ws = self._grow(self.pair_ws, max(1, lib.dgmr_splat_pair_workspace_size(n, pairs)))
+        N.check(lib.dgmr_splat_render(scene, camera, N.ptr(framebuffer), N.ptr(self.frame_ws), self.frame_ws.numel(),
+                                      N.ptr(self.pair_ws), self.pair_ws.numel(), pairs, N.ptr(self.stats), s),
+                "splat render")
+        self._last = (scene, camera, n, W, H, pairs)
+        return pairs
+
+    def frame(self) -> SplatFrame:
+        """The last rendered frame, for splat_backward; valid until the next
+        forward of this context."""
+        scene, camera, n, W, H, pairs = self._last
+        return SplatFrame(self.frame_ws, self.pair_ws, pairs, self.stats, scene, camera, n, W, H)

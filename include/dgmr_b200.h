@@ -246,6 +246,11 @@ typedef struct dgmr_render_options {
     int32_t render_mode; /* dgmr_render_mode */
     int32_t debug_bin; /* -1 = last bin */
     double max_depth; /* 20 in the reference */
+    /* Optional device counter (NULL = none), marcher forward only: the march
+     * adds the number of (ray, Gaussian, large step) bin fills it makes, each
+     * 128 CDF evaluations and 127 bin updates -- the work unit its roofline
+     * is stated in.  No reference counterpart. */
+    unsigned long long* work_counter;
 } dgmr_render_options;
 
 size_t dgmr_vr_frame_workspace_size(int32_t n_gaussians, int32_t width, int32_t height);
@@ -312,6 +317,81 @@ dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera,
  * sections instead of collecting them from the Gaussians.  n_sections = 0
  * restores adaptive sampling.  Process-wide; at most 4 sections. */
 dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections);
+
+/* ------------------------------------------------------------- serving */
+
+/* A continuous-batching request server over resident scenes -- no reference
+ * counterpart (the reference renders one view per call from its training loop
+ * or viewer).  Requests wait in a queue; whenever one of n_slots slots (a CUDA
+ * stream with grow-only workspaces) is free, the queue head is cut into one
+ * batch: splat requests by the batched entry points above, as many as fit
+ * max_views, DGMR_BATCH_MAX_SCENES scene entries and the HBM budget (arrival
+ * order kept; a gradient request gets a scene entry of its own), a
+ * vol_marcher request alone.  Pair capacities are learnt per (scene,
+ * resolution, renderer): the first request of such a key reads its pair count
+ * back once (a host synchronisation); later ones launch without one, and a
+ * batch that overflowed renders again, exactly sized, before it completes.
+ * Each result equals the plain call's: images bit-identical, gradients up to
+ * the order of atomic additions.  The caller owns every output buffer and must
+ * not touch it before the request's completion is returned.  One thread
+ * drives a server; the server allocates its own workspaces (cudaMalloc). */
+typedef struct dgmr_server dgmr_server;
+
+typedef struct dgmr_server_config {
+    int32_t device; /* CUDA device of the server and its scenes */
+    int32_t n_slots; /* batches in flight, one stream each (0 = 4) */
+    int32_t max_views; /* splat views per batch, <= DGMR_BATCH_MAX_VIEWS (0 = 8) */
+    int32_t reserved;
+    size_t hbm_budget_bytes; /* device memory held for work in flight (0 = 80 % of free memory at creation) */
+    double capacity_margin; /* pair capacity = pairs seen x margin + 1024 (<= 0 = 1.3; below 1 forces re-renders) */
+} dgmr_server_config;
+
+typedef enum dgmr_serve_kind {
+    DGMR_SERVE_SPLAT = 0, /* splat forward (+ backward); dgmr_splat_forward / dgmr_splat_backward */
+    DGMR_SERVE_MARCH = 1, /* vol_marcher forward (+ backward), Full mode; dgmr_vm_forward_* / dgmr_vm_backward */
+} dgmr_serve_kind;
+
+typedef struct dgmr_server_request {
+    int32_t kind; /* dgmr_serve_kind */
+    int32_t scene; /* index from dgmr_server_add_scene */
+    dgmr_camera camera; /* camera and background */
+    float* framebuffer; /* [3,H,W] device, written */
+    const float* grad_image; /* [3,H,W] device image gradient, or NULL for a render only */
+    dgmr_scene_grads grads; /* gradient outputs (written) when grad_image != NULL; weights [N] */
+    void* host_image; /* optional pinned host [3,H,W] float: the image is copied there as well */
+    uint64_t tag; /* the caller's identifier, returned in the completion */
+} dgmr_server_request;
+
+typedef struct dgmr_server_completion {
+    uint64_t tag;
+    dgmr_status status;
+    uint32_t n_pairs; /* pairs of the request's batch */
+    int32_t batch_size; /* requests in that batch */
+    int32_t rerendered; /* 1 if the batch rendered again after a pair overflow */
+    double submit_s, launch_s, done_s; /* host clock, seconds since the server's creation */
+} dgmr_server_completion;
+
+typedef struct dgmr_server_stats {
+    int64_t submitted, batches, rerenders, deferred;
+    int32_t reallocs; /* workspace growths */
+    int32_t reserved;
+    size_t hbm_budget_bytes, hbm_in_use_bytes, hbm_peak_bytes;
+} dgmr_server_stats;
+
+dgmr_status dgmr_server_create(const dgmr_server_config* config, dgmr_server** out);
+/* float32 scenes only; the tensors stay the caller's and must outlive the server's use */
+dgmr_status dgmr_server_add_scene(dgmr_server* server, const dgmr_scene* scene, int32_t* index);
+dgmr_status dgmr_server_submit(dgmr_server* server, const dgmr_server_request* request);
+/* Completes finished batches, launches new ones, returns up to max_out
+ * completions (never blocks). */
+int32_t dgmr_server_poll(dgmr_server* server, dgmr_server_completion* out, int32_t max_out);
+/* As poll, but waits until at least one request completes; 0 when nothing is queued or in flight. */
+int32_t dgmr_server_wait(dgmr_server* server, dgmr_server_completion* out, int32_t max_out);
+/* Requests queued, in flight or completed and not yet returned. */
+int64_t dgmr_server_pending(const dgmr_server* server);
+dgmr_status dgmr_server_get_stats(const dgmr_server* server, dgmr_server_stats* out);
+/* Waits for work in flight, frees the server's memory. */
+dgmr_status dgmr_server_destroy(dgmr_server* server);
 
 /* ---------------------------------------------------------------- misc */
 const char* dgmr_status_string(dgmr_status status);

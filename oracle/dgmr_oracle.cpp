@@ -1771,8 +1771,9 @@ void orc_fmath_f32(int which, const float* x, float* y, int n)
 }
 
 // Decision audit: on = 1 resets the counters and starts counting, 0 stops;
-// out9 = (seen, flipped, near threshold) of alpha, section-mass and rect decisions.
-void orc_audit(int on, long* out9)
+// out10 = (seen, flipped, near threshold) of alpha, section-mass and rect
+// decisions, then the marcher's bin fills.
+void orc_audit(int on, long* out10)
 {
     DecisionAudit& a = audit();
     if (on) {
@@ -1781,14 +1782,17 @@ void orc_audit(int on, long* out9)
             a.flipped[k] = 0;
             a.near[k] = 0;
         }
+        a.fills = 0;
     }
     a.on = on;
-    if (out9)
+    if (out10) {
         for (int k = 0; k < AUDIT_KINDS; ++k) {
-            out9[3 * k] = a.seen[k].load();
-            out9[3 * k + 1] = a.flipped[k].load();
-            out9[3 * k + 2] = a.near[k].load();
+            out10[3 * k] = a.seen[k].load();
+            out10[3 * k + 1] = a.flipped[k].load();
+            out10[3 * k + 2] = a.near[k].load();
         }
+        out10[9] = a.fills.load();
+    }
 }
 
 } // extern "C"

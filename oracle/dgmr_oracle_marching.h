@@ -185,6 +185,8 @@ inline void sample_gaussian(T mass, V3<T> rgb, V3<T> pos, const S3<T>& inv_cov, 
     const T mass_in_bins = mass_on_ray * integrate_normalised_inv_SD(centre, inv_sd, borders[0], borders[NB]);
     if (mass_in_bins < T(0.0001f))
         return;
+    if (audit().on.load(std::memory_order_relaxed))
+        audit().fills.fetch_add(1, std::memory_order_relaxed);
     T cdf_start = cdf_inv_SD(centre, inv_sd, borders[0]);
     for (unsigned k = 0; k < NB; ++k) {
         const T cdf_end = cdf_inv_SD(centre, inv_sd, borders[k + 1]);

@@ -63,6 +63,7 @@ struct DecisionAudit {
     std::atomic<long> seen[AUDIT_KINDS] = {};
     std::atomic<long> flipped[AUDIT_KINDS] = {};
     std::atomic<long> near[AUDIT_KINDS] = {};
+    std::atomic<long> fills { 0 }; // marcher (ray, Gaussian, large step) bin fills, the march's work unit
 };
 inline DecisionAudit& audit()
 {

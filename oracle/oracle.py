@@ -339,9 +339,10 @@ def decision_audit():
     have taken the other way, and how many lie within 16 float ulps of the
     threshold (the only ones any exp / log within 16 ulps of the shared
     routines could flip).  Yields a dict filled on exit:
-    {kind: (seen, flipped, near)}."""
+    {kind: (seen, flipped, near)}, plus "fills": the marcher's (ray,
+    Gaussian, large step) bin fills of the block."""
     L = lib()
-    out = np.zeros(9, np.int64)
+    out = np.zeros(10, np.int64)
     L.orc_audit(1, out.ctypes.data_as(C.POINTER(C.c_long)))
     res: dict = {}
     try:
@@ -350,6 +351,7 @@ def decision_audit():
         L.orc_audit(0, out.ctypes.data_as(C.POINTER(C.c_long)))
         for k, name in enumerate(("alpha", "section_mass", "rect")):
             res[name] = (int(out[3 * k]), int(out[3 * k + 1]), int(out[3 * k + 2]))
+        res["fills"] = int(out[9])
 
 
 def set_const_samples(sections) -> None:

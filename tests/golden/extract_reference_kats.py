@@ -85,7 +85,9 @@ def extract(path: str) -> dict:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_reference_kats.py <path of the reference project checkout>")
+    ref = sys.argv[1]
     data = extract(os.path.join(ref, "unittests", "marching_steps.cpp"))
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "marching_steps_kats.json")
     with open(out, "w") as f:

@@ -79,8 +79,15 @@ def test_headline_frame_1080p_1M(cuda):
 
 def check_vm(sc, cam, dev, G, dtype=torch.float32):
     npdt = np.float32 if dtype == torch.float32 else np.float64
-    ref = O.vm_forward(sc, cam, dtype=npdt)
+    with O.decision_audit() as audit:
+        ref = O.vm_forward(sc, cam, dtype=npdt)
     cache, ts = run_vm(sc, cam, dev, dtype)
+    # the march's work unit: (ray, Gaussian, large step) bin fills, counted by the kernel
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    counter = torch.zeros(1, dtype=torch.int64, device=dev)
+    cpp_binding.forward(*ts[:5], *ts[5:9], cam.width, cam.height, cam.tan_fovx, cam.tan_fovy, sc.sh_degree,
+                        work_counter=counter)
+    assert int(counter.item()) == audit["fills"] > 0
     got = dict(zip(VM_NAMES, [c.cpu().numpy() for c in cache]))
     for k in ("rects", "tiles_touched", "point_offsets", "i_ranges", "b_point_list"):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
@@ -91,7 +98,6 @@ def check_vm(sc, cam, dev, G, dtype=torch.float32):
     assert np.abs(got["remaining_transparency"] - ref["remaining_transparency"]).max() <= IMAGE_TOL
     gref = O.vm_backward(sc, cam, ref, G, dtype=npdt)
     shs, w, mu, s, q, view, proj, campos, bgt = ts
-    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
     grads = cpp_binding.backward(shs, w, mu, s, q, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx,
                                  cam.tan_fovy, sc.sh_degree, torch.tensor(G, device=dev), cache)
     torch.cuda.synchronize()
