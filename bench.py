@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--slots", type=int, default=4, help="requests in flight")
     ap.add_argument("--plain", type=int, default=64, help="plain per-call requests")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--python-server", action="store_true",
+                    help="--workload serving: the Python ContinuousServer instead of the C++ server")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the short vol_marcher (100k, 512x512) and serving (8 scenes) runs of the headline line")
     ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving", "configs"], default="served",
@@ -322,6 +324,54 @@ def run_ours(args):
     ms_value, _, value = replica_totals(ms_value, local_renders, world, max_over_ranks, sum_over_ranks)
     ms_e2e, _, e2e_value = replica_totals(ms_e2e, local_renders, world, max_over_ranks, sum_over_ranks)
 
+    # ---------------------------------------------------------------- the C++ server, same workload
+    # (continuous batching: requests cut into batches of the batched entry points; host clock
+    # from the first submission to the last completion, images to pinned host memory)
+    native = None
+    if not args.no_extras:
+        nserver = serving.NativeServer({"scene": scene}, dev, n_slots=args.slots, max_batch=args.batch)
+        hosts = [torch.empty((3, args.height, args.width), dtype=torch.float32, pin_memory=True)
+                 for _ in range(2 * args.batch)]
+        fbs = [torch.empty((3, args.height, args.width), dtype=torch.float32, device=dev) for _ in range(2 * args.batch)]
+
+        def native_leg(cam_list, to_host):
+            reqs = []
+            for i, cam in enumerate(cam_list):
+                r = serving.ServeRequest("scene", cam)
+                r.image = fbs[i % len(fbs)]
+                r.host_image = hosts[i % len(hosts)] if to_host else None
+                reqs.append(r)
+            for r in reqs[:2 * args.batch]:  # warm-up: capacities learnt, workspaces grown
+                nserver.submit(r)
+            nserver.drain()
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            for k, r in enumerate(reqs):
+                # a result buffer is reused 2 x batch requests later: wait for its request first
+                if k >= len(fbs):
+                    while reqs[k - len(fbs)].t_done == 0.0:
+                        nserver.poll()
+                r.t_done = 0.0
+                nserver.submit(r)
+                nserver.poll()
+            nserver.drain()
+            torch.cuda.synchronize(dev)
+            dt = time.perf_counter() - t
+            lat = [(r.t_done - r.t_launch) * 1e3 for r in reqs]
+            return len(reqs) / dt, lat, float(np.mean([r.batch_size for r in reqs]))
+
+        nv, nlat, nbatch = native_leg(cams[:n_req], False)
+        ne, nlat_e, nbatch_e = native_leg(cams[n_req:2 * n_req], True)
+        st = nserver.stats()
+        nserver.close()
+        del nserver, hosts, fbs
+        native = {"value": nv, "e2e": ne, "unit": UNIT, "mean_batch": nbatch, "launch_to_done_ms_p50": pct(nlat, 50),
+                  "launch_to_done_ms_p99": pct(nlat, 99), "e2e_launch_to_done_ms_p50": pct(nlat_e, 50),
+                  "rerenders": st["rerenders"],
+                  "note": "the C++ continuous-batching server (dgmr_server_*, batches of up to requests_per_step "
+                          "views), host clock over the same number of requests; e2e with each image copied to "
+                          "pinned host memory"}
+
     # ---------------------------------------------------------------- plain per-call leg
     # one request at a time on one stream, the reference's pattern: preprocess, the pair count
     # read back, binning + blend, the image copied to pinned host memory and waited for; the
@@ -420,6 +470,7 @@ def run_ours(args):
             "served_over_plain_p50": (e2e_value / plain_rps_p50) if plain_rps_p50 else None,
             "served_over_plain_note": "e2e (served, every image copied to host) over the plain per-call leg with "
                                       "the same copy; _p50 uses the plain leg's median latency",
+            "served_native": native,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": args.batch * 8 * (16 + 16 + 3 + 3 + 3 + 1),
                     "d2h_bytes_per_step": args.batch * 3 * args.width * args.height * 4,
@@ -616,19 +667,21 @@ def run_marcher(args):
     return 0
 
 
-def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0):
+def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0, native: bool = True):
     """8 resident scenes (100k-3M Gaussians, log-uniform), a Poisson request
     stream at ``rate`` req/s, resolutions drawn from 256^2 / 512^2 / 1280x720 /
     1920x1080, 20 % of requests also asking for the gradient against an N(0,1)
     image gradient.  The continuous-batching server, saturated (all requests
     queued at once) and on the Poisson arrivals, against a serial server that
     makes the plain per-request calls (preprocess, pair count read back,
-    render, backward; workspaces kept) on the same arrival times."""
+    render, backward; workspaces kept) on the same arrival times.  ``native``:
+    the C++ server (dgmr_server_*, NativeServer), else the Python one
+    (ContinuousServer)."""
     import torch
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
     from differentiable_gaussian_mixture_renderer_b200 import splat
-    from differentiable_gaussian_mixture_renderer_b200.serving import (ContinuousServer, GaussianScene, ServeRequest,
-                                                                         camera_struct)
+    from differentiable_gaussian_mixture_renderer_b200.serving import (ContinuousServer, GaussianScene, NativeServer,
+                                                                         ServeRequest, camera_struct)
     rng = np.random.default_rng(7)
     counts = np.exp(rng.uniform(np.log(1e5), np.log(3e6), size=8)).astype(int)
     scenes = {f"s{i}": GaussianScene.from_numpy(S.make_scene(int(n), seed=20 + i), dev) for i, n in enumerate(counts)}
@@ -655,7 +708,18 @@ def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0)
             out.append(req)
         return out
 
-    server = ContinuousServer(scenes, dev, n_slots=4, max_batch=8)
+    server = (NativeServer if native else ContinuousServer)(scenes, dev, n_slots=4, max_batch=8)
+
+    def counters():
+        if native:
+            st = server.stats()
+            return st["rerenders"], st["reallocs"]
+        return server.rerenders, server.reallocs
+
+    def busy():
+        if native:
+            return server.poll() > 0
+        return bool(server.queue or any(sl.batch for sl in server.slots))
     # warm-up: one pass over a request set of the same distribution (other cameras) learns every
     # (scene, resolution) pair capacity and grows the slots' workspaces to their steady size
     warm = make_requests()
@@ -673,19 +737,27 @@ def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         i = 0
-        while i < len(reqs) or server.queue or any(sl.batch for sl in server.slots):
+        while True:
             now = time.perf_counter() - t0
             while i < len(reqs) and (not poisson or reqs[i].arrival <= now):
                 reqs[i].arrival = reqs[i].arrival if poisson else 0.0
                 server.submit(reqs[i])
                 i += 1
-            server.poll()
+            if not busy() and i >= len(reqs):
+                break
+            if not native:
+                server.poll()
         torch.cuda.synchronize(dev)
         lat = [(r.t_done - t0 - r.arrival) * 1e3 for r in reqs]
         span = max(r.t_done for r in reqs) - t0
         return len(reqs) / span, lat
 
-    def batch_log():
+    def batch_log(reqs):
+        if native:
+            sizes = [r.batch_size for r in reqs]
+            infl = [(r.t_done - r.t_launch) * 1e3 for r in reqs]
+            return {"mean_requests": float(np.mean(sizes)), "in_flight_ms_p50": pct(infl, 50),
+                    "in_flight_ms_p99": pct(infl, 99)}
         lg = server.log
         server.log = []
         if not lg:
@@ -698,16 +770,23 @@ def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0)
 
     server.log = []
     reqs = make_requests()
-    r0, a0 = server.rerenders, server.reallocs
+    r0, a0 = counters()
     thr_poisson, lat_poisson = serve(reqs, True)
     batch_sizes = [r.batch_size for r in reqs]
-    log_poisson = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
+    r1, a1 = counters()
+    log_poisson = dict(batch_log(reqs), rerenders=r1 - r0, reallocs=a1 - a0)
     reqs = make_requests()
-    r0, a0 = server.rerenders, server.reallocs
+    r0, a0 = counters()
     thr_sat, lat_sat = serve(reqs, False)
-    log_sat = dict(batch_log(), rerenders=server.rerenders - r0, reallocs=server.reallocs - a0)
-    budget_gb, peak_gb = server.budget.budget / 1e9, server.budget.peak / 1e9
-    server.drain()
+    r1, a1 = counters()
+    log_sat = dict(batch_log(reqs), rerenders=r1 - r0, reallocs=a1 - a0)
+    if native:
+        st = server.stats()
+        budget_gb, peak_gb = st["hbm_budget_bytes"] / 1e9, st["hbm_peak_bytes"] / 1e9
+        server.close()
+    else:
+        budget_gb, peak_gb = server.budget.budget / 1e9, server.budget.peak / 1e9
+        server.drain()
     del server
     # plain per-request calls, one at a time, on the same arrival times
     reqs = make_requests()
@@ -745,7 +824,8 @@ def measure_serving(dev, n_req: int = 200, warmup: int = 1, rate: float = 200.0)
             "plain_per_request": {"requests_per_s": plain_thr, "p50_ms": pct(lat_plain, 50),
                                   "p99_ms": pct(lat_plain, 99),
                                   "note": "serial per-request calls (workspaces kept) on the same Poisson arrivals"},
-            "served_over_plain": thr_sat / plain_thr, "hbm_budget_gb": budget_gb, "hbm_peak_gb": peak_gb}
+            "served_over_plain": thr_sat / plain_thr, "hbm_budget_gb": budget_gb, "hbm_peak_gb": peak_gb,
+            "server": "C++ (dgmr_server_*)" if native else "Python (ContinuousServer)"}
 
 
 def run_serving(args):
@@ -753,7 +833,7 @@ def run_serving(args):
     torch, dev, local = _gpu_common()
     n_req = max(args.steps, 1) * 40
     with ClockSampler(local) as clk:
-        r = measure_serving(dev, n_req=n_req, warmup=args.warmup)
+        r = measure_serving(dev, n_req=n_req, warmup=args.warmup, native=not args.python_server)
     thr = r["saturation"]["requests_per_s"]
     line = {"metric": "served requests/s + p50/p99 ms, continuous batching, 8 scenes, Poisson 200 req/s",
             "value": thr, "unit": "requests/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,

@@ -115,3 +115,30 @@ def test_batch_bad_arguments_without_gpu():
                                                C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
     scenes, views = _batch_tables(2)
     assert lib.dgmr_splat_batch_forward(scenes, 1, views, 2, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+
+
+def test_server_entry_points_without_gpu():
+    """The native server's argument checks run on the host; without a device
+    dgmr_server_create reports DGMR_ERR_CUDA instead of crashing."""
+    import ctypes as C
+    lib = _native.load()
+    assert lib.dgmr_server_create(None, None) == _native.DGMR_ERR_BAD_ARG
+    handle = C.c_void_p()
+    cfg = _native.ServerConfig(0, 4, 8, 0, 0, 1.3)
+    st = lib.dgmr_server_create(C.byref(cfg), C.byref(handle))
+    if st == _native.DGMR_OK:  # a GPU is present: exercise the host-side checks, then release it
+        req = _native.ServerRequest()
+        assert lib.dgmr_server_submit(handle, C.byref(req)) == _native.DGMR_ERR_BAD_ARG  # no scene, no framebuffer
+        assert lib.dgmr_server_poll(handle, None, 0) == 0 and lib.dgmr_server_pending(handle) == 0
+        assert lib.dgmr_server_destroy(handle) == _native.DGMR_OK
+    else:
+        assert st == _native.DGMR_ERR_CUDA and not handle.value
+    assert lib.dgmr_server_submit(None, None) == _native.DGMR_ERR_BAD_ARG
+    assert lib.dgmr_server_poll(None, None, 0) == -1 and lib.dgmr_server_wait(None, None, 0) == -1
+    assert lib.dgmr_server_pending(None) == -1
+    assert lib.dgmr_server_get_stats(None, None) == _native.DGMR_ERR_BAD_ARG
+    assert lib.dgmr_server_destroy(None) == _native.DGMR_ERR_BAD_ARG
+    scene = _native.Scene()
+    scene.dtype = 1  # float64 scenes are not served
+    idx = C.c_int32()
+    assert lib.dgmr_server_add_scene(None, C.byref(scene), C.byref(idx)) == _native.DGMR_ERR_BAD_ARG

@@ -126,11 +126,11 @@ def test_render_server_results_are_not_reused(cuda, to_host):
         reqs.append(server.submit(Request("ab"[k % 2], S.random_cameras(1, w, h, seed=300 + k)[0], to_host=to_host)))
     server.drain()
     for k, req in enumerate(reqs):
-        fb, _ = _alone(scenes[req.scene_id], req)
+        fb = _render_alone(scenes[req.scene_id], req.camera)
         img = req.image.to(cuda) if to_host else req.image
         assert img.is_pinned() if to_host else img.is_cuda
         assert torch.equal(img, fb), f"request {k}: image was overwritten by a later request"
-    held = {r.image.data_ptr() for r in reqs}
+    held = {r.image.data_ptr() for r in reqs}  # eight distinct result buffers
     assert len(held) == 8
     for r in reqs:
         r.release()
@@ -138,5 +138,12 @@ def test_render_server_results_are_not_reused(cuda, to_host):
     again = server.submit(Request("a", S.random_cameras(1, *RES[0], seed=400)[0], to_host=to_host))
     server.drain()
     assert again.image.data_ptr() in held
-    fb, _ = _alone(scenes["a"], again)
+    fb = _render_alone(scenes["a"], again.camera)
     assert torch.equal(again.image.to(cuda) if to_host else again.image, fb)
+
+
+def _render_alone(scene, cam):
+    fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations, cam.view,
+                                cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
+                                cam.tan_fovy, scene.sh_degree)
+    return fb
