@@ -613,28 +613,40 @@ def measure_marcher(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int
     G = torch.randn(3, H, W, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
     bg = torch.zeros(3, device=dev)
     counter = torch.zeros(1, dtype=torch.int64, device=dev)
-    fwd, bwd, fills = [], [], []
+    fwd, bwd, fills, fwd_s, bwd_s = [], [], [], [], []
+    store = cpp_binding.make_step_store(W, H, 4, device=dev)
     l0 = N.lib().dgmr_launch_count()
     for k, cam in enumerate(cams):
         v, p, c = t(cam.view), t(cam.proj), t(cam.campos)
         counter.zero_()
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0, e1, e2, e3, e4 = (torch.cuda.Event(enable_timing=True) for _ in range(5))
         e0.record()
         cache = cpp_binding.forward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, work_counter=counter)
         e1.record()
         cpp_binding.backward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache)
         e2.record()
-        e2.synchronize()
+        # the same frame with the sample steps kept by the forward (vol_marcher.apply's default when memory allows)
+        cache = cpp_binding.forward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, step_store=store)
+        e3.record()
+        cpp_binding.backward(*ins, v, p, c, bg, W, H, cam.tan_fovx, cam.tan_fovy, 0, G, cache, step_store=store)
+        e4.record()
+        e4.synchronize()
         if k == 0:
             l0 = N.lib().dgmr_launch_count()
             continue
         fwd.append(e0.elapsed_time(e1))
         bwd.append(e1.elapsed_time(e2))
+        fwd_s.append(e2.elapsed_time(e3))
+        bwd_s.append(e3.elapsed_time(e4))
         fills.append(int(counter.item()))
     launches = N.lib().dgmr_launch_count() - l0
     fills_per_s = sum(fills) / (sum(fwd) * 1e-3)
     out = {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
            "backward_over_forward": statistics.median(bwd) / statistics.median(fwd),
+           "stored_steps": {"forward_ms": statistics.median(fwd_s), "backward_ms": statistics.median(bwd_s),
+                            "backward_over_forward": statistics.median(bwd_s) / statistics.median(fwd_s),
+                            "note": "forward keeps the first 4 large steps' samples of every ray, the backward reads "
+                                    "them (vol_marcher.apply when the store fits 25 % of free memory)"},
            "bin_fills_per_frame": statistics.median(fills), "cdf_evaluations_per_s": 128 * fills_per_s,
            "gpu_launches": int(launches), "frames": len(fwd),
            "workload": f"vol_marcher forward + backward, {n} Gaussians (config-0 distribution), {W}x{H}, random "

@@ -162,6 +162,13 @@ _SIGNATURES = {
     "dgmr_vm_backward": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                    C.c_void_p, C.c_void_p]),
+    "dgmr_vm_step_store_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "dgmr_vm_forward_render_stored": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderOptions),
+                                                C.POINTER(VmCache), C.c_int64, C.c_void_p, C.c_size_t, C.c_void_p,
+                                                C.c_size_t, C.c_int32, C.c_void_p, C.c_void_p]),
+    "dgmr_vm_backward_stored": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(VmCache), C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_size_t, C.c_void_p, C.c_size_t, C.c_int32, C.c_void_p, C.c_void_p]),
     "dgmr_vm_set_const_samples": (C.c_int, [C.c_int32, C.c_void_p]),
     "dgmr_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "dgmr_server_add_scene": (C.c_int, [C.c_void_p, C.POINTER(Scene), C.POINTER(C.c_int32)]),

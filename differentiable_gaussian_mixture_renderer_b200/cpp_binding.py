@@ -55,7 +55,7 @@ _MODES = {"full": N.RENDER_FULL, "bins": N.RENDER_BINS, "depth": N.RENDER_DEPTH}
 def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
             background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
             render_mode: str = "full", debug_render_bin: int = -1, max_depth: float = 20.0,
-            formulation: str | None = None, work_counter: torch.Tensor | None = None):
+            formulation: str | None = None, work_counter: torch.Tensor | None = None, step_store=None):
     """``render_mode`` / ``debug_render_bin`` / ``max_depth`` are
     vol_marcher::ForwardData's debug fields (vol_marcher.h:48-56), which the
     reference's Python binding leaves at their defaults (Full, -1, 20).
@@ -63,7 +63,10 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
     vol_marcher::config::gaussian_mixture_formulation (vol_marcher.h:66); None
     keeps its Opacity.  backward must be given the same one.
     ``work_counter`` (an int64 device tensor of one element, not in the
-    reference): the march adds its (ray, Gaussian, large step) bin fills to it."""
+    reference): the march adds its (ray, Gaussian, large step) bin fills to it.
+    ``step_store`` (not in the reference): ``(uint8 device tensor, steps)``
+    from ``make_step_store``; the forward keeps its sample steps there for a
+    backward given the same store."""
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -106,14 +109,19 @@ def forward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matri
             raise ValueError(f"render_mode must be one of {sorted(_MODES)}")
         opts = N.RenderOptions(_MODES[render_mode], int(debug_render_bin), float(max_depth),
                                N.ptr(work_counter) if work_counter is not None else None)
-        N.check(lib.dgmr_vm_forward_render_options(scene, cam, opts, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
-                "vol_marcher forward render")
+        if step_store is None:
+            N.check(lib.dgmr_vm_forward_render_options(scene, cam, opts, c, n_pairs, N.ptr(ws), ws.numel(), None, stream),
+                    "vol_marcher forward render")
+        else:
+            buf, steps = step_store
+            N.check(lib.dgmr_vm_forward_render_stored(scene, cam, opts, c, n_pairs, N.ptr(ws), ws.numel(), N.ptr(buf),
+                                                      buf.numel(), int(steps), None, stream), "vol_marcher forward render")
     return cache
 
 
 def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix, cam_position,
              background, render_width: int, render_height: int, tan_fovx: float, tan_fovy: float, sh_degree: int,
-             grad_framebuffer, cache_vector, formulation: str | None = None):
+             grad_framebuffer, cache_vector, formulation: str | None = None, step_store=None):
     names = ("sh_params", "weights", "centroids", "cov_scales", "cov_rotations", "view_matrix", "proj_matrix",
              "cam_position", "background")
     dt, dev = _check_inputs([sh_params, weights, centroids, cov_scales, cov_rotations, view_matrix, proj_matrix,
@@ -143,10 +151,28 @@ def backward(sh_params, weights, centroids, cov_scales, cov_rotations, view_matr
         # sized with the frame's pair count: the march uses the room for its per-ray Gaussian masks
         n_pairs = int(cache[11].numel()) if cache[11] is not None else 0
         ws = torch.empty(lib.dgmr_vm_workspace_size(n, W, H, n_pairs, N.dtype_code(dt)), dtype=torch.uint8, device=dev)
-        N.check(lib.dgmr_vm_backward(scene, cam, c, N.ptr(grad_framebuffer), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
-                                     N.ptr(g_s), N.ptr(g_q), N.ptr(ws), ws.numel(), None, N.stream_handle()),
-                "vol_marcher backward")
+        if step_store is None:
+            N.check(lib.dgmr_vm_backward(scene, cam, c, N.ptr(grad_framebuffer), N.ptr(g_sh), N.ptr(g_w), N.ptr(g_mu),
+                                         N.ptr(g_s), N.ptr(g_q), N.ptr(ws), ws.numel(), None, N.stream_handle()),
+                    "vol_marcher backward")
+        else:
+            buf, steps = step_store
+            N.check(lib.dgmr_vm_backward_stored(scene, cam, c, N.ptr(grad_framebuffer), N.ptr(g_sh), N.ptr(g_w),
+                                                N.ptr(g_mu), N.ptr(g_s), N.ptr(g_q), N.ptr(ws), ws.numel(), N.ptr(buf),
+                                                buf.numel(), int(steps), None, N.stream_handle()), "vol_marcher backward")
     return [g_sh, g_w, g_mu, g_s, g_q]
+
+
+def make_step_store(render_width: int, render_height: int, steps: int, dtype=torch.float32, device=None):
+    """A sample-step store for ``steps`` large steps of every ray of a frame
+    (not in the reference): pass it to forward and to the backward of the
+    same frame, which then skips recomputing those steps' section sets and
+    sample positions.  Returns ``(tensor, steps)``."""
+    lib = N.lib()
+    nbytes = lib.dgmr_vm_step_store_size(int(render_width), int(render_height), int(steps), N.dtype_code(dtype))
+    if nbytes == 0:
+        raise ValueError("invalid step store size")
+    return torch.empty(nbytes, dtype=torch.uint8, device=device or "cuda"), int(steps)
 
 
 def set_const_samples(sections) -> None:

@@ -360,6 +360,16 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
         if (lane == 0)
             sample_positions(sec, sm.borders);
         __syncwarp();
+        if (step < a.store_steps) {
+            // keep this step's samples for the backward (coalesced: 32 lanes x 4 rounds)
+            const size_t ray = size_t(py) * cam.W + px, rays = size_t(cam.W) * cam.H;
+            T* dst = a.store_borders + (size_t(step) * rays + ray) * kSmallSteps;
+#pragma unroll
+            for (unsigned r = 0; r < kRayRounds; ++r)
+                dst[32 * r + lane] = sm.borders[32 * r + lane];
+            if (lane == 0)
+                a.store_sections[size_t(step) * rays + ray] = int32_t(sec.n);
+        }
         Bin<T> acc[kRayRounds];
         fills += warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
         warp_store_bins(sm.bins, acc, lane, a.mode != DGMR_RENDER_BINS);
@@ -526,13 +536,26 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
                 atomicOr(&a.stats[1], DGMR_FLAG_STEP_LIMIT);
             break;
         }
-        if (lane == 0)
-            sec.reset(start);
-        __syncwarp();
-        warp_collect(sec, a, b, e, o, d, rm, lane);
-        if (lane == 0)
-            sample_positions(sec, sm.borders);
-        __syncwarp();
+        int n_sections;
+        if (step < a.store_steps) {
+            // the forward kept this step's samples: no section set, no sampling
+            const size_t ray = size_t(py) * cam.W + px, rays = size_t(cam.W) * cam.H;
+            const T* src = a.store_borders + (size_t(step) * rays + ray) * kSmallSteps;
+#pragma unroll
+            for (unsigned r = 0; r < kRayRounds; ++r)
+                sm.borders[32 * r + lane] = src[32 * r + lane];
+            n_sections = a.store_sections[size_t(step) * rays + ray];
+            __syncwarp();
+        } else {
+            if (lane == 0)
+                sec.reset(start);
+            __syncwarp();
+            warp_collect(sec, a, b, e, o, d, rm, lane);
+            if (lane == 0)
+                sample_positions(sec, sm.borders);
+            __syncwarp();
+            n_sections = int(sec.n);
+        }
         Bin<T> acc[kRayRounds];
         warp_fill(acc, sm.borders, a, b, e, o, d, rm, lane);
         warp_store_bins(sm.bins, acc, lane, false);
@@ -565,7 +588,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
                 sm.gbins[k] = Bin<T> { T(0), T(0), T(0), T(0) };
         __syncwarp();
         warp_grad(sm.gbins, sm.borders, sm.queue, a, b, e, o, d, rm, lane, live_end);
-        const bool done = sec.n == 0 || tr < T(1.f / 255.f);
+        const bool done = n_sections == 0 || tr < T(1.f / 255.f);
         start = sm.borders[kSmallSteps - 1];
         __syncwarp();
         if (done)

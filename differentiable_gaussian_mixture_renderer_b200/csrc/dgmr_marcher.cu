@@ -218,7 +218,27 @@ struct VmMarch {
     int debug_bin;
     T max_depth;
     unsigned long long* work; // forward, optional: (ray, Gaussian, large step) bin fills
+    // optional step store: the forward writes, the backward reads, for the first
+    // store_steps large steps of every ray, its kSmallSteps sample borders
+    // ([step][ray][kSmallSteps]) and its section count ([step][ray])
+    T* store_borders;
+    int32_t* store_sections;
+    uint32_t store_steps;
 };
+
+// the step store inside one buffer: the borders first, then the section counts
+template <class T>
+inline void carve_step_store(void* base, uint32_t n_rays, uint32_t steps, T** borders, int32_t** sections)
+{
+    char* p = static_cast<char*>(base);
+    *borders = reinterpret_cast<T*>(p);
+    *sections = reinterpret_cast<int32_t*>(p + align_up(size_t(steps) * n_rays * kSmallSteps * sizeof(T)));
+}
+
+inline size_t step_store_bytes(uint32_t n_rays, uint32_t steps, size_t elem)
+{
+    return align_up(size_t(steps) * n_rays * kSmallSteps * elem) + align_up(size_t(steps) * n_rays * sizeof(int32_t));
+}
 
 // Which Gaussians of the tile list a ray can use.  Both passes of every large
 // step only act on a Gaussian that passes its gate -- pass 1's (mass on the
@@ -415,7 +435,7 @@ dgmr_status vm_preprocess(const dgmr_scene* scene, const dgmr_camera* camera, dg
 
 template <class T>
 dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_vm_cache* c, int64_t cap64, void* workspace, size_t workspace_bytes,
-    dgmr_frame_stats* stats, cudaStream_t s, const dgmr_render_options* options)
+    dgmr_frame_stats* stats, cudaStream_t s, const dgmr_render_options* options, void* store = nullptr, uint32_t store_steps = 0)
 {
     const uint32_t N = uint32_t(scene->n_gaussians), cap = uint32_t(cap64);
     const VmLayout<T> L = vm_layout<T>(N, frame_tiles(camera), cap, workspace);
@@ -449,6 +469,10 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
     a.debug_bin = options ? options->debug_bin : -1;
     a.max_depth = options ? T(options->max_depth) : T(20);
     a.work = options ? options->work_counter : nullptr;
+    if (store && store_steps > 0) {
+        carve_step_store<T>(store, uint32_t(camera->width) * uint32_t(camera->height), store_steps, &a.store_borders, &a.store_sections);
+        a.store_steps = store_steps;
+    }
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
     k_vm_march_warp<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
     note_launch();
@@ -457,7 +481,8 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
 
 template <class T>
 dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* c, const void* grad_fb, void* g_sh, void* g_weights,
-    void* g_centroids, void* g_scales, void* g_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, cudaStream_t s)
+    void* g_centroids, void* g_scales, void* g_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats, cudaStream_t s,
+    const void* store = nullptr, uint32_t store_steps = 0)
 {
     const uint32_t N = uint32_t(scene->n_gaussians);
     const VmLayout<T> L = vm_layout<T>(N, frame_tiles(camera), 0, workspace);
@@ -482,6 +507,11 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
     a.acc = L.acc;
     a.stats = st_dev;
     a.cs = const_samples<T>();
+    if (store && store_steps > 0) {
+        carve_step_store<T>(const_cast<void*>(store), uint32_t(camera->width) * uint32_t(camera->height), store_steps, &a.store_borders,
+            &a.store_sections);
+        a.store_steps = store_steps;
+    }
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
     k_vm_march_warp_bwd<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
     note_launch();
@@ -574,6 +604,56 @@ dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera,
             workspace_bytes, stats, s);
     return vm_backward<float>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
         workspace_bytes, stats, s);
+}
+
+size_t dgmr_vm_step_store_size(int32_t width, int32_t height, int32_t store_steps, int32_t dtype)
+{
+    if (width <= 0 || height <= 0 || store_steps < 0 || store_steps > int32_t(kMaxLargeSteps))
+        return 0;
+    return step_store_bytes(uint32_t(width) * uint32_t(height), uint32_t(store_steps), dtype == DGMR_F64 ? sizeof(double) : sizeof(float));
+}
+
+dgmr_status dgmr_vm_forward_render_stored(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options, dgmr_vm_cache* cache,
+    int64_t pair_capacity, void* workspace, size_t workspace_bytes, void* step_store, size_t step_store_bytes_given, int32_t store_steps,
+    dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    dgmr_status st = check_scene(scene, camera, -1);
+    if (st != DGMR_OK)
+        return st;
+    if (!cache_ok(cache, pair_capacity > 0, scene->n_gaussians) || !workspace || pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    if (options && options->render_mode != DGMR_RENDER_FULL && options->render_mode != DGMR_RENDER_BINS && options->render_mode != DGMR_RENDER_DEPTH)
+        return DGMR_ERR_BAD_ARG;
+    if (store_steps < 0 || (store_steps > 0 && !step_store))
+        return DGMR_ERR_BAD_ARG;
+    if (store_steps > 0 && step_store_bytes_given < dgmr_vm_step_store_size(camera->width, camera->height, store_steps, scene->dtype))
+        return DGMR_ERR_WORKSPACE;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (scene->dtype == DGMR_F64)
+        return vm_render<double>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s, options, step_store, uint32_t(store_steps));
+    return vm_render<float>(scene, camera, cache, pair_capacity, workspace, workspace_bytes, stats, s, options, step_store, uint32_t(store_steps));
+}
+
+dgmr_status dgmr_vm_backward_stored(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* cache, const void* grad_framebuffer,
+    void* grad_sh, void* grad_weights, void* grad_centroids, void* grad_scales, void* grad_rotations, void* workspace, size_t workspace_bytes,
+    const void* step_store, size_t step_store_bytes_given, int32_t store_steps, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    if (!scene || !camera || store_steps < 0 || (store_steps > 0 && !step_store))
+        return DGMR_ERR_BAD_ARG;
+    if (store_steps > 0 && step_store_bytes_given < dgmr_vm_step_store_size(camera->width, camera->height, store_steps, scene->dtype))
+        return DGMR_ERR_WORKSPACE;
+    dgmr_status st = check_scene(scene, camera, -1);
+    if (st != DGMR_OK)
+        return st;
+    const bool grads_ok = scene->n_gaussians == 0 || (grad_sh && grad_weights && grad_centroids && grad_scales && grad_rotations);
+    if (!cache_ok(cache, false, scene->n_gaussians) || !workspace || !grad_framebuffer || !grads_ok)
+        return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (scene->dtype == DGMR_F64)
+        return vm_backward<double>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
+            workspace_bytes, stats, s, step_store, uint32_t(store_steps));
+    return vm_backward<float>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
+        workspace_bytes, stats, s, step_store, uint32_t(store_steps));
 }
 
 dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections)

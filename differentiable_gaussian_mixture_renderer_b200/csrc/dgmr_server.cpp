@@ -381,12 +381,16 @@ void reap(dgmr_server* s)
             // more pairs than the learnt capacities: grow them, render the batch again
             ++s->st.rerenders;
             const double grow = double(pairs) / double(std::max<int64_t>(sl.capacity, 1));
+            std::vector<Key> grown; // each key of the batch grows once, however many of its requests the batch holds
             for (Request& q2 : sl.batch) {
                 const Key k = key_of(q2.r);
-                s->capacity[k] = int64_t(std::ceil(double(s->capacity[k]) * std::max(s->cfg.capacity_margin, grow)));
+                q2.rerendered = 1;
+                if (std::find(grown.begin(), grown.end(), k) != grown.end())
+                    continue;
+                grown.push_back(k);
+                s->capacity[k] = std::min<int64_t>(int64_t(std::ceil(double(s->capacity[k]) * std::max(s->cfg.capacity_margin, grow))), 0x7fffffff);
                 for (int g = 0; g < 2; ++g)
                     s->unit_cost.erase(std::make_tuple(q2.r.scene, q2.r.camera.width, q2.r.camera.height, q2.r.kind, int32_t(g)));
-                q2.rerendered = 1;
             }
             sl.capacity = int64_t(pairs) + 1024;
             const dgmr_status st = launch(s, sl);
@@ -426,7 +430,7 @@ void dispatch(dgmr_server* s)
                 err = learn_capacity(s, q.r, &kc);
             if (err != DGMR_OK)
                 break;
-            if (s->in_use + bytes + c > s->budget)
+            if (s->in_use + bytes + c > s->budget || cap + kc > int64_t(0x7fffffff))
                 break;
             bytes += c;
             cap += kc;

@@ -511,12 +511,16 @@ class ContinuousServer:
             # exact count, asynchronously -- the slot stays busy and completes on a later poll
             self.rerenders += 1
             grow = n_pairs / max(slot.capacity, 1)
+            grown = set()  # each key grows once, however many of its requests the batch holds
             for req in slot.batch:
+                req.rerendered = True
                 key = (req.scene_id, req.camera.width, req.camera.height)
-                self.capacity[key] = int(math.ceil(self.capacity[key] * max(self.margin, grow)))
+                if key in grown:
+                    continue
+                grown.add(key)
+                self.capacity[key] = min(int(math.ceil(self.capacity[key] * max(self.margin, grow))), 0x7fffffff)
                 self._unit_cost.pop((*key, False), None)
                 self._unit_cost.pop((*key, True), None)
-                req.rerendered = True
             self._launch(slot, slot.batch, n_pairs + 1024)
             return
         self.log.append((len(slot.batch), slot.capacity, n_pairs, now - slot.batch[0].t_launch,

@@ -14,7 +14,26 @@ from __future__ import annotations
 
 import torch
 
+from . import _native as N
 from . import cpp_binding
+
+# The backward recomputes each ray's section sets and sample positions (as the
+# reference does) only when memory is tight: a frame whose step store -- the
+# first STORE_STEPS large steps of every ray -- takes at most
+# STORE_MEMORY_FRACTION of the free device memory keeps them from the forward
+# instead (same results, a shorter backward).  STORE_STEPS = 0 always recomputes.
+STORE_STEPS = 4
+STORE_MEMORY_FRACTION = 0.25
+
+
+def _step_store(width: int, height: int, dtype, device):
+    if STORE_STEPS <= 0:
+        return None
+    nbytes = N.lib().dgmr_vm_step_store_size(int(width), int(height), STORE_STEPS, N.dtype_code(dtype))
+    free, _ = torch.cuda.mem_get_info(device)
+    if nbytes == 0 or nbytes > free * STORE_MEMORY_FRACTION:
+        return None
+    return cpp_binding.make_step_store(width, height, STORE_STEPS, dtype, device)
 
 
 class VolMarcher(torch.autograd.Function):
@@ -22,9 +41,12 @@ class VolMarcher(torch.autograd.Function):
     def forward(ctx, shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
                 camera_center, bg_color, image_width: int, image_height: int, tanfovx: float, tanfovy: float,
                 active_sh_degree: int, formulation: str | None = None):
+        store = _step_store(image_width, image_height, means3D.dtype, means3D.device) \
+            if any(ctx.needs_input_grad[:5]) else None
         cache = cpp_binding.forward(shs, opacity, means3D, scales, rotations, world_view_transform,
                                     full_proj_transform, camera_center, bg_color, image_width, image_height, tanfovx,
-                                    tanfovy, active_sh_degree, formulation=formulation)
+                                    tanfovy, active_sh_degree, formulation=formulation, step_store=store)
+        ctx.step_store = store
         ctx.save_for_backward(shs, opacity, means3D, scales, rotations, world_view_transform, full_proj_transform,
                               camera_center, bg_color, *cache)
         ctx.frame = (int(image_width), int(image_height), float(tanfovx), float(tanfovy), int(active_sh_degree))
@@ -41,7 +63,8 @@ class VolMarcher(torch.autograd.Function):
         W, H, tfx, tfy, deg = ctx.frame
         g_sh, g_w, g_mu, g_s, g_q = cpp_binding.backward(shs, opacity, means3D, scales, rotations, view, proj, campos,
                                                          bg, W, H, tfx, tfy, deg, grad_output, cache,
-                                                         formulation=ctx.formulation)
+                                                         formulation=ctx.formulation, step_store=ctx.step_store)
+        ctx.step_store = None
         if opacity.dim() == 1:
             g_w = g_w.reshape(-1)
         return g_sh, g_w, g_mu, g_s, g_q, None, None, None, None, None, None, None, None, None, None

@@ -311,6 +311,23 @@ dgmr_status dgmr_vm_backward(const dgmr_scene* scene, const dgmr_camera* camera,
     void* grad_weights, void* grad_centroids, void* grad_scales, void* grad_rotations, void* workspace, size_t workspace_bytes, dgmr_frame_stats* stats,
     dgmr_stream stream);
 
+/* Sample-step store -- no reference counterpart.  The reference's backward
+ * recomputes every ray's section set and its 128 sample positions per large
+ * step (vol_marcher_backward.cu:172-230) before the bin adjoints.  When the
+ * memory is there, the forward can keep them instead: for the first
+ * store_steps large steps of each ray, its sample borders and its section
+ * count; the backward given the same store reads them and recomputes only
+ * steps beyond store_steps.  Results are the same bits as without a store.
+ * Bytes of a store: dgmr_vm_step_store_size (W*H rays x store_steps x
+ * (128 borders + a count)). */
+size_t dgmr_vm_step_store_size(int32_t width, int32_t height, int32_t store_steps, int32_t dtype);
+dgmr_status dgmr_vm_forward_render_stored(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_render_options* options,
+    dgmr_vm_cache* cache, int64_t pair_capacity, void* workspace, size_t workspace_bytes, void* step_store, size_t step_store_bytes,
+    int32_t store_steps, dgmr_frame_stats* stats, dgmr_stream stream);
+dgmr_status dgmr_vm_backward_stored(const dgmr_scene* scene, const dgmr_camera* camera, const dgmr_vm_cache* cache, const void* grad_framebuffer,
+    void* grad_sh, void* grad_weights, void* grad_centroids, void* grad_scales, void* grad_rotations, void* workspace, size_t workspace_bytes,
+    const void* step_store, size_t step_store_bytes, int32_t store_steps, dgmr_frame_stats* stats, dgmr_stream stream);
+
 /* Gradient-check mode of the marcher (the reference's compile-time
  * DGMR_TORCH_GRAD_CHECK_CONST_SAMPLES, vol_marcher_forward.cu:343-350): with
  * n_sections > 0 every large step uses these fixed (start, end, delta_t)

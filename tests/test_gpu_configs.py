@@ -123,3 +123,52 @@ def test_vol_marcher_tile_lists_beyond_ray_masks(cuda):
     ref = check_vm(sc, cam, cuda, G)
     r = ref["i_ranges"].reshape(-1, 2)
     assert int((r[:, 1] - r[:, 0]).max()) > 4096
+
+
+@pytest.mark.parametrize("steps", [4, 1])
+def test_c2_step_store_gives_the_recomputed_results(cuda, steps):
+    """The forward keeps the first `steps` large steps' samples of every ray and
+    the backward reads them (steps beyond are recomputed): the image is the
+    same bits and the gradients equal the recomputing backward's up to the
+    order of the double-precision totals."""
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    sc = S.make_scene(100_000, seed=0)
+    cam = S.random_cameras(1, 512, 512, seed=1)[0]
+    G = torch.tensor(np.random.default_rng(2).normal(size=(3, 512, 512)).astype(np.float32), device=cuda)
+    shs, w, mu, s, q = to_dev(sc, cuda)
+    view, proj, campos, bgt = cam_tensors(cam, cuda)
+    args = (shs, w, mu, s, q, view, proj, campos, bgt, 512, 512, cam.tan_fovx, cam.tan_fovy, 0)
+    plain = cpp_binding.forward(*args)
+    g_plain = cpp_binding.backward(*args, G, plain)
+    store = cpp_binding.make_step_store(512, 512, steps, device=cuda)
+    kept = cpp_binding.forward(*args, step_store=store)
+    g_kept = cpp_binding.backward(*args, G, kept, step_store=store)
+    torch.cuda.synchronize()
+    assert torch.equal(plain[0], kept[0]) and torch.equal(plain[12], kept[12])
+    for name, a, b in zip(GRAD_NAMES, g_kept, g_plain):
+        err = float((a - b).abs().max()) / (float(b.abs().max()) + 1e-30)
+        assert err <= 1e-5, (name, err)
+
+
+def test_vol_marcher_apply_keeps_steps_when_memory_allows(cuda):
+    """vol_marcher.apply stores the sample steps (memory is plentiful here) and
+    gives the gradients of the recomputing path."""
+    from differentiable_gaussian_mixture_renderer_b200 import vol_marcher
+    sc = S.make_scene(20_000, seed=3, sh_degree=1)
+    cam = S.make_camera(128, 96, eye=(0.3, -0.2, -3.0))
+    G = torch.tensor(np.random.default_rng(4).normal(size=(3, 96, 128)).astype(np.float32), device=cuda)
+    view, proj, campos, bgt = cam_tensors(cam, cuda)
+    grads = []
+    for steps in (vol_marcher.STORE_STEPS, 0):
+        saved = vol_marcher.STORE_STEPS
+        vol_marcher.STORE_STEPS = steps
+        try:
+            ins = [t.clone().requires_grad_(True) for t in to_dev(sc, cuda)]
+            img = vol_marcher.apply(*ins, view, proj, campos, bgt, 128, 96, cam.tan_fovx, cam.tan_fovy, 1)
+            (img * G).sum().backward()
+            grads.append([t.grad for t in ins])
+        finally:
+            vol_marcher.STORE_STEPS = saved
+    for name, a, b in zip(GRAD_NAMES, *grads):
+        err = float((a - b).abs().max()) / (float(b.abs().max()) + 1e-30)
+        assert err <= 1e-5, (name, err)

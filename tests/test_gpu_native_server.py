@@ -127,3 +127,19 @@ def test_native_server_rerenders_overflowed_batches(cuda):
     assert server.stats()["rerenders"] > 0 and any(r.rerendered for r in reqs)
     _check_all(scenes, reqs)
     server.close()
+
+
+def test_native_server_capacity_grows_once_per_overflow(cuda):
+    """A batch of many requests of one (scene, resolution) that overflows grows
+    that key's capacity once, not once per request: memory held stays of the
+    order of the frames' real needs."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene, NativeServer, ServeRequest
+    scenes = {"big": GaussianScene.from_numpy(S.make_scene(20000, seed=12), cuda)}
+    server = NativeServer(scenes, cuda, n_slots=2, max_batch=8, capacity_margin=0.25)
+    reqs = [server.submit(ServeRequest("big", S.random_cameras(1, 256, 256, seed=900 + k)[0])) for k in range(32)]
+    server.drain()
+    st = server.stats()
+    assert st["rerenders"] > 0
+    assert st["hbm_peak_bytes"] < (1 << 30), st
+    _check_all(scenes, reqs)
+    server.close()

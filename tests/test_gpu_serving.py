@@ -127,8 +127,8 @@ def test_render_server_results_are_not_reused(cuda, to_host):
     server.drain()
     for k, req in enumerate(reqs):
         fb = _render_alone(scenes[req.scene_id], req.camera)
+        assert req.image.is_pinned() if to_host else req.image.is_cuda
         img = req.image.to(cuda) if to_host else req.image
-        assert img.is_pinned() if to_host else img.is_cuda
         assert torch.equal(img, fb), f"request {k}: image was overwritten by a later request"
     held = {r.image.data_ptr() for r in reqs}  # eight distinct result buffers
     assert len(held) == 8
