@@ -62,9 +62,10 @@ def parse():
                     help="--workload serving: the Python ContinuousServer instead of the C++ server")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the short vol_marcher (100k, 512x512) and serving (8 scenes) runs of the headline line")
-    ap.add_argument("--workload", choices=["served", "batched", "marcher", "serving", "configs"], default="served",
+    ap.add_argument("--workload", choices=["served", "batched", "marcher", "raster", "serving", "configs"], default="served",
                     help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
                          "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512; "
+                         "raster: vol_raster forward, 100k, 512x512; "
                          "serving: 8 scenes, Poisson 200 req/s, mixed resolutions, 20%% gradient requests; "
                          "configs: per-call GPU and oracle timings of the parity configurations")
     return ap.parse_args()
@@ -329,7 +330,10 @@ def run_ours(args):
     # from the first submission to the last completion, images to pinned host memory)
     native = None
     if not args.no_extras:
-        nserver = serving.NativeServer({"scene": scene}, dev, n_slots=args.slots, max_batch=args.batch)
+        # at this frame size views gain nothing from sharing a launch sequence: one view per batch,
+        # args.slots batches in flight (smaller requests would still be batched)
+        nserver = serving.NativeServer({"scene": scene}, dev, n_slots=args.slots, max_batch=args.batch,
+                                       max_batch_pixels=args.width * args.height)
         hosts = [torch.empty((3, args.height, args.width), dtype=torch.float32, pin_memory=True)
                  for _ in range(2 * args.batch)]
         fbs = [torch.empty((3, args.height, args.width), dtype=torch.float32, device=dev) for _ in range(2 * args.batch)]
@@ -368,9 +372,9 @@ def run_ours(args):
         native = {"value": nv, "e2e": ne, "unit": UNIT, "mean_batch": nbatch, "launch_to_done_ms_p50": pct(nlat, 50),
                   "launch_to_done_ms_p99": pct(nlat, 99), "e2e_launch_to_done_ms_p50": pct(nlat_e, 50),
                   "rerenders": st["rerenders"],
-                  "note": "the C++ continuous-batching server (dgmr_server_*, batches of up to requests_per_step "
-                          "views), host clock over the same number of requests; e2e with each image copied to "
-                          "pinned host memory"}
+                  "note": "the C++ continuous-batching server (dgmr_server_*, batches capped at one frame's pixels, "
+                          "slots_in_flight batches in flight), host clock over the same number of requests; e2e with "
+                          "each image copied to pinned host memory"}
 
     # ---------------------------------------------------------------- plain per-call leg
     # one request at a time on one stream, the reference's pattern: preprocess, the pair count
@@ -444,6 +448,7 @@ def run_ours(args):
         del fb, frame, ctx, fb_plain, host_plain
         server.release_buffers()
         extras["vol_marcher_c2"] = measure_marcher(dev, n_cams=3)
+        extras["vol_raster_c2_scene"] = measure_vol_raster(dev, n_cams=3)
         extras["batched_c3"] = measure_batched(dev, steps=3, warmup=2)
         extras["serving_c4"] = measure_serving(dev, n_req=200, warmup=1)
 
@@ -662,6 +667,44 @@ def measure_marcher(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int
                                    "1965 MHz maximum clock; FP32 instructions per fill from "
                                    f"profiles/{MARCHER_PROFILE}"}
     return out
+
+
+def measure_vol_raster(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int = 512):
+    """vol_raster forward (the volume rasteriser, forward only) through
+    vol_raster.forward at the c2 scene: 100k Gaussians, 512x512, one warm-up
+    camera then ``n_cams`` timed ones (CUDA events around the call)."""
+    import torch
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200 import vol_raster
+    sc = S.make_scene(n, seed=0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
+    ins = (t(sc.sh), t(sc.weights), t(sc.centroids), t(sc.scales), t(sc.rotations))
+    cams = S.random_cameras(n_cams + 1, W, H, seed=1)
+    ms = []
+    for k, cam in enumerate(cams):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        vol_raster.forward(*ins, t(cam.view), t(cam.proj), t(cam.campos), torch.zeros(3, device=dev), W, H,
+                           cam.tan_fovx, cam.tan_fovy, 0)
+        e1.record()
+        e1.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    return {"forward_ms": statistics.median(ms), "mpix_per_s": W * H / 1e6 / (statistics.median(ms) * 1e-3),
+            "workload": f"vol_raster forward, {n} Gaussians (config-0 distribution), {W}x{H}, random cameras r=2.5-4"}
+
+
+def run_raster(args):
+    """The vol_raster workload (measure_vol_raster) as its own JSON line."""
+    torch, dev, local = _gpu_common()
+    with ClockSampler(local) as clk:
+        r = measure_vol_raster(dev, n_cams=max(args.steps, 1))
+    line = {"metric": "vol_raster forward ms/frame, 100k Gaussians, 512x512", "value": r["forward_ms"], "unit": "ms",
+            "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": r["forward_ms"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": r.pop("workload")}, **r, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_marcher(args):
@@ -962,6 +1005,8 @@ def main():
         return run_batched(args)
     if args.workload == "marcher":
         return run_marcher(args)
+    if args.workload == "raster":
+        return run_raster(args)
     if args.workload == "serving":
         return run_serving(args)
     if args.workload == "configs":

@@ -91,7 +91,7 @@ SERVE_SPLAT, SERVE_MARCH = 0, 1
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("n_slots", C.c_int32), ("max_views", C.c_int32), ("reserved", C.c_int32),
-                ("hbm_budget_bytes", C.c_size_t), ("capacity_margin", C.c_double)]
+                ("hbm_budget_bytes", C.c_size_t), ("capacity_margin", C.c_double), ("max_batch_pixels", C.c_int64)]
 
 
 class ServerRequest(C.Structure):

@@ -6,7 +6,8 @@
 // (B) every Gaussian of the tile adds its CDF mass and its border values to
 // the bins; (blend) each bin is fitted with the four-channel piecewise-linear
 // model (create_approximation) and integrated with 256 midpoint steps.  The
-// binning (tile | depth order) is the splat renderer's.
+// binning (tile | depth order) is the splat renderer's; the render runs one
+// warp per pixel, a lane per bin (dgmr_raster_warp.cuh).
 #include <cstdint>
 #include <cstring>
 #include <cuda_runtime.h>
@@ -23,7 +24,6 @@ constexpr unsigned kVrStepsPerBin = 256; // vol_raster_forward.h:62
 constexpr float kVrTransmission = 0.005f; // vol_raster_forward.h:63
 constexpr float kVrRelevanceSigma = 3.f; // vol_raster_forward.h:64
 constexpr float kVrFilterSD = 0.55f; // vol_raster_forward.h:60
-constexpr unsigned kVrThreads = 256; // one 16x16 tile per block
 
 // Frame workspace: per-Gaussian preprocess, tile ranges and binning scratch;
 // pair workspace: the (tile, Gaussian) pairs and sort scratch.
@@ -200,197 +200,10 @@ __device__ __forceinline__ V3<float> vr_pixel_dir(const CameraT<float>& cam, uns
     return mul3(d, il);
 }
 
-struct VrShared {
-    uint32_t id[kVrThreads];
-    float mu[3][kVrThreads];
-    float Q[6][kVrThreads];
-    float mass[kVrThreads];
-};
-
-__device__ __forceinline__ void vr_load_batch(VrShared& sh, const VrRender& a, int32_t k, int32_t e)
-{
-    if (k < e) {
-        uint32_t id = a.list[k];
-        if (id >= a.N) {
-            flag_bounds(a.stats, 0x41u);
-            id = 0;
-        }
-        sh.id[threadIdx.x] = id;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            sh.mu[c][threadIdx.x] = a.centroids[3 * size_t(id) + c];
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-            sh.Q[c][threadIdx.x] = a.inv_cov[6 * size_t(id) + c];
-        sh.mass[threadIdx.x] = a.masses[id];
-    }
-}
-
-__device__ __forceinline__ Gauss1d<float> vr_intersect(const VrShared& sh, int j, V3<float> o, V3<float> d)
-{
-    const V3<float> mu = { sh.mu[0][j], sh.mu[1][j], sh.mu[2][j] };
-    const S3<float> Q = { { sh.Q[0][j], sh.Q[1][j], sh.Q[2][j], sh.Q[3][j], sh.Q[4][j], sh.Q[5][j] } };
-    return intersect_with_ray_inv_C(mu, Q, o, d);
-}
-
-// vol_raster_forward.cu:253-517
-__global__ void __launch_bounds__(kVrThreads) k_vr_render(VrRender a, CameraT<float> cam)
-{
-    __shared__ VrShared sh;
-    const unsigned tile = blockIdx.x;
-    const unsigned tx = tile % cam.gx, ty = tile / cam.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
-    const bool inside = px < cam.W && py < cam.H;
-    const V3<float> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
-    const V3<float> d = vr_pixel_dir(cam, px, py);
-    int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
-    if (b < 0 || e < b || uint32_t(e) > a.cap) {
-        if (threadIdx.x == 0)
-            flag_bounds(a.stats, 0x42u);
-        b = e = 0;
-    }
-    // pass A: bin sizes, until the ray's mass is used up
-    RasterBinSizer<kVrBins> sizer;
-    sizer.init(kVrRelevanceSigma, kVrTransmission);
-    bool done = !inside;
-    for (int32_t base = b; base < e; base += int32_t(kVrThreads)) {
-        if (__syncthreads_count(done) == int(kVrThreads))
-            break;
-        vr_load_batch(sh, a, base + int32_t(threadIdx.x), e);
-        __syncthreads();
-        if (done)
-            continue;
-        const int n = min(int(kVrThreads), e - base);
-        for (int j = 0; j < n; ++j) {
-            const Gauss1d<float> g = vr_intersect(sh, j, o, d);
-            const float mor = g.weight * sh.mass[j];
-            if (mor < 0.001f || mor > 1000.f)
-                continue;
-            if (g.C + 0.f <= 0.f)
-                continue;
-            sizer.add_gaussian(mor, g.centre, dgmr_fm::sqrt_f(g.C + 0.f));
-            if (sizer.is_full()) {
-                done = true;
-                break;
-            }
-        }
-    }
-    __syncthreads();
-    sizer.finalise();
-    float res[3] = { 0.f, 0.f, 0.f };
-    float transparency = 1.f; // of the final colour: 1 in Full and Bins mode, 0 in Depth mode
-    if (a.mode == DGMR_RENDER_FULL) {
-        // pass B: bin masses and border values of every Gaussian of the tile
-        float bin_mass[kVrBins][4];
-        float bin_eval[kVrBins + 1][4];
-        for (unsigned q = 0; q < kVrBins; ++q)
-            for (int c = 0; c < 4; ++c)
-                bin_mass[q][c] = 0.f;
-        for (unsigned q = 0; q <= kVrBins; ++q)
-            for (int c = 0; c < 4; ++c)
-                bin_eval[q][c] = 0.f;
-        const float max_distance = sizer.end_of(kVrBins - 1);
-        done = !inside;
-        for (int32_t base = b; base < e; base += int32_t(kVrThreads)) {
-            if (__syncthreads_count(done) == int(kVrThreads))
-                break;
-            vr_load_batch(sh, a, base + int32_t(threadIdx.x), e);
-            __syncthreads();
-            if (done)
-                continue;
-            const int n = min(int(kVrThreads), e - base);
-            for (int j = 0; j < n; ++j) {
-                const Gauss1d<float> g = vr_intersect(sh, j, o, d);
-                const float centre = g.centre;
-                const float variance = g.C + 0.f;
-                const float sd = dgmr_fm::sqrt_f(variance);
-                const float inv_sd = 1.f / sd;
-                const float weight = g.weight * sh.mass[j];
-                if (variance <= 0.f || dgmr_fm::isnan_f(variance) || dgmr_fm::isnan_f(weight) || weight > 100000.f)
-                    continue;
-                if (weight * (cdf_inv_SD_inline(centre, inv_sd, max_distance) - cdf_inv_SD_inline(centre, inv_sd, 0.f)) <= 0.001f)
-                    continue;
-                const uint32_t id = sh.id[j];
-                const V3<float> rgb = { a.rgb[3 * size_t(id)], a.rgb[3 * size_t(id) + 1], a.rgb[3 * size_t(id) + 2] };
-                float cdf_start = cdf_inv_SD_inline(centre, inv_sd, 0.f);
-                for (unsigned q = 0; q < kVrBins; ++q) {
-                    const float cdf_end = cdf_inv_SD_inline(centre, inv_sd, sizer.end_of(q));
-                    const float mass = (cdf_end - cdf_start) * weight;
-                    cdf_start = cdf_end;
-                    if (mass < 0.0001f)
-                        continue;
-                    bin_mass[q][0] = bin_mass[q][0] + rgb.x * mass;
-                    bin_mass[q][1] = bin_mass[q][1] + rgb.y * mass;
-                    bin_mass[q][2] = bin_mass[q][2] + rgb.z * mass;
-                    bin_mass[q][3] = bin_mass[q][3] + mass;
-                    const float ev = weight * eval_exponential_1d(centre, variance, sizer.begin_of(q));
-                    bin_eval[q][0] = bin_eval[q][0] + rgb.x * ev;
-                    bin_eval[q][1] = bin_eval[q][1] + rgb.y * ev;
-                    bin_eval[q][2] = bin_eval[q][2] + rgb.z * ev;
-                    bin_eval[q][3] = bin_eval[q][3] + ev;
-                }
-                const float ev = weight * eval_exponential_1d(centre, variance, max_distance);
-                bin_eval[kVrBins][0] = bin_eval[kVrBins][0] + rgb.x * ev;
-                bin_eval[kVrBins][1] = bin_eval[kVrBins][1] + rgb.y * ev;
-                bin_eval[kVrBins][2] = bin_eval[kVrBins][2] + rgb.z * ev;
-                bin_eval[kVrBins][3] = bin_eval[kVrBins][3] + ev;
-            }
-        }
-        // blend: the split of a bin's mass between its halves evaluates to 0.5 for
-        // every bin and channel (vol_raster_forward.cu:473)
-        const float half[4] = { 0.5f, 0.5f, 0.5f, 0.5f };
-        float cur = 1.f;
-        for (unsigned q = 0; q < kVrBins; ++q) {
-            const float t_right = sizer.end_of(q) - sizer.begin_of(q);
-            if (t_right <= 0.f)
-                continue;
-            const FunctionGroup<float> f = create_approximation(half, bin_mass[q], bin_eval[q], bin_eval[q + 1], t_right);
-            const float dt = f.t_right / float(kVrStepsPerBin);
-            float t = dt / 2.f;
-            for (unsigned s = 0; s < kVrStepsPerBin; ++s) {
-                const float e0 = f.sample(0, t), e1 = f.sample(1, t), e2 = f.sample(2, t), e3 = f.sample(3, t);
-                res[0] = res[0] + (e0 * cur) * dt;
-                res[1] = res[1] + (e1 * cur) * dt;
-                res[2] = res[2] + (e2 * cur) * dt;
-                cur = cur * max_f(0.f, 1.f - e3 * dt);
-                t = t + dt;
-            }
-        }
-    } else if (a.mode == DGMR_RENDER_DEPTH) {
-        // vol_raster_forward.cu:495-507
-        const unsigned bin = min(unsigned(a.debug_bin), kVrBins - 1);
-        const float distance = sizer.end_of(bin);
-        float c0 = distance / a.max_depth, c1 = c0, c2 = c0;
-        if (distance == 0.f) {
-            c0 = 0.f;
-            c1 = 1.f;
-            c2 = 0.f;
-        }
-        if (dgmr_fm::isnan_f(distance)) {
-            c0 = 1.f;
-            c1 = 0.f;
-            c2 = 0.5f;
-        }
-        if (distance < 0.f) {
-            c0 = 1.f;
-            c1 = 0.5f;
-            c2 = 0.f;
-        }
-        res[0] = c0;
-        res[1] = c1;
-        res[2] = c2;
-        transparency = 0.f;
-    }
-    if (!inside)
-        return;
-    const size_t pix = size_t(py) * cam.W + px;
-    const size_t plane = size_t(cam.W) * cam.H;
-    a.fb[pix] = res[0] + transparency * cam.bg[0];
-    a.fb[plane + pix] = res[1] + transparency * cam.bg[1];
-    a.fb[2 * plane + pix] = res[2] + transparency * cam.bg[2];
-}
 
 } // namespace dgmr
+
+#include "dgmr_raster_warp.cuh"
 
 using namespace dgmr;
 
@@ -472,7 +285,7 @@ dgmr_status dgmr_vr_forward(const dgmr_scene* scene, const dgmr_camera* camera, 
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
     VrRender a { L.ranges, L.bin.pair_val[par], static_cast<const float*>(scene->centroids), L.inv_cov, L.masses, L.rgb, framebuffer, N, cap, st_dev, mode,
         options ? options->debug_bin : -1, options ? float(options->max_depth) : 20.f };
-    k_vr_render<<<cam.gx * cam.gy, kVrThreads, 0, s>>>(a, cam);
+    k_vr_render_warp<<<cam.gx * cam.gy * (kTilePixels / kVrRayWarps), kVrRayWarps * 32, 0, s>>>(a, cam);
     note_launch();
     return launch_status();
 }

@@ -411,14 +411,17 @@ void dispatch(dgmr_server* s)
             continue;
         std::vector<Request> batch;
         size_t bytes = 0;
-        int64_t cap = 0;
+        int64_t cap = 0, pixels = 0;
         int entries = 0;
         std::vector<int32_t> render_scenes;
         dgmr_status err = DGMR_OK;
         while (!s->queue.empty()) {
             const Request& q = s->queue.front();
             const bool march = is_march(q.r);
-            if (!batch.empty() && (march || is_march(batch.front().r) || int32_t(batch.size()) >= s->cfg.max_views))
+            const int64_t px = int64_t(q.r.camera.width) * int64_t(q.r.camera.height);
+            if (!batch.empty()
+                && (march || is_march(batch.front().r) || int32_t(batch.size()) >= s->cfg.max_views
+                    || (s->cfg.max_batch_pixels > 0 && pixels + px > s->cfg.max_batch_pixels)))
                 break;
             const bool new_entry = wants_grad(q.r) || std::find(render_scenes.begin(), render_scenes.end(), q.r.scene) == render_scenes.end();
             if (!march && new_entry && entries + 1 > DGMR_BATCH_MAX_SCENES)
@@ -434,6 +437,7 @@ void dispatch(dgmr_server* s)
                 break;
             bytes += c;
             cap += kc;
+            pixels += px;
             if (new_entry)
                 ++entries;
             if (!wants_grad(q.r))

@@ -583,11 +583,11 @@ class NativeServer:
     completed request's results equal the plain call's."""
 
     def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
-                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3):
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3, max_batch_pixels: int = 0):
         self.device = torch.device(device or "cuda")
         self.lib = N.lib()
         cfg = N.ServerConfig(self.device.index if self.device.index is not None else torch.cuda.current_device(),
-                             n_slots, max_batch, 0, int(hbm_budget_bytes or 0), capacity_margin)
+                             n_slots, max_batch, 0, int(hbm_budget_bytes or 0), capacity_margin, int(max_batch_pixels))
         handle = C.c_void_p()
         N.check(self.lib.dgmr_server_create(C.byref(cfg), C.byref(handle)), "server create")
         self._h = handle

@@ -431,3 +431,148 @@ extern "C" long kat_section_overflows(unsigned seed, int trials)
     }
     return bad;
 }
+
+// The volume rasteriser's warp-parallel bin sizer (csrc/dgmr_raster_warp.cuh),
+// its lanes emulated as arrays: the insertion position from the "not greater"
+// ballot (highest set lane + 1), the shift, the left-to-right transmittance
+// product, the lane-parallel merge costs and the first-of-equals minimum --
+// against RasterBinSizer<32> on random add sequences; counts sequences whose
+// saturation flags or final borders differ in any bit.
+namespace {
+
+struct WarpSizerEmu {
+    float mass[32], border[32], sd[32];
+    float total = 0.f, far = 0.f, full_mass = 0.f;
+
+    void init(float transmission_threshold)
+    {
+        for (int i = 0; i < 32; ++i) {
+            mass[i] = 0.f;
+            border[i] = 1.f / 0.f;
+            sd[i] = 0.f;
+        }
+        full_mass = -dgmr_fm::log_f(transmission_threshold);
+    }
+
+    void add(float m, float centre, float s, float sigma)
+    {
+        if (m < 0.0001f)
+            return;
+        const float reach = centre + s * sigma;
+        const float on_ray = m * (dgmr::RasterBinSizer<32>::cdf(centre, s, reach) - dgmr::RasterBinSizer<32>::cdf(centre, s, 0.f));
+        far = dgmr_fm::max_f(reach, far);
+        total = total + on_ray;
+        uint32_t not_greater = 0;
+        for (int l = 0; l < 31; ++l)
+            if (!(border[l] > centre))
+                not_greater |= 1u << l;
+        int p = 0;
+        for (int l = 31; l >= 0; --l)
+            if (not_greater >> l & 1u) {
+                p = l + 1;
+                break;
+            }
+        for (int l = 31; l > p; --l) {
+            mass[l] = mass[l - 1];
+            border[l] = border[l - 1];
+            sd[l] = sd[l - 1];
+        }
+        mass[p] = on_ray;
+        border[p] = centre;
+        sd[p] = s;
+        if (!(mass[31] > 0.f))
+            return;
+        float front[32];
+        float run = 1.f;
+        front[0] = 1.f;
+        for (int i = 0; i < 31; ++i) {
+            run = run * dgmr_fm::exp_f(-mass[i]);
+            front[i + 1] = run;
+        }
+        float key[31], mm[31], mc[31], msd[31];
+        for (int j = 0; j < 31; ++j) {
+            const float sa = front[j] * mass[j], sb = front[j + 1] * mass[j + 1];
+            const float pa = (sa + sb >= 0.0000001f) ? dgmr_fm::min_f(sa / (sa + sb), 0.999999f) : 0.5f;
+            const float pb = 1.f - pa;
+            const float c = pa * border[j] + pb * border[j + 1];
+            const float va = sd[j] * sd[j], vb = sd[j + 1] * sd[j + 1];
+            const float v = pa * (va + (border[j] - c) * (border[j] - c)) + pb * (vb + (border[j + 1] - c) * (border[j + 1] - c));
+            mm[j] = mass[j] + mass[j + 1];
+            mc[j] = c;
+            msd[j] = dgmr_fm::sqrt_f(v);
+            const auto kl = [](float c1, float sd1, float c2, float sd2) {
+                return ((c1 - c2) * (c1 - c2) + sd1 * sd1 - sd2 * sd2) / (2.f * sd2 * sd2) + dgmr_fm::log_f(sd2 / sd1);
+            };
+            const float cost = front[j + 1] * (kl(border[j], sd[j], c, msd[j]) + kl(border[j + 1], sd[j + 1], c, msd[j]));
+            key[j] = cost < 1.f / 0.f ? cost : 1.f / 0.f;
+        }
+        float lo = 1.f / 0.f;
+        for (int j = 0; j < 31; ++j)
+            lo = std::fmin(lo, key[j]);
+        if (!(lo < 1.f / 0.f))
+            return;
+        int pick = 0;
+        while (!(key[pick] == lo))
+            ++pick;
+        mass[pick] = mm[pick];
+        border[pick] = mc[pick];
+        sd[pick] = msd[pick];
+        for (int l = pick + 1; l < 31; ++l) {
+            mass[l] = mass[l + 1];
+            border[l] = border[l + 1];
+            sd[l] = sd[l + 1];
+        }
+    }
+
+    void finalise()
+    {
+        float prev = 0.f;
+        for (int i = 0; i < 32; ++i) {
+            float b = border[i];
+            const bool empty = b == 1.f / 0.f;
+            if (!empty)
+                b = dgmr_fm::max_f(b, prev + 0.00001f);
+            else
+                b = prev + (far - prev) / float(32 - i);
+            prev = b;
+            border[i] = b;
+            if (empty)
+                mass[i] = 0.f;
+        }
+    }
+};
+
+} // namespace
+
+extern "C" long kat_compare_warp_sizer(unsigned seed, int trials)
+{
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    long bad = 0;
+    for (int t = 0; t < trials; ++t) {
+        dgmr::RasterBinSizer<32> a;
+        WarpSizerEmu w;
+        a.init(3.f, 0.005f);
+        w.init(0.005f);
+        const int n = 1 + int(u(rng) * 90.f);
+        bool ok = true;
+        float prev_centre = 2.f;
+        for (int i = 0; i < n && ok; ++i) {
+            const float mass = u(rng) < 0.1f ? 0.00005f : 0.0002f + 0.6f * u(rng) * u(rng);
+            const float centre = u(rng) < 0.1f ? prev_centre : 2.f + 3.f * u(rng);
+            prev_centre = centre;
+            const float sd = 0.005f + 0.1f * u(rng);
+            a.add_gaussian(mass, centre, sd);
+            w.add(mass, centre, sd, 3.f);
+            ok = a.is_full() == (w.total >= w.full_mass);
+        }
+        a.finalise();
+        w.finalise();
+        for (unsigned i = 0; i < 32 && ok; ++i) {
+            const float e = i == 31 ? w.far : w.border[i];
+            ok = same_bits(a.end_of(i), e);
+        }
+        bad += ok ? 0 : 1;
+    }
+    return bad;
+}

@@ -143,3 +143,20 @@ def test_native_server_capacity_grows_once_per_overflow(cuda):
     assert st["hbm_peak_bytes"] < (1 << 30), st
     _check_all(scenes, reqs)
     server.close()
+
+
+def test_native_server_pixel_cap_keeps_large_views_apart(cuda):
+    """max_batch_pixels: a batch takes no further view once its pixels would
+    pass the cap (it always takes one); small views still share batches."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import NativeServer, ServeRequest
+    scenes = _scenes(cuda)
+    server = NativeServer(scenes, cuda, n_slots=1, max_batch=8, max_batch_pixels=128 * 96)
+    big = [ServeRequest("a", S.random_cameras(1, 128, 96, seed=800 + k)[0]) for k in range(4)]
+    small = [ServeRequest("b", S.random_cameras(1, 32, 24, seed=850 + k)[0]) for k in range(8)]
+    for r in big + small:
+        server.submit(r)
+    server.drain()
+    assert all(r.batch_size == 1 for r in big)
+    assert max(r.batch_size for r in small) > 1
+    _check_all(scenes, big + small)
+    server.close()

@@ -49,6 +49,8 @@ def shim():
     lib.kat_compare_sizers.restype = C.c_long
     lib.kat_compare_fits.argtypes = [C.c_uint, C.c_int]
     lib.kat_compare_fits.restype = C.c_long
+    lib.kat_compare_warp_sizer.argtypes = [C.c_uint, C.c_int]
+    lib.kat_compare_warp_sizer.restype = C.c_long
     return lib
 
 
@@ -317,6 +319,15 @@ def test_oracle_and_product_bin_sizers_agree(shim):
     """20k random add sequences (32 and 4 bins): saturation after every add
     and the final borders, bit for bit."""
     assert shim.kat_compare_sizers(7, 10000) == 0
+
+
+def test_warp_parallel_bin_sizer_matches_the_one_thread_sizer(shim):
+    """The volume rasteriser's warp form of the sizer (one slot per lane: the
+    insertion position from a ballot, merge costs priced lane-parallel, the
+    first of equal minimum costs), emulated lane by lane: 20k random add
+    sequences give the one-thread RasterBinSizer's saturation flags and final
+    borders bit for bit."""
+    assert shim.kat_compare_warp_sizer(5, 20000) == 0
 
 
 def test_oracle_and_product_bin_fits_agree(shim):
