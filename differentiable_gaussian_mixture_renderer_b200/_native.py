@@ -176,6 +176,7 @@ _SIGNATURES = {
     "dgmr_server_poll": (C.c_int32, [C.c_void_p, C.POINTER(ServerCompletion), C.c_int32]),
     "dgmr_server_wait": (C.c_int32, [C.c_void_p, C.POINTER(ServerCompletion), C.c_int32]),
     "dgmr_server_pending": (C.c_int64, [C.c_void_p]),
+    "dgmr_server_now": (C.c_double, [C.c_void_p]),
     "dgmr_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "dgmr_server_destroy": (C.c_int, [C.c_void_p]),
     "dgmr_status_string": (C.c_char_p, [C.c_int]),

@@ -308,6 +308,24 @@ dgmr_status launch(dgmr_server* s, Slot& sl)
         if (st == DGMR_OK && wants_grad(head))
             st = dgmr_vm_backward(&sc, &head.camera, &sl.vm, head.grad_image, head.grads.sh, head.grads.weights, head.grads.centroids,
                 head.grads.scales, head.grads.rotations, sl.frame_ws.p, sl.frame_ws.bytes, nullptr, ds);
+    } else if (sl.batch.size() == 1) {
+        // one view: the single-frame entry points (the same bits as the batched ones, a
+        // shorter launch sequence)
+        const dgmr_scene& sc = s->scenes[size_t(head.scene)];
+        const int n = sc.n_gaussians;
+        const size_t fb = dgmr_splat_frame_workspace_size(n, head.camera.width, head.camera.height);
+        const size_t pb = std::max<size_t>(1, dgmr_splat_pair_workspace_size(n, sl.capacity));
+        if (!fb)
+            return DGMR_ERR_BAD_ARG;
+        if (!sl.frame_ws.ensure(fb, &s->st.reallocs) || !sl.pair_ws.ensure(pb, &s->st.reallocs))
+            return DGMR_ERR_CUDA;
+        st = dgmr_splat_forward(&sc, &head.camera, head.framebuffer, sl.frame_ws.p, sl.frame_ws.bytes, sl.pair_ws.p, sl.pair_ws.bytes, sl.capacity,
+            sl.stats_dev, ds);
+        if (st == DGMR_OK)
+            cudaMemcpyAsync(sl.stats_host, sl.stats_dev, sizeof(dgmr_frame_stats), cudaMemcpyDeviceToHost, cs);
+        if (st == DGMR_OK && wants_grad(head))
+            st = dgmr_splat_backward(&sc, &head.camera, head.grad_image, head.grads.sh, head.grads.weights, head.grads.centroids, head.grads.scales,
+                head.grads.rotations, sl.frame_ws.p, sl.frame_ws.bytes, sl.pair_ws.p, sl.pair_ws.bytes, sl.capacity, ds);
     } else {
         splat_tables(s, sl);
         const int32_t nv = int32_t(sl.views.size()), ns = int32_t(sl.scenes.size());
@@ -519,7 +537,6 @@ dgmr_status dgmr_server_create(const dgmr_server_config* config, dgmr_server** o
         return DGMR_ERR_BAD_ARG;
     s->cfg = cfg;
     s->device = cfg.device;
-    s->t0 = now_s();
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         delete s;
@@ -543,9 +560,12 @@ dgmr_status dgmr_server_create(const dgmr_server_config* config, dgmr_server** o
         dgmr_server_destroy(s);
         return DGMR_ERR_CUDA;
     }
+    s->t0 = now_s(); // the completions' clock starts once the server exists
     *out = s;
     return DGMR_OK;
 }
+
+double dgmr_server_now(const dgmr_server* s) { return s ? now_s() - s->t0 : -1.0; }
 
 dgmr_status dgmr_server_add_scene(dgmr_server* s, const dgmr_scene* scene, int32_t* index)
 {

@@ -591,7 +591,8 @@ class NativeServer:
         handle = C.c_void_p()
         N.check(self.lib.dgmr_server_create(C.byref(cfg), C.byref(handle)), "server create")
         self._h = handle
-        self._t0 = time.perf_counter()
+        # completions carry the server's clock: align it with this process's perf_counter
+        self._t0 = time.perf_counter() - self.lib.dgmr_server_now(self._h)
         self.scenes = scenes
         self._index = {}
         self._c_scenes = {}

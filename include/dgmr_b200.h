@@ -408,6 +408,8 @@ int32_t dgmr_server_poll(dgmr_server* server, dgmr_server_completion* out, int32
 int32_t dgmr_server_wait(dgmr_server* server, dgmr_server_completion* out, int32_t max_out);
 /* Requests queued, in flight or completed and not yet returned. */
 int64_t dgmr_server_pending(const dgmr_server* server);
+/* The server's clock now (seconds since its creation), the clock of the completions' times. */
+double dgmr_server_now(const dgmr_server* server);
 dgmr_status dgmr_server_get_stats(const dgmr_server* server, dgmr_server_stats* out);
 /* Waits for work in flight, frees the server's memory. */
 dgmr_status dgmr_server_destroy(dgmr_server* server);

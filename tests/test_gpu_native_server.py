@@ -78,8 +78,10 @@ def test_native_server_results_equal_alone_and_in_the_mix(cuda, n_slots, max_bat
 
 def test_native_server_copies_to_pinned_host_images(cuda):
     from differentiable_gaussian_mixture_renderer_b200.serving import NativeServer, ServeRequest
+    import time
     scenes = _scenes(cuda)
     server = NativeServer(scenes, cuda, n_slots=2, max_batch=4)
+    t_before = time.perf_counter()
     reqs = []
     for k in range(6):
         w, h = RES[k % len(RES)]
@@ -87,8 +89,11 @@ def test_native_server_copies_to_pinned_host_images(cuda):
         r.host_image = torch.empty((3, h, w), dtype=torch.float32, pin_memory=True)
         reqs.append(server.submit(r))
     server.drain()
+    t_after = time.perf_counter()
     for r in reqs:
         assert torch.equal(r.host_image, r.image.cpu())
+        # completion times are on this process's clock: after submission, before drain returned
+        assert t_before - 1e-3 <= r.t_launch <= r.t_done <= t_after + 1e-3, (t_before, r.t_launch, r.t_done, t_after)
     _check_all(scenes, reqs)
     server.close()
 
