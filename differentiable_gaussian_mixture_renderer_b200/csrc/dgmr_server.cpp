@@ -586,7 +586,8 @@ dgmr_status dgmr_server_submit(dgmr_server* s, const dgmr_server_request* reques
     if (r.scene < 0 || size_t(r.scene) >= s->scenes.size() || !r.framebuffer || r.camera.width <= 0 || r.camera.height <= 0
         || (r.kind != DGMR_SERVE_SPLAT && r.kind != DGMR_SERVE_MARCH))
         return DGMR_ERR_BAD_ARG;
-    if (wants_grad(r)
+    // gradient outputs of a scene without Gaussians may have no address
+    if (wants_grad(r) && s->scenes[size_t(r.scene)].n_gaussians > 0
         && (!r.grads.sh || !r.grads.weights || !r.grads.centroids || !r.grads.scales || !r.grads.rotations))
         return DGMR_ERR_BAD_ARG;
     Request q;

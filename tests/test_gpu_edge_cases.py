@@ -120,3 +120,53 @@ def test_degenerate_gaussians_vol_raster(cuda):
     fb = vol_raster.forward(shs, w, mu, s, q, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx,
                             cam.tan_fovy, sc.sh_degree).cpu().numpy()
     assert np.isfinite(fb).all() and np.abs(fb - ref["fb"]).max() <= IMAGE_TOL
+
+
+def test_step_store_on_empty_and_degenerate_scenes(cuda):
+    """The marcher's step store on an empty scene (every ray ends at its first
+    step) and on the degenerate scene: the same image and gradients as the
+    recomputing backward."""
+    for sc in (S.make_scene(0, seed=1), degenerate_scene()):
+        cam = S.make_camera(40, 32, eye=(0.1, -0.1, -3.0))
+        ts = to_dev(sc, cuda)
+        view, proj, campos, bgt = cam_tensors(cam, cuda, bg=BG)
+        args = (*ts, view, proj, campos, bgt, cam.width, cam.height, cam.tan_fovx, cam.tan_fovy, sc.sh_degree)
+        G = torch.tensor(np.random.default_rng(6).normal(size=(3, 32, 40)).astype(np.float32), device=cuda)
+        plain = cpp_binding.forward(*args)
+        g_plain = cpp_binding.backward(*args, G, plain)
+        store = cpp_binding.make_step_store(cam.width, cam.height, 2, device=cuda)
+        kept = cpp_binding.forward(*args, step_store=store)
+        g_kept = cpp_binding.backward(*args, G, kept, step_store=store)
+        torch.cuda.synchronize()
+        assert torch.equal(plain[0], kept[0])
+        for name, a, b in zip(NAMES, g_kept, g_plain):
+            assert a.shape == b.shape
+            if b.numel():
+                err = float((a - b).abs().max()) / (float(b.abs().max()) + 1e-30)
+                assert err <= 1e-5, (name, err)
+
+
+def test_native_server_on_an_empty_and_a_culled_scene(cuda):
+    """Scenes with no Gaussian, or none in front of the camera: splat and
+    marcher requests, with gradients, complete with the background and the
+    plain calls' (zero) gradients."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene, NativeServer, ServeRequest
+    culled = S.make_scene(500, seed=11)
+    culled.centroids[:, 2] -= 10.0
+    scenes = {"empty": GaussianScene.from_numpy(S.make_scene(0, seed=1), cuda),
+              "culled": GaussianScene.from_numpy(culled, cuda)}
+    server = NativeServer(scenes, cuda, n_slots=2, max_batch=4)
+    cam = S.make_camera(48, 40)
+    reqs = []
+    for sid in ("empty", "culled"):
+        for kind in ("splat", "march"):
+            g = torch.ones((3, 40, 48), device=cuda)
+            reqs.append(server.submit(ServeRequest(sid, cam, backward=True, grad_image=g, kind=kind)))
+    server.drain()
+    want = torch.zeros((3, 40, 48), device=cuda)  # camera_struct's background is black
+    for r in reqs:
+        assert r.status == 0
+        assert torch.equal(r.image, want)
+        for g in r.grads:
+            assert g.numel() == 0 or float(g.abs().max()) == 0.0
+    server.close()
