@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--python-server", action="store_true",
                     help="--workload serving: the Python ContinuousServer instead of the C++ server")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the short vol_marcher (100k, 512x512) and serving (8 scenes) runs of the headline line")
+                    help="skip the short vol_marcher (100k, 512x512; 16 views of 64x64 batched), vol_raster, batched "
+                         "(c3) and serving (c4) runs of the headline line")
     ap.add_argument("--workload", choices=["served", "batched", "marcher", "raster", "serving", "configs"], default="served",
                     help="served: the headline line (default); batched: 3 scenes x 16 views, mixed resolutions, "
                          "forward+backward under CUDA graphs; marcher: vol_marcher forward+backward, 100k, 512x512; "
@@ -448,6 +449,7 @@ def run_ours(args):
         del fb, frame, ctx, fb_plain, host_plain
         server.release_buffers()
         extras["vol_marcher_c2"] = measure_marcher(dev, n_cams=3)
+        extras["vol_marcher_batched_small_views"] = measure_marcher_batched(dev)
         extras["vol_raster_c2_scene"] = measure_vol_raster(dev, n_cams=3)
         extras["batched_c3"] = measure_batched(dev, steps=3, warmup=2)
         extras["serving_c4"] = measure_serving(dev, n_req=200, warmup=1)
@@ -667,6 +669,59 @@ def measure_marcher(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int
                                    "1965 MHz maximum clock; FP32 instructions per fill from "
                                    f"profiles/{MARCHER_PROFILE}"}
     return out
+
+
+def measure_marcher_batched(dev, n_views: int = 16, n: int = 100_000, W: int = 64, H: int = 64, reps: int = 2):
+    """vol_marcher forward + backward of many small views (training-sized
+    crops) of the c2 scene: one reference-facing call per view
+    (cpp_binding.forward / backward) against one batched launch sequence
+    (batch.BatchRenderer(kind="march"), dgmr_vm_batch_*).  CUDA events around
+    the whole view set, one warm-up then the median of ``reps``."""
+    import torch
+    from differentiable_gaussian_mixture_renderer_b200 import cpp_binding
+    from differentiable_gaussian_mixture_renderer_b200 import scene as S
+    from differentiable_gaussian_mixture_renderer_b200.batch import BatchRenderer
+    from differentiable_gaussian_mixture_renderer_b200.serving import GaussianScene
+    sc = GaussianScene.from_numpy(S.make_scene(n, seed=0), dev)
+    cams = S.random_cameras(n_views, W, H, seed=1)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32).to(dev)
+    gen = torch.Generator(device=dev).manual_seed(2)
+    grads = [torch.randn(3, H, W, device=dev, generator=gen) for _ in cams]
+    bg = torch.zeros(3, device=dev)
+
+    def per_call():
+        for cam, g in zip(cams, grads):
+            args = (sc.shs, sc.weights.reshape(-1, 1), sc.centroids, sc.scales, sc.rotations, t(cam.view), t(cam.proj),
+                    t(cam.campos), bg, W, H, cam.tan_fovx, cam.tan_fovy, 0)
+            cpp_binding.backward(*args, g, cpp_binding.forward(*args))
+
+    r = BatchRenderer({"c2": sc}, dev, kind="march")
+    plan = r.plan([("c2", cam) for cam in cams], backward=True)
+    for dst, g in zip(plan.grad_framebuffers, grads):
+        dst.copy_(g)
+
+    def batched():
+        r.forward(plan)
+        r.backward(plan)
+
+    def timed(f):
+        f()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    t_call, t_batch = timed(per_call), timed(batched)
+    return {"per_call_ms": t_call, "batched_ms": t_batch, "views_per_s_per_call": 1e3 * n_views / t_call,
+            "views_per_s_batched": 1e3 * n_views / t_batch, "batched_over_per_call": t_call / t_batch,
+            "workload": f"vol_marcher forward + backward of {n_views} views of {W}x{H}, {n} Gaussians (the c2 scene), "
+                        "one call per view vs one dgmr_vm_batch_* launch sequence"}
 
 
 def measure_vol_raster(dev, n_cams: int = 3, n: int = 100_000, W: int = 512, H: int = 512):

@@ -1,14 +1,17 @@
-"""Batched multi-view splat rendering: many cameras of several resident scenes,
+"""Batched multi-view rendering: many cameras of several resident scenes,
 uneven Gaussian counts and resolutions, in one launch sequence, optionally
-captured in a CUDA graph, with an autotuner over the batch depth.
+captured in a CUDA graph, with an autotuner over the batch depth -- for the
+splat renderer (``kind="splat"``) and the volume marcher (``kind="march"``).
 
-The reference renders one view per call (splat_forward.cu:30-338); here a
-``BatchPlan`` holds everything one batch needs (view table, workspaces,
-framebuffers, gradient buffers), so a forward (and backward) of the whole
-batch is two C calls -- ``dgmr_splat_batch_forward`` / ``_backward`` -- that
-allocate nothing and never synchronise the host, which is what lets a plan
-be captured once and replayed.  Every view's image is bit-identical to
-rendering it alone; per-scene gradients are the sum over that scene's views.
+The reference renders one view per call (splat_forward.cu:30-338; its
+vol_marcher.apply, python_bindings/vol_marcher.py:19-65, marches one camera);
+here a ``BatchPlan`` holds everything one batch needs (view table,
+workspaces, framebuffers, gradient buffers), so a forward (and backward) of
+the whole batch is two C calls -- ``dgmr_splat_batch_forward`` /
+``_backward``, or ``dgmr_vm_batch_forward`` / ``_backward`` -- that allocate
+nothing and never synchronise the host, which is what lets a plan be
+captured once and replayed.  Every view's image is bit-identical to rendering
+it alone; per-scene gradients are the sum over that scene's views.
 """
 from __future__ import annotations
 
@@ -52,13 +55,23 @@ class BatchPlan:
 
 
 class BatchRenderer:
-    """Resident scenes rendered in batches of views."""
+    """Resident scenes rendered in batches of views, by the splat renderer
+    (``kind="splat"``) or the volume marcher (``kind="march"``, float32,
+    full render mode)."""
 
-    def __init__(self, scenes: dict, device=None, capacity_margin: float = 1.1):
+    def __init__(self, scenes: dict, device=None, capacity_margin: float = 1.1, kind: str = "splat"):
+        if kind not in ("splat", "march"):
+            raise ValueError("kind must be 'splat' or 'march'")
         self.device = torch.device(device or "cuda")
         self.scenes: dict = scenes
         self.lib = N.lib()
         self.margin = capacity_margin
+        self.kind = kind
+        pre = "dgmr_splat_batch_" if kind == "splat" else "dgmr_vm_batch_"
+        self._c_size = getattr(self.lib, pre + "workspace_size")
+        self._c_pre = getattr(self.lib, pre + "preprocess")
+        self._c_fwd = getattr(self.lib, pre + "forward")
+        self._c_bwd = getattr(self.lib, pre + "backward")
 
     # ------------------------------------------------------------ planning
     def _tables(self, views, backward: bool):
@@ -77,8 +90,8 @@ class BatchRenderer:
 
     def _sizes(self, c_scenes, c_views, cap: int):
         fb, pb = C.c_size_t(0), C.c_size_t(0)
-        N.check(self.lib.dgmr_splat_batch_workspace_size(c_scenes, len(c_scenes), c_views, len(c_views), cap,
-                                                         C.byref(fb), C.byref(pb)), "batch workspace size")
+        N.check(self._c_size(c_scenes, len(c_scenes), c_views, len(c_views), cap, C.byref(fb), C.byref(pb)),
+                "batch workspace size")
         return int(fb.value), int(pb.value)
 
     def count_pairs(self, views) -> int:
@@ -87,8 +100,8 @@ class BatchRenderer:
         fbytes, _ = self._sizes(c_scenes, c_views, 0)
         ws = torch.empty(max(fbytes, 1), dtype=torch.uint8, device=self.device)
         stats = torch.zeros(4, dtype=torch.int32, device=self.device)
-        N.check(self.lib.dgmr_splat_batch_preprocess(c_scenes, len(c_scenes), c_views, len(c_views), N.ptr(ws), fbytes,
-                                                     N.ptr(stats), N.stream_handle()), "batch preprocess")
+        N.check(self._c_pre(c_scenes, len(c_scenes), c_views, len(c_views), N.ptr(ws), fbytes, N.ptr(stats),
+                            N.stream_handle()), "batch preprocess")
         return int(stats[0].item())
 
     def plan(self, views, backward: bool = False, capacity: int | None = None) -> BatchPlan:
@@ -122,17 +135,18 @@ class BatchRenderer:
     # ------------------------------------------------------------ running
     def forward(self, p: BatchPlan, stream: torch.cuda.Stream | None = None):
         s = N.stream_handle(stream)
-        N.check(self.lib.dgmr_splat_batch_forward(p.c_scenes, len(p.c_scenes), p.c_views, p.n_views, N.ptr(p.frame_ws),
-                                                  p.frame_ws.numel(), N.ptr(p.pair_ws), p.pair_ws.numel(), p.capacity,
-                                                  N.ptr(p.stats), s), "batch forward")
+        N.check(self._c_fwd(p.c_scenes, len(p.c_scenes), p.c_views, p.n_views, N.ptr(p.frame_ws), p.frame_ws.numel(),
+                            N.ptr(p.pair_ws), p.pair_ws.numel(), p.capacity, N.ptr(p.stats), s), "batch forward")
 
     def backward(self, p: BatchPlan, stream: torch.cuda.Stream | None = None):
         if p.c_grads is None:
             raise ValueError("plan was made without backward buffers")
         s = N.stream_handle(stream)
-        N.check(self.lib.dgmr_splat_batch_backward(p.c_scenes, len(p.c_scenes), p.c_views, p.n_views, p.c_grads,
-                                                   N.ptr(p.frame_ws), p.frame_ws.numel(), N.ptr(p.pair_ws),
-                                                   p.pair_ws.numel(), p.capacity, s), "batch backward")
+        args = [p.c_scenes, len(p.c_scenes), p.c_views, p.n_views, p.c_grads, N.ptr(p.frame_ws), p.frame_ws.numel(),
+                N.ptr(p.pair_ws), p.pair_ws.numel(), p.capacity]
+        if self.kind == "march":
+            args.append(N.ptr(p.stats))  # the step-limit flag
+        N.check(self._c_bwd(*args, s), "batch backward")
 
     def capture(self, p: BatchPlan, backward: bool = False) -> BatchPlan:
         """Capture forward (+ backward) of the plan in a CUDA graph.  Replays

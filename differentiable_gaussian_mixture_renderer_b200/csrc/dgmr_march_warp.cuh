@@ -97,17 +97,38 @@ __device__ __forceinline__ RayEntry<T> load_entry(const VmMarch<T>& a, int32_t k
     return en;
 }
 
-// Tile work order for the march: heaviest tile first (k_tile_order), so the
-// longest rays start at the head of the grid.
+// The frames a march launch covers.  A single frame: one camera (a kernel
+// parameter) and the image planes of VmMarch.  A batch (VmBatchFrames, float)
+// looks each tile's view up in its view table; its tiles are numbered across
+// views and its rays index one array of all views' pixels.
 template <class T>
-__device__ __forceinline__ bool ray_pixel(const CameraT<T>& cam, const uint32_t* order, unsigned* tile, unsigned* px, unsigned* py)
+struct VmSingleFrame {
+    CameraT<T> cam0;
+    __device__ __forceinline__ unsigned view(unsigned) const { return 0u; }
+    __device__ __forceinline__ const CameraT<T>& cam(unsigned) const { return cam0; }
+    __device__ __forceinline__ unsigned tile_base(unsigned) const { return 0u; }
+    __device__ __forceinline__ size_t px_base(unsigned) const { return 0; }
+    __device__ __forceinline__ size_t rays() const { return size_t(cam0.W) * cam0.H; }
+    __device__ __forceinline__ T* fb(unsigned, const VmMarch<T>& a) const { return a.fb; }
+    __device__ __forceinline__ T* remaining_T(unsigned, const VmMarch<T>& a) const { return a.remaining_T; }
+    __device__ __forceinline__ const T* grad_fb(unsigned, const VmMarch<T>& a) const { return a.grad_fb; }
+};
+
+// Tile work order for the march: heaviest tile first (k_tile_order), so the
+// longest rays start at the head of the grid.  tile = the launch-wide tile
+// (it indexes the ranges), view = its frame, (px, py) = the ray's pixel there.
+template <class T, class Frames>
+__device__ __forceinline__ bool ray_pixel(const Frames& frames, const uint32_t* order, unsigned* tile, unsigned* view, unsigned* px, unsigned* py)
 {
     const unsigned groups = kTilePixels / kRayWarps;
     const unsigned item = blockIdx.x / groups, group = blockIdx.x % groups;
     *tile = order ? order[item] : item;
+    *view = frames.view(*tile);
+    const CameraT<T>& cam = frames.cam(*view);
+    const unsigned lt = *tile - frames.tile_base(*view);
     const unsigned p = group * kRayWarps + (threadIdx.x >> 5);
-    *px = (*tile % cam.gx) * kTile + (p % kTile);
-    *py = (*tile / cam.gx) * kTile + (p / kTile);
+    *px = (lt % cam.gx) * kTile + (p % kTile);
+    *py = (lt / cam.gx) * kTile + (p / kTile);
     return *px < cam.W && *py < cam.H;
 }
 
@@ -328,15 +349,17 @@ __device__ __forceinline__ void warp_store_bins(Bin<T>* bins, const Bin<T> (&acc
     __syncwarp();
 }
 
-template <class T>
-__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_march_warp(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+template <class T, class Frames>
+__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_march_warp(VmMarch<T> a, const __grid_constant__ Frames frames,
+    const uint32_t* __restrict__ order)
 {
     __shared__ RayWarpShared<T> shared_rays[kRayWarps];
     RayWarpShared<T>& sm = shared_rays[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31u;
-    unsigned tile, px, py;
-    if (!ray_pixel(cam, order, &tile, &px, &py))
+    unsigned tile, view, px, py;
+    if (!ray_pixel<T>(frames, order, &tile, &view, &px, &py))
         return; // the whole warp: no block-level barrier below
+    const CameraT<T>& cam = frames.cam(view);
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
     const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
@@ -362,7 +385,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
         __syncwarp();
         if (step < a.store_steps) {
             // keep this step's samples for the backward (coalesced: 32 lanes x 4 rounds)
-            const size_t ray = size_t(py) * cam.W + px, rays = size_t(cam.W) * cam.H;
+            const size_t ray = frames.px_base(view) + size_t(py) * cam.W + px, rays = frames.rays();
             T* dst = a.store_borders + (size_t(step) * rays + ray) * kSmallSteps;
 #pragma unroll
             for (unsigned r = 0; r < kRayRounds; ++r)
@@ -415,10 +438,11 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
             atomicAdd(a.work, fills);
         const size_t pix = size_t(py) * cam.W + px;
         const size_t plane = size_t(cam.W) * cam.H;
-        a.fb[pix] = colour.x + tr * cam.bg[0];
-        a.fb[plane + pix] = colour.y + tr * cam.bg[1];
-        a.fb[2 * plane + pix] = colour.z + tr * cam.bg[2];
-        a.remaining_T[pix] = tr;
+        T* fb = frames.fb(view, a);
+        fb[pix] = colour.x + tr * cam.bg[0];
+        fb[plane + pix] = colour.y + tr * cam.bg[1];
+        fb[2 * plane + pix] = colour.z + tr * cam.bg[2];
+        frames.remaining_T(view, a)[pix] = tr;
     }
 }
 
@@ -508,24 +532,30 @@ __device__ __forceinline__ void warp_grad(const Bin<T>* gbins, const T* borders,
 }
 
 // vol_marcher_backward.cu:115-319 with one warp per ray
-template <class T>
-__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_march_warp_bwd(VmMarch<T> a, CameraT<T> cam, const uint32_t* __restrict__ order)
+template <class T, class Frames>
+__global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_march_warp_bwd(VmMarch<T> a, const __grid_constant__ Frames frames,
+    const uint32_t* __restrict__ order)
 {
     __shared__ RayWarpSharedBwd<T> shared_rays[kRayWarps];
     RayWarpSharedBwd<T>& sm = shared_rays[threadIdx.x >> 5];
     const unsigned lane = threadIdx.x & 31u;
-    unsigned tile, px, py;
-    if (!ray_pixel(cam, order, &tile, &px, &py))
+    unsigned tile, view, px, py;
+    if (!ray_pixel<T>(frames, order, &tile, &view, &px, &py))
         return;
+    const T* grad_fb = frames.grad_fb(view, a);
+    if (!grad_fb) // a view of a batch without an image gradient
+        return;
+    const CameraT<T>& cam = frames.cam(view);
     const V3<T> o = { cam.campos[0], cam.campos[1], cam.campos[2] };
     const V3<T> d = pixel_dir(cam, px, py);
     const int32_t b = a.ranges[2 * tile], e = a.ranges[2 * tile + 1];
     const WarpRayMasks rm = warp_ray_masks(a, b, e, o, d, lane);
     const size_t pix = size_t(py) * cam.W + px;
     const size_t plane = size_t(cam.W) * cam.H;
-    const T final_T = a.remaining_T[pix];
-    V3<T> colour = { a.fb[pix] - final_T * cam.bg[0], a.fb[plane + pix] - final_T * cam.bg[1], a.fb[2 * plane + pix] - final_T * cam.bg[2] };
-    const V3<T> gc = { a.grad_fb[pix], a.grad_fb[plane + pix], a.grad_fb[2 * plane + pix] };
+    const T* fb = frames.fb(view, a);
+    const T final_T = frames.remaining_T(view, a)[pix];
+    V3<T> colour = { fb[pix] - final_T * cam.bg[0], fb[plane + pix] - final_T * cam.bg[1], fb[2 * plane + pix] - final_T * cam.bg[2] };
+    const V3<T> gc = { grad_fb[pix], grad_fb[plane + pix], grad_fb[2 * plane + pix] };
     const T gt = (gc.x * cam.bg[0] + gc.y * cam.bg[1]) + gc.z * cam.bg[2];
     T tr = T(1);
     T start = T(0);
@@ -539,7 +569,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
         int n_sections;
         if (step < a.store_steps) {
             // the forward kept this step's samples: no section set, no sampling
-            const size_t ray = size_t(py) * cam.W + px, rays = size_t(cam.W) * cam.H;
+            const size_t ray = frames.px_base(view) + size_t(py) * cam.W + px, rays = frames.rays();
             const T* src = a.store_borders + (size_t(step) * rays + ray) * kSmallSteps;
 #pragma unroll
             for (unsigned r = 0; r < kRayRounds; ++r)

@@ -6,6 +6,7 @@
 
 #include "../../include/dgmr_b200.h"
 #include "dgmr_abi_common.h"
+#include "dgmr_batch.cuh"
 #include "dgmr_binning.cuh"
 #include "dgmr_device_grad.cuh"
 #include "dgmr_marching.cuh"
@@ -99,28 +100,26 @@ struct VmPre {
     Formulation form;
 };
 
-// vol_marcher_forward.cu:98-176
+// vol_marcher_forward.cu:98-176.  Gaussian i of the scene, written to slot o
+// of the per-frame arrays (o = i for one frame; the view's offset + i in a batch).
 template <class T>
-__global__ void __launch_bounds__(128) k_vm_preprocess(VmPre<T> p, CameraT<T> cam)
+__device__ __forceinline__ void vm_preprocess_one(const VmPre<T>& p, const CameraT<T>& cam, uint32_t i, uint32_t o)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.N)
-        return;
-    p.tiles_touched[i] = 0;
-    p.rects[2 * i] = 0;
-    p.rects[2 * i + 1] = 0;
-    p.xy[2 * i] = T(0);
-    p.xy[2 * i + 1] = T(0);
-    p.depths[i] = T(0);
-    p.masses[i] = T(0);
+    p.tiles_touched[o] = 0;
+    p.rects[2 * o] = 0;
+    p.rects[2 * o + 1] = 0;
+    p.xy[2 * o] = T(0);
+    p.xy[2 * o + 1] = T(0);
+    p.depths[o] = T(0);
+    p.masses[o] = T(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        p.rgb[3 * i + k] = T(0);
-        p.clamped[3 * i + k] = 0;
+        p.rgb[3 * o + k] = T(0);
+        p.clamped[3 * o + k] = 0;
     }
 #pragma unroll
     for (int k = 0; k < 6; ++k)
-        p.inv_cov[6 * i + k] = T(0);
+        p.inv_cov[6 * o + k] = T(0);
     const V3<T> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
     if (view_z(cam.view, mu) < T(0.2f))
         return;
@@ -149,32 +148,40 @@ __global__ void __launch_bounds__(128) k_vm_preprocess(VmPre<T> p, CameraT<T> ca
     };
     const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[0], T(1.f / 255.f))));
     const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[2], T(1.f / 255.f))));
-    p.rects[2 * i] = ex;
-    p.rects[2 * i + 1] = ey;
+    p.rects[2 * o] = ex;
+    p.rects[2 * o + 1] = ey;
     const TileRect r = get_rect(float(g.centroid.x), float(g.centroid.y), ex, ey, cam.gx, cam.gy);
     const unsigned touched = (r.x1 - r.x0) * (r.y1 - r.y0);
     if (touched == 0)
         return;
-    p.tiles_touched[i] = touched;
-    p.xy[2 * i] = g.centroid.x;
-    p.xy[2 * i + 1] = g.centroid.y;
+    p.tiles_touched[o] = touched;
+    p.xy[2 * o] = g.centroid.x;
+    p.xy[2 * o + 1] = g.centroid.y;
     const S3<T> inv = inverse_sym3(filtered);
     const T smax = max_f(sc.x, max_f(sc.y, sc.z));
     const T depth = dist - (smax * T(kRelevanceSigma)) / T(2);
-    p.depths[i] = depth;
+    p.depths[o] = depth;
     const V3<T> dir = { (mu.x - campos.x) / dist, (mu.y - campos.y) / dist, (mu.z - campos.z) / dist };
     uint8_t mask[3];
     const V3<T> col = sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, mask);
-    p.rgb[3 * i] = col.x;
-    p.rgb[3 * i + 1] = col.y;
-    p.rgb[3 * i + 2] = col.z;
+    p.rgb[3 * o] = col.x;
+    p.rgb[3 * o + 1] = col.y;
+    p.rgb[3 * o + 2] = col.z;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        p.clamped[3 * i + k] = mask[k];
+        p.clamped[3 * o + k] = mask[k];
 #pragma unroll
     for (int k = 0; k < 6; ++k)
-        p.inv_cov[6 * i + k] = inv.v[k];
-    p.masses[i] = mass;
+        p.inv_cov[6 * o + k] = inv.v[k];
+    p.masses[o] = mass;
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_vm_preprocess(VmPre<T> p, CameraT<T> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.N)
+        vm_preprocess_one(p, cam, i, i);
 }
 
 // Ray through the pixel centre (vol_marcher_forward.cu:308-315)
@@ -288,31 +295,48 @@ struct VmBwdGauss {
     Formulation form;
 };
 
-// vol_marcher_backward.cu:321-384
-template <class T>
-__global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, CameraT<T> cam)
+// vol_marcher_backward.cu:321-384, for Gaussian i of the scene seen in slot o
+// (o = i for one frame).  kAdd = false writes the gradient rows (a single
+// frame); kAdd = true adds this view's rows to them (a batch, whose views of
+// one scene are added in view order after the rows are zeroed).  Each term
+// added is the value a single frame writes, so a batch's gradient is the sum,
+// in view order, of the single-view gradients.
+template <class T, bool kAdd>
+__device__ __forceinline__ void vm_bwd_gaussian_one(const VmBwdGauss<T>& p, const CameraT<T>& cam, T aa, uint32_t i, uint32_t o)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.N)
+    const double* a = p.acc + size_t(o) * kVmAcc;
+    const V3<T> g_march = { T(a[10]), T(a[11]), T(a[12]) }; // the march's own centroid gradient
+    const auto put_centroid = [&](V3<T> g) {
+        if (kAdd) {
+            p.g_centroids[3 * i] += g.x;
+            p.g_centroids[3 * i + 1] += g.y;
+            p.g_centroids[3 * i + 2] += g.z;
+        } else {
+            p.g_centroids[3 * i] = g.x;
+            p.g_centroids[3 * i + 1] = g.y;
+            p.g_centroids[3 * i + 2] = g.z;
+        }
+    };
+    if (!kAdd) {
+        for (int k = 0; k < p.sh_stride * 3; ++k)
+            p.g_sh[size_t(i) * p.sh_stride * 3 + k] = T(0);
+        p.g_weights[i] = T(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            p.g_scales[3 * i + k] = T(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            p.g_rotations[4 * i + k] = T(0);
+    }
+    if (p.tiles_touched[o] == 0) {
+        put_centroid(g_march);
         return;
-    const double* a = p.acc + size_t(i) * kVmAcc;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        p.g_centroids[3 * i + k] = T(a[10 + k]);
-    for (int k = 0; k < p.sh_stride * 3; ++k)
-        p.g_sh[size_t(i) * p.sh_stride * 3 + k] = T(0);
-    p.g_weights[i] = T(0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        p.g_scales[3 * i + k] = T(0);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        p.g_rotations[4 * i + k] = T(0);
-    if (p.tiles_touched[i] == 0)
-        return;
+    }
     const V3<T> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
-    if (view_z(cam.view, mu) < T(0.2))
+    if (view_z(cam.view, mu) < T(0.2)) {
+        put_centroid(g_march);
         return;
+    }
     const T w = p.weights[i];
     // the reference does not apply cov_scale_multiplier in the backward (vol_marcher_backward.cu:342)
     const V3<T> sc = { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] };
@@ -322,7 +346,7 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     const V3<T> delta = sub3(mu, campos);
     const T dist = len3(delta);
     const S3<T> cov3 = compute_cov(sc, R);
-    const T fks = dist * p.aa;
+    const T fks = dist * aa;
     S3<T> filtered = cov3;
     filtered.v[0] = filtered.v[0] + fks * fks;
     filtered.v[3] = filtered.v[3] + fks * fks;
@@ -330,10 +354,13 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     const M3<T> W3 = upper3(cam.view);
     const S2<T> cov2d = affine_transform_and_cut(cov3, W3);
     const T mass = weight_to_mass(p.form, w, sc, cov2d);
-    if (mass <= T(0))
+    if (mass <= T(0)) {
+        put_centroid(g_march);
         return;
+    }
     const V3<T> dir = { delta.x / dist, delta.y / dist, delta.z / dist };
-    const V3<T> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<T> { T(a[1]), T(a[2]), T(a[3]) }, p.clamped + 3 * size_t(i), T(1), p.g_sh);
+    const V3<T> g_dir = grad_sh_to_colour(p.sh, i, p.sh_stride, p.sh_degree, dir, V3<T> { T(a[1]), T(a[2]), T(a[3]) }, p.clamped + 3 * size_t(o), T(1),
+        p.g_sh, kAdd);
     V3<T> g_mu = mul3(g_dir, T(1) / dist);
     T g_dist = -dot3(g_dir, delta) / (dist * dist);
     S3<T> g_inv;
@@ -368,21 +395,37 @@ __global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, Camer
     }
     S3<T> g_cov3 = g_filtered;
     const T g_fks2 = (g_filtered.v[0] + g_filtered.v[3]) + g_filtered.v[5];
-    g_dist = g_dist + (g_fks2 * T(2) * fks) * p.aa;
+    g_dist = g_dist + (g_fks2 * T(2) * fks) * aa;
     grad_affine_transform_and_cut(cov3, W3, g_cov2d, &g_cov3, static_cast<M3<T>*>(nullptr));
     T g_q[4] = { T(0), T(0), T(0), T(0) };
     grad_compute_cov(sc, q[0], q[1], q[2], q[3], g_cov3, &g_s, g_q);
     g_mu = add3(g_mu, mul3(delta, g_dist / dist));
-    p.g_weights[i] = g_w;
-    p.g_scales[3 * i] = g_s.x;
-    p.g_scales[3 * i + 1] = g_s.y;
-    p.g_scales[3 * i + 2] = g_s.z;
+    if (kAdd) {
+        p.g_weights[i] += g_w;
+        p.g_scales[3 * i] += g_s.x;
+        p.g_scales[3 * i + 1] += g_s.y;
+        p.g_scales[3 * i + 2] += g_s.z;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-        p.g_rotations[4 * i + k] = g_q[k];
-    p.g_centroids[3 * i] += g_mu.x;
-    p.g_centroids[3 * i + 1] += g_mu.y;
-    p.g_centroids[3 * i + 2] += g_mu.z;
+        for (int k = 0; k < 4; ++k)
+            p.g_rotations[4 * i + k] += g_q[k];
+    } else {
+        p.g_weights[i] = g_w;
+        p.g_scales[3 * i] = g_s.x;
+        p.g_scales[3 * i + 1] = g_s.y;
+        p.g_scales[3 * i + 2] = g_s.z;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            p.g_rotations[4 * i + k] = g_q[k];
+    }
+    put_centroid(V3<T> { g_march.x + g_mu.x, g_march.y + g_mu.y, g_march.z + g_mu.z });
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_vm_bwd_gaussians(VmBwdGauss<T> p, CameraT<T> cam)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.N)
+        vm_bwd_gaussian_one<T, false>(p, cam, p.aa, i, i);
 }
 
 // Heaviest-tile-first order of the march's blocks, in the workspace past the
@@ -402,7 +445,7 @@ inline const uint32_t* march_order(const int32_t* ranges, const CameraT<T>& cam,
 }
 
 template <class T>
-inline T aa_multiplier(const CameraT<T>& cam)
+__host__ __device__ inline T aa_multiplier(const CameraT<T>& cam)
 {
     return ((T(kFilterSD) * cam.tan_fovx) * T(2)) / T(float(cam.W));
 }
@@ -474,7 +517,7 @@ dgmr_status vm_render(const dgmr_scene* scene, const dgmr_camera* camera, dgmr_v
         a.store_steps = store_steps;
     }
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
-    k_vm_march_warp<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
+    k_vm_march_warp<T, VmSingleFrame<T>><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, VmSingleFrame<T> { cam }, order);
     note_launch();
     return launch_status();
 }
@@ -513,7 +556,7 @@ dgmr_status vm_backward(const dgmr_scene* scene, const dgmr_camera* camera, cons
         a.store_steps = store_steps;
     }
     const uint32_t* order = march_order(c->i_ranges, cam, workspace, L.bytes, workspace_bytes, s);
-    k_vm_march_warp_bwd<T><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, cam, order);
+    k_vm_march_warp_bwd<T, VmSingleFrame<T>><<<cam.gx * cam.gy * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, VmSingleFrame<T> { cam }, order);
     note_launch();
     VmBwdGauss<T> p { N, static_cast<const T*>(scene->centroids), static_cast<const T*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const T*>(scene->weights), static_cast<const T*>(scene->scales), static_cast<const T*>(scene->rotations), c->rgb_sh_clamped,
@@ -533,6 +576,228 @@ inline bool cache_ok(const dgmr_vm_cache* c, bool need_list, int32_t n_gaussians
     return n_gaussians == 0
         || (c->rects && c->rgb && c->rgb_sh_clamped && c->depths && c->points_xy_image && c->inverse_filtered_cov3d && c->filtered_masses
             && c->tiles_touched && c->point_offsets);
+}
+
+// ---------------------------------------------------------------------------
+// Batched volume marching (no reference counterpart: the reference marches
+// one view per call, vol_marcher_forward.cu:42-503).  Many views of one or
+// several scenes (float32) go through ONE launch sequence over the view table
+// of dgmr_batch.cuh: one preprocess over every (view, Gaussian) slot, the
+// splat renderer's batched binning, one march over the tiles of all views
+// (heaviest first) and, for the backward, one backward march plus one pass
+// over every scene Gaussian that adds its views in view order.  Each view's
+// point list is the one it gets alone (the binning keeps every view's
+// (depth, index) order), and the march of a ray reads only its own view's
+// list, camera and planes, so each image is the same, bit for bit, as a
+// dgmr_vm_forward_render of that view.
+
+// The batch's frames for the march kernels.
+struct VmBatchFrames {
+    BatchTable tab;
+    __device__ __forceinline__ unsigned view(unsigned t) const { return BatchTable::owner(tab.tile_off, tab.n_views, t); }
+    __device__ __forceinline__ const CameraT<float>& cam(unsigned v) const { return tab.views[v].cam; }
+    __device__ __forceinline__ unsigned tile_base(unsigned v) const { return tab.tile_off[v]; }
+    __device__ __forceinline__ size_t px_base(unsigned v) const { return tab.views[v].px_off; }
+    __device__ __forceinline__ size_t rays() const { return tab.px_total; }
+    __device__ __forceinline__ float* fb(unsigned v, const VmMarch<float>&) const { return tab.views[v].fb; }
+    __device__ __forceinline__ float* remaining_T(unsigned v, const VmMarch<float>&) const { return tab.final_T + tab.views[v].px_off; }
+    __device__ __forceinline__ const float* grad_fb(unsigned v, const VmMarch<float>&) const { return tab.views[v].grad_fb; }
+};
+
+// Frame workspace: statistics, the per-slot arrays (the single frame's cache,
+// plus a copy of each slot's centroid so the march reads every list entry by
+// its slot), the backward's accumulators, ranges, remaining transmittance of
+// every pixel, the march order and the binning's Gaussian-sized buffers.
+// Pair workspace: the binning's pair buffers and sort scratch.
+struct VmBatchLayout {
+    uint32_t* stats;
+    int32_t* rects;
+    float* rgb;
+    uint8_t* clamped;
+    float* depths;
+    float* xy;
+    float* inv_cov;
+    float* masses;
+    uint32_t* tiles_touched;
+    uint32_t* point_offsets;
+    float* centroids;
+    double* acc;
+    int32_t* ranges;
+    float* remaining_T;
+    uint32_t* tile_order;
+    BinningBuffers bin;
+    size_t bytes;
+    size_t pair_bytes;
+};
+
+inline VmBatchLayout vm_batch_layout(uint32_t G, uint32_t n_tiles, size_t n_px, uint32_t cap, void* base, void* pair_base)
+{
+    VmBatchLayout L;
+    Carver c;
+    c.base = static_cast<char*>(base);
+    L.stats = c.take<uint32_t>(4);
+    L.rects = c.take<int32_t>(size_t(G) * 2);
+    L.rgb = c.take<float>(size_t(G) * 3);
+    L.clamped = c.take<uint8_t>(size_t(G) * 3);
+    L.depths = c.take<float>(G);
+    L.xy = c.take<float>(size_t(G) * 2);
+    L.inv_cov = c.take<float>(size_t(G) * 6);
+    L.masses = c.take<float>(G);
+    L.tiles_touched = c.take<uint32_t>(G);
+    L.point_offsets = c.take<uint32_t>(G);
+    L.centroids = c.take<float>(size_t(G) * 3);
+    L.acc = c.take<double>(size_t(G) * kVmAcc);
+    L.ranges = c.take<int32_t>(size_t(n_tiles) * 2);
+    L.remaining_T = c.take<float>(n_px);
+    L.tile_order = c.take<uint32_t>(n_tiles);
+    carve_binning_gaussians(c, L.bin, G, n_tiles);
+    L.bytes = c.off;
+    Carver pc;
+    pc.base = static_cast<char*>(pair_base);
+    carve_binning_pairs(pc, L.bin, G, cap);
+    L.pair_bytes = pc.off;
+    return L;
+}
+
+// One thread per (view, Gaussian) slot: the single frame's preprocess with the
+// view's camera, then the slot's depth key, identity permutation and centroid.
+__global__ void __launch_bounds__(128) k_vm_batch_preprocess(VmPre<float> out, float* __restrict__ slot_centroids, uint32_t* __restrict__ depth_key,
+    uint32_t* __restrict__ perm, const __grid_constant__ BatchTable tab)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= tab.G)
+        return;
+    const uint32_t v = BatchTable::owner(tab.g_off, tab.n_views, g);
+    const BatchView& bv = tab.views[v];
+    const BatchScene& sc = tab.scenes[bv.scene];
+    const uint32_t i = g - tab.g_off[v];
+    VmPre<float> p = out;
+    p.N = sc.n;
+    p.centroids = sc.centroids;
+    p.sh = sc.sh;
+    p.sh_stride = sc.sh_stride;
+    p.sh_degree = sc.sh_degree;
+    p.weights = sc.weights;
+    p.scales = sc.scales;
+    p.rotations = sc.rotations;
+    p.aa = aa_multiplier(bv.cam);
+    p.form = sc.form;
+    vm_preprocess_one(p, bv.cam, i, g);
+    depth_key[g] = __float_as_uint(p.depths[g]);
+    perm[g] = g;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        slot_centroids[3 * size_t(g) + k] = sc.centroids[3 * size_t(i) + k];
+}
+
+// per scene Gaussian: zero its gradient rows, then add the chain rule of every
+// view of its scene that has an image gradient, in view order
+__global__ void __launch_bounds__(128) k_vm_batch_bwd_gaussians(VmBwdGauss<float> state, const __grid_constant__ BatchTable tab)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= tab.scene_off[tab.n_scenes])
+        return;
+    const uint32_t s = BatchTable::owner(tab.scene_off, tab.n_scenes, k);
+    const BatchScene& sc = tab.scenes[s];
+    const uint32_t i = k - tab.scene_off[s];
+    if (!sc.g_sh) // a scene entry without gradient outputs
+        return;
+    VmBwdGauss<float> p = state;
+    p.N = sc.n;
+    p.centroids = sc.centroids;
+    p.sh = sc.sh;
+    p.sh_stride = sc.sh_stride;
+    p.sh_degree = sc.sh_degree;
+    p.weights = sc.weights;
+    p.scales = sc.scales;
+    p.rotations = sc.rotations;
+    p.g_sh = sc.g_sh;
+    p.g_weights = sc.g_weights;
+    p.g_centroids = sc.g_centroids;
+    p.g_scales = sc.g_scales;
+    p.g_rotations = sc.g_rotations;
+    p.form = sc.form;
+    for (int c = 0; c < p.sh_stride * 3; ++c)
+        p.g_sh[size_t(i) * p.sh_stride * 3 + c] = 0.f;
+    p.g_weights[i] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        p.g_centroids[3 * i + c] = 0.f;
+        p.g_scales[3 * i + c] = 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        p.g_rotations[4 * i + c] = 0.f;
+    for (uint32_t q = sc.view_begin; q < sc.view_end; ++q) {
+        const uint32_t v = tab.view_by_scene[q];
+        if (tab.views[v].grad_fb)
+            vm_bwd_gaussian_one<float, true>(p, tab.views[v].cam, aa_multiplier(tab.views[v].cam), i, tab.g_off[v] + i);
+    }
+}
+
+struct VmBatchPlan {
+    BatchTable tab;
+    VmBatchLayout L;
+};
+
+// Validates the batch and builds its table and layout.  grads may be null
+// (forward); the bases may be null (size query).
+dgmr_status make_vm_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, const dgmr_scene_grads* grads,
+    int64_t pair_capacity, void* frame_ws, void* pair_ws, VmBatchPlan& plan)
+{
+    if (pair_capacity < 0 || pair_capacity > int64_t(0x7fffffff))
+        return DGMR_ERR_BAD_ARG;
+    BatchTable& t = plan.tab;
+    const dgmr_status st = build_batch_table(scenes, n_scenes, views, n_views, grads, Formulation::Opacity, t);
+    if (st != DGMR_OK)
+        return st;
+    plan.L = vm_batch_layout(t.G, t.n_tiles, t.px_total, uint32_t(pair_capacity), frame_ws, pair_ws);
+    t.final_T = plan.L.remaining_T;
+    t.n_contrib = nullptr;
+    return DGMR_OK;
+}
+
+dgmr_status vm_batch_check_ws(const VmBatchPlan& plan, void* frame_ws, size_t frame_bytes, void* pair_ws, size_t pair_bytes, int64_t pair_capacity,
+    bool need_pairs = true)
+{
+    if (!frame_ws || (need_pairs && pair_capacity > 0 && !pair_ws))
+        return DGMR_ERR_BAD_ARG;
+    if (frame_bytes < plan.L.bytes || (need_pairs && pair_bytes < plan.L.pair_bytes))
+        return DGMR_ERR_WORKSPACE;
+    return DGMR_OK;
+}
+
+void vm_batch_preprocess(const VmBatchPlan& plan, uint32_t* st_dev, cudaStream_t s)
+{
+    const VmBatchLayout& L = plan.L;
+    const uint32_t G = plan.tab.G;
+    cudaMemsetAsync(st_dev, 0, 16, s);
+    if (G == 0)
+        return;
+    VmPre<float> p { G, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.rects, L.rgb, L.clamped, L.depths, L.xy, L.inv_cov, L.masses,
+        L.tiles_touched, 0.f, Formulation::Opacity };
+    k_vm_batch_preprocess<<<(G + 127) / 128, 128, 0, s>>>(p, L.centroids, L.bin.depth_key, L.bin.perm, plan.tab);
+    note_launch();
+    inclusive_scan_u32(L.tiles_touched, L.point_offsets, G, L.bin.scan_tmp, s);
+}
+
+// the march's entries: every list entry is a slot of the batch
+VmMarch<float> vm_batch_march(const VmBatchLayout& L, const uint32_t* list, uint32_t* st_dev)
+{
+    VmMarch<float> a {};
+    a.ranges = L.ranges;
+    a.list = reinterpret_cast<const int32_t*>(list);
+    a.centroids = L.centroids;
+    a.inv_cov = L.inv_cov;
+    a.masses = L.masses;
+    a.rgb = L.rgb;
+    a.depths = L.depths;
+    a.stats = st_dev;
+    a.cs = const_samples<float>();
+    a.mode = DGMR_RENDER_FULL;
+    a.debug_bin = -1;
+    a.max_depth = 20.f;
+    return a;
 }
 
 } // namespace dgmr
@@ -654,6 +919,101 @@ dgmr_status dgmr_vm_backward_stored(const dgmr_scene* scene, const dgmr_camera* 
             workspace_bytes, stats, s, step_store, uint32_t(store_steps));
     return vm_backward<float>(scene, camera, cache, grad_framebuffer, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, workspace,
         workspace_bytes, stats, s, step_store, uint32_t(store_steps));
+}
+
+dgmr_status dgmr_vm_batch_workspace_size(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, int64_t pair_capacity,
+    size_t* frame_workspace_bytes, size_t* pair_workspace_bytes)
+{
+    if (!frame_workspace_bytes || !pair_workspace_bytes)
+        return DGMR_ERR_BAD_ARG;
+    static thread_local VmBatchPlan plan;
+    const dgmr_status st = make_vm_batch(scenes, n_scenes, views, n_views, nullptr, pair_capacity, nullptr, nullptr, plan);
+    if (st != DGMR_OK)
+        return st;
+    *frame_workspace_bytes = plan.L.bytes;
+    *pair_workspace_bytes = plan.L.pair_bytes;
+    return DGMR_OK;
+}
+
+dgmr_status dgmr_vm_batch_preprocess(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    static thread_local VmBatchPlan plan;
+    dgmr_status st = make_vm_batch(scenes, n_scenes, views, n_views, nullptr, 0, frame_workspace, nullptr, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = vm_batch_check_ws(plan, frame_workspace, frame_workspace_bytes, nullptr, 0, 0, false);
+    if (st != DGMR_OK)
+        return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : plan.L.stats;
+    vm_batch_preprocess(plan, st_dev, s);
+    if (plan.tab.G > 0) {
+        k_pair_count<<<1, 1, 0, s>>>(plan.L.point_offsets, plan.tab.G, 0xffffffffu, st_dev, plan.L.bin.n_sort);
+        note_launch();
+    }
+    return launch_status();
+}
+
+dgmr_status dgmr_vm_batch_forward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    static thread_local VmBatchPlan plan;
+    dgmr_status st = make_vm_batch(scenes, n_scenes, views, n_views, nullptr, pair_capacity, frame_workspace, pair_workspace, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = vm_batch_check_ws(plan, frame_workspace, frame_workspace_bytes, pair_workspace, pair_workspace_bytes, pair_capacity);
+    if (st != DGMR_OK)
+        return st;
+    for (int v = 0; v < n_views; ++v)
+        if (!views[v].framebuffer)
+            return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    VmBatchLayout& L = plan.L;
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    const uint32_t G = plan.tab.G, cap = uint32_t(pair_capacity), n_tiles = plan.tab.n_tiles;
+    vm_batch_preprocess(plan, st_dev, s);
+    const int par = run_binning_grids<float>(G, n_tiles, plan.tab.n_stiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges,
+        st_dev, num_sms(), s, true);
+    k_tile_order<<<1, 1024, 0, s>>>(L.ranges, n_tiles, L.tile_order);
+    const VmMarch<float> a = vm_batch_march(L, L.bin.pair_val[par], st_dev);
+    k_vm_march_warp<float, VmBatchFrames><<<n_tiles * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, VmBatchFrames { plan.tab }, L.tile_order);
+    note_launch(2);
+    return launch_status();
+}
+
+dgmr_status dgmr_vm_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
+    const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
+    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream)
+{
+    if (!grads)
+        return DGMR_ERR_BAD_ARG;
+    static thread_local VmBatchPlan plan;
+    dgmr_status st = make_vm_batch(scenes, n_scenes, views, n_views, grads, pair_capacity, frame_workspace, pair_workspace, plan);
+    if (st != DGMR_OK)
+        return st;
+    st = vm_batch_check_ws(plan, frame_workspace, frame_workspace_bytes, pair_workspace, pair_workspace_bytes, pair_capacity);
+    if (st != DGMR_OK)
+        return st;
+    for (int v = 0; v < n_views; ++v)
+        if (!views[v].framebuffer)
+            return DGMR_ERR_BAD_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    VmBatchLayout& L = plan.L;
+    uint32_t* st_dev = stats ? reinterpret_cast<uint32_t*>(stats) : L.stats;
+    const uint32_t G = plan.tab.G, n_tiles = plan.tab.n_tiles;
+    const uint32_t n_scene_gaussians = plan.tab.scene_off[n_scenes];
+    if (n_scene_gaussians == 0)
+        return DGMR_OK;
+    cudaMemsetAsync(L.acc, 0, size_t(G) * kVmAcc * sizeof(double), s);
+    VmMarch<float> a = vm_batch_march(L, L.bin.pair_val[tile_sort_parity(plan.tab.n_stiles)], st_dev);
+    a.acc = L.acc;
+    k_vm_march_warp_bwd<float, VmBatchFrames><<<n_tiles * (kTilePixels / kRayWarps), kRayWarps * 32, 0, s>>>(a, VmBatchFrames { plan.tab }, L.tile_order);
+    VmBwdGauss<float> state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, reinterpret_cast<const int32_t*>(L.tiles_touched), L.acc,
+        nullptr, nullptr, nullptr, nullptr, nullptr, 0.f, Formulation::Opacity };
+    k_vm_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);
+    note_launch(2);
+    return launch_status();
 }
 
 dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections)

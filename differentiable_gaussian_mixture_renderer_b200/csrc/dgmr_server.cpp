@@ -7,12 +7,16 @@
 // (optionally with its backward).  Each of n_slots slots owns a CUDA stream,
 // grow-only workspaces and an event; whenever a slot is free the queue head
 // is cut into one batch:
-//   * splat requests: as many as fit the view / scene-entry limits of one
-//     dgmr_splat_batch_forward (+ _backward) launch sequence and the HBM
-//     budget, in arrival order (a gradient request gets its own scene entry,
-//     so its gradients never mix with another request's);
-//   * a marcher request: alone (its ray march already fills the GPU), through
-//     dgmr_vm_forward_preprocess / _render_options / dgmr_vm_backward.
+//   * requests of one kind (splat or marcher) in arrival order, as many as
+//     fit the view / scene-entry limits of one batched launch sequence
+//     (dgmr_splat_batch_* or dgmr_vm_batch_*), the batch's pixel cap and the
+//     HBM budget (a gradient request gets its own scene entry, so its
+//     gradients never mix with another request's); small marcher frames gain
+//     most from sharing a launch (a few rays with long tile lists each do not
+//     fill the GPU);
+//   * a batch of one request goes through the single-frame entry points
+//     (dgmr_splat_forward / _backward; dgmr_vm_forward_preprocess /
+//     _render_options / dgmr_vm_backward): the same bits, a shorter sequence.
 // Pair capacities are learnt per (scene, resolution, renderer): the first
 // request of a key sizes itself with one synchronous read of its pair count,
 // later ones launch with the learnt capacity and no host synchronisation; a
@@ -221,9 +225,9 @@ dgmr_status learn_capacity(dgmr_server* s, const dgmr_server_request& r, int64_t
     return DGMR_OK;
 }
 
-// Tables of a splat batch: a scene entry per scene of render-only requests,
-// one of its own per gradient request.
-void splat_tables(dgmr_server* s, Slot& sl)
+// Tables of a batch: a scene entry per scene of render-only requests, one of
+// its own per gradient request.
+void batch_tables(dgmr_server* s, Slot& sl)
 {
     sl.scenes.clear();
     sl.views.clear();
@@ -293,7 +297,7 @@ dgmr_status launch(dgmr_server* s, Slot& sl)
     const dgmr_stream ds = reinterpret_cast<dgmr_stream>(cs);
     dgmr_status st = DGMR_OK;
     const dgmr_server_request& head = sl.batch.front().r;
-    if (is_march(head)) {
+    if (is_march(head) && sl.batch.size() == 1) {
         const dgmr_scene& sc = s->scenes[size_t(head.scene)];
         const int n = sc.n_gaussians, w = head.camera.width, h = head.camera.height;
         const size_t ws = dgmr_vm_workspace_size(n, w, h, sl.capacity, DGMR_F32);
@@ -326,8 +330,27 @@ dgmr_status launch(dgmr_server* s, Slot& sl)
         if (st == DGMR_OK && wants_grad(head))
             st = dgmr_splat_backward(&sc, &head.camera, head.grad_image, head.grads.sh, head.grads.weights, head.grads.centroids, head.grads.scales,
                 head.grads.rotations, sl.frame_ws.p, sl.frame_ws.bytes, sl.pair_ws.p, sl.pair_ws.bytes, sl.capacity, ds);
+    } else if (is_march(head)) {
+        batch_tables(s, sl);
+        const int32_t nv = int32_t(sl.views.size()), ns = int32_t(sl.scenes.size());
+        size_t fb = 0, pb = 0;
+        st = dgmr_vm_batch_workspace_size(sl.scenes.data(), ns, sl.views.data(), nv, sl.capacity, &fb, &pb);
+        if (st != DGMR_OK)
+            return st;
+        if (!sl.frame_ws.ensure(fb, &s->st.reallocs) || !sl.pair_ws.ensure(std::max<size_t>(pb, 1), &s->st.reallocs))
+            return DGMR_ERR_CUDA;
+        st = dgmr_vm_batch_forward(sl.scenes.data(), ns, sl.views.data(), nv, sl.frame_ws.p, sl.frame_ws.bytes, sl.pair_ws.p, sl.pair_ws.bytes,
+            sl.capacity, sl.stats_dev, ds);
+        if (st == DGMR_OK)
+            cudaMemcpyAsync(sl.stats_host, sl.stats_dev, sizeof(dgmr_frame_stats), cudaMemcpyDeviceToHost, cs);
+        bool any_grad = false;
+        for (const Request& q : sl.batch)
+            any_grad = any_grad || wants_grad(q.r);
+        if (st == DGMR_OK && any_grad)
+            st = dgmr_vm_batch_backward(sl.scenes.data(), ns, sl.views.data(), nv, sl.grads.data(), sl.frame_ws.p, sl.frame_ws.bytes, sl.pair_ws.p,
+                sl.pair_ws.bytes, sl.capacity, nullptr, ds);
     } else {
-        splat_tables(s, sl);
+        batch_tables(s, sl);
         const int32_t nv = int32_t(sl.views.size()), ns = int32_t(sl.scenes.size());
         size_t fb = 0, pb = 0;
         st = dgmr_splat_batch_workspace_size(sl.scenes.data(), ns, sl.views.data(), nv, sl.capacity, &fb, &pb);
@@ -438,11 +461,11 @@ void dispatch(dgmr_server* s)
             const bool march = is_march(q.r);
             const int64_t px = int64_t(q.r.camera.width) * int64_t(q.r.camera.height);
             if (!batch.empty()
-                && (march || is_march(batch.front().r) || int32_t(batch.size()) >= s->cfg.max_views
+                && (march != is_march(batch.front().r) || int32_t(batch.size()) >= s->cfg.max_views
                     || (s->cfg.max_batch_pixels > 0 && pixels + px > s->cfg.max_batch_pixels)))
                 break;
             const bool new_entry = wants_grad(q.r) || std::find(render_scenes.begin(), render_scenes.end(), q.r.scene) == render_scenes.end();
-            if (!march && new_entry && entries + 1 > DGMR_BATCH_MAX_SCENES)
+            if (new_entry && entries + 1 > DGMR_BATCH_MAX_SCENES)
                 break;
             size_t c = 0;
             int64_t kc = 0;

@@ -573,7 +573,8 @@ class ContinuousServer:
 # admission, the capacity learning and the re-render of overflowed batches run
 # in C++ behind dgmr_server_* (csrc/dgmr_server.cpp); Python only hands it
 # device pointers and reads completions.  It also serves vol_marcher requests
-# (kind="march"), forward and backward, one per batch.
+# (kind="march"), forward and backward, batched with other marcher requests
+# (a batch holds one kind).
 
 
 class NativeServer:

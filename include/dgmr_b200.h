@@ -224,6 +224,37 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
     int64_t pair_capacity, dgmr_stream stream);
 
+/* --------------------------------------------------- batched vol_marcher */
+
+/* Many views of one or several scenes marched by ONE launch sequence (no
+ * reference counterpart: the reference's vol_marcher.apply marches one view
+ * per call, python_bindings/vol_marcher.py:19-65, vol_marcher_forward.cu:42-503).
+ * Float32, RenderMode::Full, a scene with DGMR_FORMULATION_DEFAULT gets the
+ * marcher's default (Opacity).  Same view table, workspaces and rules as the
+ * batched splat above: each view's image is bit-identical to a
+ * dgmr_vm_forward_render of that view alone; no allocation, no host
+ * synchronisation, capturable in a CUDA graph. */
+dgmr_status dgmr_vm_batch_workspace_size(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, int64_t pair_capacity,
+    size_t* frame_workspace_bytes, size_t* pair_workspace_bytes);
+
+/* Preprocess of every view and the batch's pair count into stats->n_pairs. */
+dgmr_status dgmr_vm_batch_preprocess(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, dgmr_frame_stats* stats, dgmr_stream stream);
+
+dgmr_status dgmr_vm_batch_forward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views, void* frame_workspace,
+    size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
+/* Backward of the last batched march run in these workspaces (replaces
+ * dgmr::vol_marcher_backward per view, vol_marcher_backward.cu:53-386, the
+ * march recomputed).  Gradients of every scene entry are written, not
+ * accumulated: the sum over that entry's views with a grad_framebuffer, added
+ * in view order, each term the value the single-view dgmr_vm_backward gives.
+ * Views without a grad_framebuffer and scene entries whose grads[s].sh is NULL
+ * take no part.  stats (may be NULL) receives the step-limit flag. */
+dgmr_status dgmr_vm_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
+    const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
+    int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
+
 /* ---------------------------------------------------------- vol_raster */
 
 /* Replaces dgmr::vol_raster_forward(VolRasterForwardData&)
@@ -341,10 +372,11 @@ dgmr_status dgmr_vm_set_const_samples(int32_t n_sections, const double* sections
  * counterpart (the reference renders one view per call from its training loop
  * or viewer).  Requests wait in a queue; whenever one of n_slots slots (a CUDA
  * stream with grow-only workspaces) is free, the queue head is cut into one
- * batch: splat requests by the batched entry points above, as many as fit
- * max_views, DGMR_BATCH_MAX_SCENES scene entries and the HBM budget (arrival
- * order kept; a gradient request gets a scene entry of its own), a
- * vol_marcher request alone.  Pair capacities are learnt per (scene,
+ * batch of requests of one kind (splat or vol_marcher) for the batched entry
+ * points above, as many as fit max_views, DGMR_BATCH_MAX_SCENES scene
+ * entries, max_batch_pixels and the HBM budget (arrival order kept; a
+ * gradient request gets a scene entry of its own); a batch of one request
+ * takes the single-frame entry points.  Pair capacities are learnt per (scene,
  * resolution, renderer): the first request of such a key reads its pair count
  * back once (a host synchronisation); later ones launch without one, and a
  * batch that overflowed renders again, exactly sized, before it completes.
@@ -357,17 +389,17 @@ typedef struct dgmr_server dgmr_server;
 typedef struct dgmr_server_config {
     int32_t device; /* CUDA device of the server and its scenes */
     int32_t n_slots; /* batches in flight, one stream each (0 = 4) */
-    int32_t max_views; /* splat views per batch, <= DGMR_BATCH_MAX_VIEWS (0 = 8) */
+    int32_t max_views; /* views per batch, <= DGMR_BATCH_MAX_VIEWS (0 = 8) */
     int32_t reserved;
     size_t hbm_budget_bytes; /* device memory held for work in flight (0 = 80 % of free memory at creation) */
     double capacity_margin; /* pair capacity = pairs seen x margin + 1024 (<= 0 = 1.3; below 1 forces re-renders) */
-    int64_t max_batch_pixels; /* a splat batch takes no further view once its pixels would pass this (0 = no limit; a
+    int64_t max_batch_pixels; /* a batch takes no further view once its pixels would pass this (0 = no limit; a
                                  batch always takes one); large frames gain nothing from sharing a launch sequence */
 } dgmr_server_config;
 
 typedef enum dgmr_serve_kind {
     DGMR_SERVE_SPLAT = 0, /* splat forward (+ backward); dgmr_splat_forward / dgmr_splat_backward */
-    DGMR_SERVE_MARCH = 1, /* vol_marcher forward (+ backward), Full mode; dgmr_vm_forward_* / dgmr_vm_backward */
+    DGMR_SERVE_MARCH = 1, /* vol_marcher forward (+ backward), Full mode; dgmr_vm_forward_* / dgmr_vm_backward, or dgmr_vm_batch_* */
 } dgmr_serve_kind;
 
 typedef struct dgmr_server_request {

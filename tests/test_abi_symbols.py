@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from differentiable_gaussian_mixture_renderer_b200 import _native, build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -90,31 +92,40 @@ def _batch_tables(n_views, scene_index=0, n_scenes=1):
     return scenes, views
 
 
-def test_batch_workspace_query_without_gpu():
+@pytest.mark.parametrize("prefix", ["dgmr_splat_batch_", "dgmr_vm_batch_"])
+def test_batch_workspace_query_without_gpu(prefix):
     import ctypes as C
     lib = _native.load()
+    size = getattr(lib, prefix + "workspace_size")
     fb, pb = C.c_size_t(0), C.c_size_t(0)
     scenes, views = _batch_tables(3)
-    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 3, 1000, C.byref(fb), C.byref(pb)) == 0
+    assert size(scenes, 1, views, 3, 1000, C.byref(fb), C.byref(pb)) == 0
     three = (fb.value, pb.value)
     scenes, views = _batch_tables(6)
-    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 6, 1000, C.byref(fb), C.byref(pb)) == 0
+    assert size(scenes, 1, views, 6, 1000, C.byref(fb), C.byref(pb)) == 0
     assert fb.value > three[0]  # twice the view-Gaussian slots
-    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 6, 100000, C.byref(fb), C.byref(pb)) == 0
+    assert size(scenes, 1, views, 6, 100000, C.byref(fb), C.byref(pb)) == 0
     assert pb.value > three[1]
 
 
-def test_batch_bad_arguments_without_gpu():
+@pytest.mark.parametrize("prefix", ["dgmr_splat_batch_", "dgmr_vm_batch_"])
+def test_batch_bad_arguments_without_gpu(prefix):
     import ctypes as C
     lib = _native.load()
+    size = getattr(lib, prefix + "workspace_size")
     fb, pb = C.c_size_t(0), C.c_size_t(0)
     scenes, views = _batch_tables(2, scene_index=1)  # scene index out of range
-    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, 2, 0, C.byref(fb), C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
+    assert size(scenes, 1, views, 2, 0, C.byref(fb), C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
     scenes, views = _batch_tables(_native.BATCH_MAX_VIEWS + 1)
-    assert lib.dgmr_splat_batch_workspace_size(scenes, 1, views, _native.BATCH_MAX_VIEWS + 1, 0, C.byref(fb),
-                                               C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
+    assert size(scenes, 1, views, _native.BATCH_MAX_VIEWS + 1, 0, C.byref(fb), C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
     scenes, views = _batch_tables(2)
-    assert lib.dgmr_splat_batch_forward(scenes, 1, views, 2, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+    scenes[0].dtype = 1  # float64: batches are float32 only
+    assert size(scenes, 1, views, 2, 0, C.byref(fb), C.byref(pb)) == _native.DGMR_ERR_BAD_ARG
+    scenes, views = _batch_tables(2)
+    assert getattr(lib, prefix + "forward")(scenes, 1, views, 2, None, 0, None, 0, 0, None, None) == _native.DGMR_ERR_BAD_ARG
+    tail = [None] if prefix == "dgmr_vm_batch_" else []  # the marcher's backward also takes stats
+    assert getattr(lib, prefix + "backward")(scenes, 1, views, 2, None, None, 0, None, 0, 0, *tail,
+                                             None) == _native.DGMR_ERR_BAD_ARG
 
 
 def test_server_entry_points_without_gpu():

@@ -165,3 +165,29 @@ def test_native_server_pixel_cap_keeps_large_views_apart(cuda):
     assert max(r.batch_size for r in small) > 1
     _check_all(scenes, big + small)
     server.close()
+
+
+def test_native_server_batches_marcher_requests(cuda):
+    """Marcher requests of small views share batches (dgmr_vm_batch_*), with
+    and without gradients, across two scenes; a batch holds one kind, and
+    every result equals the plain call's."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import NativeServer, ServeRequest
+    scenes = _scenes(cuda)
+    server = NativeServer(scenes, cuda, n_slots=1, max_batch=8)
+    gen = torch.Generator(device=cuda).manual_seed(9)
+    reqs = []
+    for k in range(14):
+        cam = S.random_cameras(1, 48, 40, seed=950 + k)[0]
+        bwd = k % 3 == 1
+        g = torch.randn((3, 40, 48), device=cuda, generator=gen) if bwd else None
+        kind = "splat" if k == 6 else "march"
+        reqs.append(ServeRequest("a" if k % 2 else "b", cam, backward=bwd, grad_image=g, kind=kind))
+    for r in reqs:
+        server.submit(r)
+    server.drain()
+    assert all(r.status == 0 for r in reqs)
+    march = [r for r in reqs if r.kind == "march"]
+    assert max(r.batch_size for r in march) > 1
+    assert any(r.backward and r.batch_size > 1 for r in march)
+    _check_all(scenes, reqs)
+    server.close()
