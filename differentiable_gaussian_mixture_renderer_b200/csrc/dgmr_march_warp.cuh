@@ -33,6 +33,7 @@ struct RayWarpShared {
     T borders[kSmallSteps];
     Bin<T> bins[kSmallSteps]; // forward: (r, g, b, exp(-mass)); backward: (r, g, b, mass)
     SectionSet<kLargeSteps, T> sec;
+    Section<T> pieces[2 * kLargeSteps + 1]; // warp_put: the merged sections of one insertion
 };
 
 template <class T>
@@ -42,7 +43,10 @@ struct RayWarpSharedBwd {
     Bin<T> gbins[kSmallSteps]; // bin adjoints
     int32_t queue[32]; // pass 3: list entries waiting for a lane
     SectionSet<kLargeSteps, T> sec;
+    Section<T> pieces[2 * kLargeSteps + 1];
 };
+
+static_assert(kLargeSteps <= 16, "warp_put moves the kept sections on lanes 0-15 and writes pieces on lanes 16-31");
 
 // The gates of both passes (see ray_can_use) as a 32-bit mask per batch of 32
 // list entries, held in registers: lane l keeps the masks of batches l, l+32,
@@ -187,12 +191,87 @@ __device__ __forceinline__ bool warp_section_covered(const SectionSet<kLargeStep
     return __ballot_sync(0xffffffffu, bad) == 0u;
 }
 
-// Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
-// intersected lane-parallel, then walked in list order; lane 0 inserts them
-// into the warp's section set (in shared memory), which every lane reads.
+// SectionSet::put (dgmr_sections.h) by the whole warp, for an s that reaches
+// into [lo, hi): the overlapped range [first, last) found by ballots, the
+// merged sections by lane 0 (merge_pieces, into the warp's scratch), then the
+// kept tail moved (lanes 0-15) and the pieces written (lanes 16-31) in one
+// step -- put()'s set, bit for bit (put_by_pieces, the serial form of this
+// split, is tested against put() on random insertion sequences).  put() on one
+// lane moved every section after the insertion through a ring buffer in local
+// memory, one dependent access at a time: most of the march's pass 1.
 template <class T>
-__device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o, V3<T> d,
-    const WarpRayMasks& rm, unsigned lane)
+__device__ __forceinline__ void warp_put(SectionSet<kLargeSteps, T>& sec, Section<T>* pieces, Section<T> s, unsigned lane)
+{
+    s.start = max_f(sec.lo, s.start);
+    s.end = min_f(sec.hi, s.end);
+    const unsigned n = sec.n;
+    Section<T> my = { T(0), T(0), T(0) };
+    if (lane < n)
+        my = sec.e[lane];
+    const uint32_t after = __ballot_sync(0xffffffffu, lane < n && my.end > s.start);
+    const unsigned first = after ? unsigned(__ffs(int(after)) - 1) : n;
+    if (first >= n) {
+        if (lane == 0) {
+            if (first < kLargeSteps) {
+                sec.e[n] = s;
+                sec.n = n + 1;
+            } else {
+                sec.hi = s.start;
+            }
+        }
+        __syncwarp();
+        return;
+    }
+    const uint32_t beyond = __ballot_sync(0xffffffffu, lane >= first && lane < n && my.end > s.end);
+    unsigned last = beyond ? unsigned(__ffs(int(beyond)) - 1) : n;
+    const T last_start = __shfl_sync(0xffffffffu, my.start, int(last < n ? last : 0u));
+    if (last < n && last_start < s.end)
+        ++last;
+    unsigned np = 0, end = last;
+    if (lane == 0)
+        np = sec.merge_pieces(s, first, last, pieces, &end);
+    np = __shfl_sync(0xffffffffu, np, 0);
+    end = __shfl_sync(0xffffffffu, end, 0);
+    __syncwarp();
+    const unsigned k = lane - 16u;
+    const bool move = lane >= end && lane < n && first + np + (lane - end) < kLargeSteps;
+    const bool write = lane >= 16u && k < np && first + k < kLargeSteps;
+    Section<T> pv = { T(0), T(0), T(0) };
+    if (write)
+        pv = pieces[k];
+    __syncwarp();
+    if (move)
+        sec.e[first + np + (lane - end)] = my;
+    if (write)
+        sec.e[first + k] = pv;
+    __syncwarp();
+    if (lane == 0) {
+        const unsigned nn = min(kLargeSteps, first + np + (n - end));
+        sec.n = nn;
+        if (nn == kLargeSteps)
+            sec.hi = min_f(sec.hi, sec.e[kLargeSteps - 1].end);
+    }
+    __syncwarp();
+}
+
+// warp_put as a call: the backward march, whose loop is sensitive to its code
+// size (instruction fetch), is faster with the insertion out of line (53.2 ms
+// per c2 frame, against 58.3 inline and 54.2 with put() on lane 0); the
+// forward inlines it.
+template <class T>
+__device__ __noinline__ void warp_put_call(SectionSet<kLargeSteps, T>& sec, Section<T>* pieces, Section<T> s, unsigned lane)
+{
+    warp_put(sec, pieces, s, lane);
+}
+
+enum class PutMode { Inline, Call };
+
+// Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
+// intersected lane-parallel, then walked in list order and inserted into the
+// warp's section set (in shared memory, warp_put), which every lane reads.
+template <PutMode kPut = PutMode::Inline, class T>
+__device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, Section<T>* pieces, const VmMarch<T>& a, int32_t b, int32_t e, V3<T> o,
+    V3<T> d, const WarpRayMasks& rm, unsigned lane)
 {
     if (a.cs.n > 0) {
         if (lane == 0)
@@ -236,9 +315,10 @@ __device__ __forceinline__ void warp_collect(SectionSet<kLargeSteps, T>& sec, co
             // set unchanged for a covered one: skip both without the call
             if (sj.end <= sec.lo || sj.start >= sec.hi || warp_section_covered(sec, sj, lane))
                 continue;
-            if (lane == 0)
-                sec.put(sj);
-            __syncwarp();
+            if (kPut == PutMode::Inline)
+                warp_put(sec, pieces, sj, lane);
+            else
+                warp_put_call(sec, pieces, sj, lane);
         }
         if (stop)
             break;
@@ -379,7 +459,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
         if (lane == 0)
             sec.reset(start);
         __syncwarp();
-        warp_collect(sec, a, b, e, o, d, rm, lane);
+        warp_collect(sec, sm.pieces, a, b, e, o, d, rm, lane);
         if (lane == 0)
             sample_positions(sec, sm.borders);
         __syncwarp();
@@ -580,7 +660,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
             if (lane == 0)
                 sec.reset(start);
             __syncwarp();
-            warp_collect(sec, a, b, e, o, d, rm, lane);
+            warp_collect<PutMode::Call>(sec, sm.pieces, a, b, e, o, d, rm, lane);
             if (lane == 0)
                 sample_positions(sec, sm.borders);
             __syncwarp();

@@ -170,6 +170,98 @@ struct SectionSet {
         if (n == MAX)
             hi = min_f(hi, e[n - 1].end);
     }
+
+    // put() for an s (clipped to [lo, hi)) that overlaps the set from
+    // e[first] (the first section ending after s.start) up to e[last - 1]
+    // (last: one past the last section starting before s.end), split in two
+    // steps.  merge_pieces() walks the overlapped sections in order, as put()'s
+    // ring loop does, and returns the pieces that replace e[first, *end); the
+    // set is then e[0, first) + pieces + e[*end, n), cut to MAX sections (hi
+    // pulled in to the last end when it is full).  put()'s ring exists only to
+    // write that sequence in place; the marcher's warps instead move the kept
+    // tail and write the pieces lane-parallel (put_by_pieces is the serial
+    // form, checked against put() on random insertion sequences).
+    DGMR_HD unsigned merge_pieces(Section<T> s, unsigned first, unsigned last, Section<T>* pieces, unsigned* end) const
+    {
+        unsigned np = 0, i = first;
+        for (; i < last; ++i) {
+            const Section<T> head = e[i];
+            if (head.end <= s.start) {
+                pieces[np++] = head;
+                continue;
+            }
+            if (head.start >= s.end)
+                break;
+            Section<T> p[3];
+            combine(head, s, p);
+            if (p[0].delta_t == p[1].delta_t) {
+                p[1].start = p[0].start;
+                p[0].end = p[0].start;
+            }
+            s = p[2];
+            if (p[0].end - p[0].start <= T(0)) {
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                pieces[np++] = p[1];
+            } else {
+                pieces[np++] = p[0];
+                if (p[1].delta_t == p[2].delta_t) {
+                    s.start = p[1].start;
+                    continue;
+                }
+                pieces[np++] = p[1];
+            }
+        }
+        *end = i;
+        if (s.end - s.start > T(0))
+            pieces[np++] = s;
+        return np;
+    }
+
+    DGMR_HD void put_by_pieces(Section<T> s)
+    {
+        if (s.end <= lo || s.start >= hi)
+            return;
+        s.start = max_f(lo, s.start);
+        s.end = min_f(hi, s.end);
+        unsigned first = n;
+        for (unsigned i = 0; i < n; ++i)
+            if (e[i].end > s.start) {
+                first = i;
+                break;
+            }
+        if (first >= n) {
+            if (first < MAX)
+                e[n++] = s;
+            else
+                hi = s.start;
+            return;
+        }
+        unsigned last = n;
+        for (unsigned i = first; i < n; ++i)
+            if (e[i].end > s.end) {
+                last = i;
+                break;
+            }
+        if (last < n && e[last].start < s.end)
+            ++last;
+        Section<T> pieces[2 * MAX + 1], tail[MAX];
+        unsigned end = last;
+        const unsigned np = merge_pieces(s, first, last, pieces, &end);
+        const unsigned nt = n - end;
+        for (unsigned i = 0; i < nt; ++i)
+            tail[i] = e[end + i];
+        unsigned w = first;
+        for (unsigned i = 0; i < np && w < MAX; ++i)
+            e[w++] = pieces[i];
+        for (unsigned i = 0; i < nt && w < MAX; ++i)
+            e[w++] = tail[i];
+        n = w;
+        if (n == MAX)
+            hi = min_f(hi, e[n - 1].end);
+    }
 };
 
 // marching_steps.h:202-220: NS monotone sample positions (all zero for an empty set)

@@ -365,7 +365,64 @@ long check_unchanged(unsigned seed, int trials, long* covered)
     return bad;
 }
 
+// The same kind of sequences, inserted into two sets: one by put(), one by
+// put_by_pieces() (the merged pieces written after the kept prefix, then the
+// kept tail, cut to the capacity).  After every insertion both sets must be
+// the same bits.  Returns the mismatches; *merges counts insertions that went
+// through the merge (not an append or a full-set cut).
+template <class T, unsigned MAX>
+long check_by_pieces(unsigned seed, int trials, long* merges)
+{
+    std::mt19937 rng(seed);
+    long bad = 0, merged = 0;
+    for (int trial = 0; trial < trials; ++trial) {
+        dgmr::SectionSet<MAX, T> a, b;
+        a.reset(T(rng() % 3) * T(0.5));
+        b = a;
+        const int n_put = 5 + int(rng() % 80);
+        for (int k = 0; k < n_put; ++k) {
+            T c = T(std::uniform_real_distribution<double>(0.0, 10.0)(rng));
+            T w = T(0.02 + std::uniform_real_distribution<double>(0.0, 2.0)(rng));
+            if (rng() % 2) {
+                c = T(int(c * T(4))) / T(4);
+                w = T(1 + rng() % 8) / T(4);
+            }
+            const T dt = (rng() % 3 == 0) ? T(1 + rng() % 4) / T(32) : w / T(31);
+            const dgmr::Section<T> s { c - w, c + w, dt };
+            const unsigned n0 = a.n;
+            a.put(s);
+            b.put_by_pieces(s);
+            if (a.n != n0 || a.n == MAX)
+                ++merged;
+            bool same = a.n == b.n && std::memcmp(&a.lo, &b.lo, sizeof(T)) == 0 && std::memcmp(&a.hi, &b.hi, sizeof(T)) == 0;
+            for (unsigned q = 0; same && q < a.n; ++q)
+                same = std::memcmp(&a.e[q], &b.e[q], sizeof(dgmr::Section<T>)) == 0;
+            if (!same) {
+                ++bad;
+                b = a; // continue the sequence from the reference state
+            }
+        }
+    }
+    *merges = merged;
+    return bad;
+}
+
 } // namespace
+
+extern "C" long kat_section_by_pieces_f32(unsigned seed, int trials, long* merges)
+{
+    long m1 = 0, m2 = 0;
+    const long bad = check_by_pieces<float, 16>(seed, trials, &m1) + check_by_pieces<float, 4>(seed + 7, trials, &m2);
+    *merges = m1 + m2;
+    return bad;
+}
+extern "C" long kat_section_by_pieces_f64(unsigned seed, int trials, long* merges)
+{
+    long m1 = 0, m2 = 0;
+    const long bad = check_by_pieces<double, 16>(seed, trials, &m1) + check_by_pieces<double, 4>(seed + 7, trials, &m2);
+    *merges = m1 + m2;
+    return bad;
+}
 
 extern "C" long kat_section_unchanged_f32(unsigned seed, int trials, long* covered) { return check_unchanged<float>(seed, trials, covered); }
 extern "C" long kat_section_unchanged_f64(unsigned seed, int trials, long* covered) { return check_unchanged<double>(seed, trials, covered); }

@@ -371,6 +371,21 @@ def test_insertions_claimed_unchanged_leave_the_set_unchanged(shim, suffix):
     assert covered.value > 100000
 
 
+@pytest.mark.parametrize("suffix", ["f32", "f64"])
+def test_insertion_by_pieces_equals_put(shim, suffix):
+    """The marcher's warps insert a section as SectionSet::merge_pieces plus a
+    lane-parallel move of the kept tail (put_by_pieces is its serial form)
+    instead of put()'s ring walk.  On random insertion sequences (capacities 16
+    and 4, so full sets and cuts are common) both must leave the same set, bit
+    for bit, after every insertion."""
+    f = getattr(shim, f"kat_section_by_pieces_{suffix}")
+    f.restype = C.c_long
+    f.argtypes = [C.c_uint, C.c_int, C.POINTER(C.c_long)]
+    merges = C.c_long(0)
+    assert f(5, 20000, C.byref(merges)) == 0
+    assert merges.value > 1000000
+
+
 def test_range_specialised_exp_is_bit_identical(shim):
     """The blend's exp_f_nonpos must return exp_f's bits for every input."""
     f = shim.kat_exp_nonpos_mismatches
