@@ -142,6 +142,29 @@ def test_render_server_results_are_not_reused(cuda, to_host):
     assert torch.equal(again.image.to(cuda) if to_host else again.image, fb)
 
 
+@pytest.mark.parametrize("to_host", [False, True])
+def test_render_server_rerenders_overflowed_frames(cuda, to_host):
+    """RenderServer with learnt capacities far too small: the frames launched
+    with them overflow, render again exactly sized before they complete, and
+    every result equals its frame rendered alone (a grown capacity serves the
+    requests launched after it)."""
+    from differentiable_gaussian_mixture_renderer_b200.serving import RenderServer, Request
+    scenes = _scenes(cuda)
+    server = RenderServer(scenes, cuda, n_slots=3)
+    reqs = [Request("ab"[k % 2], S.random_cameras(1, *RES[k % 2], seed=500 + k)[0], to_host=to_host) for k in range(9)]
+    for r in reqs:
+        server.capacity[(r.scene_id, r.camera.width, r.camera.height)] = 16
+    for r in reqs:
+        server.submit(r)
+    server.drain()
+    assert reqs[0].rerendered and server.rerenders >= 2  # the first frame of each key at least
+    assert len(server.completed) == len(reqs)
+    for k, req in enumerate(reqs):
+        fb = _render_alone(scenes[req.scene_id], req.camera)
+        assert torch.equal(req.image.to(cuda) if to_host else req.image, fb), f"request {k}"
+        assert req.meta["n_pairs"] > 16
+
+
 def _render_alone(scene, cam):
     fb, _ = splat.splat_forward(scene.shs, scene.weights, scene.centroids, scene.scales, scene.rotations, cam.view,
                                 cam.proj, cam.campos, (0.0, 0.0, 0.0), cam.width, cam.height, cam.tan_fovx,
