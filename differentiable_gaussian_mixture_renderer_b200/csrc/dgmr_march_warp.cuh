@@ -256,8 +256,8 @@ __device__ __forceinline__ void warp_put(SectionSet<kLargeSteps, T>& sec, Sectio
 
 // warp_put as a call: the backward march, whose loop is sensitive to its code
 // size (instruction fetch), is faster with the insertion out of line (53.2 ms
-// per c2 frame, against 58.3 inline and 54.2 with put() on lane 0); the
-// forward inlines it.
+// per frame at 100k Gaussians, 512^2, against 58.3 inline and 54.2 with put()
+// on lane 0); the forward inlines it.
 template <class T>
 __device__ __noinline__ void warp_put_call(SectionSet<kLargeSteps, T>& sec, Section<T>* pieces, Section<T> s, unsigned lane)
 {
@@ -265,6 +265,48 @@ __device__ __noinline__ void warp_put_call(SectionSet<kLargeSteps, T>& sec, Sect
 }
 
 enum class PutMode { Inline, Call };
+
+// sample_positions (marching_steps.h:202-220) by the warp, in the form of
+// sample_positions_by_sections (dgmr_sections.h): lane j < n runs section j's
+// chain -- counting its samples, then, after a prefix over the counts, writing
+// them behind the samples of the sections before it -- and the lanes fill the
+// rest with the last section's end.  The same positions, bit for bit, with the
+// longest section's chain as the critical path instead of all 128 samples.
+template <class T>
+__device__ __forceinline__ void warp_sample_positions(const SectionSet<kLargeSteps, T>& d, T* out, unsigned lane)
+{
+    const unsigned n = d.n;
+    if (n == 0) {
+        for (unsigned k = lane; k < kSmallSteps; k += 32)
+            out[k] = T(0);
+        __syncwarp();
+        return;
+    }
+    const unsigned len = lane < n ? section_samples<kSmallSteps>(d, lane) : 0u;
+    unsigned incl = len;
+#pragma unroll
+    for (unsigned o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o)
+            incl += t;
+    }
+    const unsigned off = 1u + incl - len; // out[0] is the first section's start
+    const unsigned filled = 1u + __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0)
+        out[0] = d.e[0].start;
+    if (lane < n) {
+        const T end = d.e[lane].end, dt = d.e[lane].delta_t;
+        T v = lane == 0 ? d.e[0].start : d.e[lane - 1].end;
+        for (unsigned k = 0; k < len && off + k < kSmallSteps; ++k) {
+            v = min_f(end, v + dt);
+            out[off + k] = v;
+        }
+    }
+    const T last = d.e[n - 1].end;
+    for (unsigned k = filled + lane; k < kSmallSteps; k += 32)
+        out[k] = last;
+    __syncwarp();
+}
 
 // Pass 1 (vol_marcher_forward.cu:351-403): the masked entries of a batch are
 // intersected lane-parallel, then walked in list order and inserted into the
@@ -460,9 +502,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 8 : 2) k_vm_m
             sec.reset(start);
         __syncwarp();
         warp_collect(sec, sm.pieces, a, b, e, o, d, rm, lane);
-        if (lane == 0)
-            sample_positions(sec, sm.borders);
-        __syncwarp();
+        warp_sample_positions(sec, sm.borders, lane);
         if (step < a.store_steps) {
             // keep this step's samples for the backward (coalesced: 32 lanes x 4 rounds)
             const size_t ray = frames.px_base(view) + size_t(py) * cam.W + px, rays = frames.rays();
@@ -661,9 +701,7 @@ __global__ void __launch_bounds__(kRayWarps * 32, sizeof(T) == 4 ? 6 : 2) k_vm_m
                 sec.reset(start);
             __syncwarp();
             warp_collect<PutMode::Call>(sec, sm.pieces, a, b, e, o, d, rm, lane);
-            if (lane == 0)
-                sample_positions(sec, sm.borders);
-            __syncwarp();
+            warp_sample_positions(sec, sm.borders, lane);
             n_sections = int(sec.n);
         }
         Bin<T> acc[kRayRounds];

@@ -23,12 +23,6 @@ constexpr float kRelevanceSigma = 3.f; // vol_marcher.h:65
 constexpr float kFilterSD = 0.55f; // vol_marcher.h:60
 constexpr unsigned kMaxLargeSteps = 4096; // a ray that makes no progress stops here and flags it
 
-template <unsigned MAX, class T>
-__device__ __forceinline__ void sample_positions(const SectionSet<MAX, T>& d, T* out)
-{
-    sample_positions_n<kSmallSteps>(d, out);
-}
-
 template <class T>
 struct alignas(sizeof(T) * 4) Bin {
     T r, g, b, m;

@@ -285,5 +285,56 @@ DGMR_HD void sample_positions_n(const SectionSet<MAX, T>& d, T* out)
     }
 }
 
+// The same positions, section by section: section j's samples are the chain
+// v <- min(end_j, v + delta_j) from the previous section's end (from e[0].start
+// for j = 0) until v reaches end_j -- sample_positions_n advances to the next
+// section exactly there -- and the last section's chain continues to NS.  So
+// each section's chain can run on its own lane, placed after the samples of
+// the sections before it (the marcher's warps do that); this is the serial
+// form, checked against sample_positions_n on random section sets.
+// section_samples returns how many samples section j places (the last: its
+// steps until v reaches its end; every count capped at NS - 1).
+template <unsigned NS, unsigned MAX, class T>
+DGMR_HD unsigned section_samples(const SectionSet<MAX, T>& d, unsigned j)
+{
+    const T end = d.e[j].end, dt = d.e[j].delta_t;
+    T v = j == 0 ? d.e[0].start : d.e[j - 1].end;
+    unsigned len = 0;
+    while (len < NS - 1) {
+        v = min_f(end, v + dt);
+        ++len;
+        if (v == end)
+            break;
+    }
+    return len;
+}
+
+template <unsigned NS, unsigned MAX, class T>
+DGMR_HD void sample_positions_by_sections(const SectionSet<MAX, T>& d, T* out)
+{
+    if (d.n == 0) {
+        for (unsigned i = 0; i < NS; ++i)
+            out[i] = T(0);
+        return;
+    }
+    out[0] = d.e[0].start;
+    unsigned off = 1;
+    T v = out[0];
+    for (unsigned j = 0; j < d.n && off < NS; ++j) {
+        const T end = d.e[j].end, dt = d.e[j].delta_t;
+        const unsigned len = section_samples<NS>(d, j);
+        v = j == 0 ? d.e[0].start : d.e[j - 1].end;
+        for (unsigned k = 0; k < len && off + k < NS; ++k) {
+            v = min_f(end, v + dt);
+            out[off + k] = v;
+        }
+        off += len;
+    }
+    // the last section's chain after it reached its end: min(end, end + dt) = end
+    const T last = d.e[d.n - 1].end;
+    for (unsigned i = off; i < NS; ++i)
+        out[i] = last;
+}
+
 
 } // namespace dgmr

@@ -28,7 +28,7 @@ struct SplatLayout {
     int32_t* ranges;
     float* final_T;
     int32_t* n_contrib;
-    float* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3)
+    double* grad_acc; // [N,9]: xy(2) conic(3) opacity rgb(3), summed over pixels in double
     float4* blend_rec; // [N,2]: (x, y, a, c), (2b, opacity, q_cut, 0) -- the blend's 32-byte record
     uint32_t* tile_order; // [tiles] launch order of the per-tile kernels, heaviest first
     uint32_t* tile_cost; // [tiles] predicted blend cost of each tile as a bucket, 0 = heaviest
@@ -55,7 +55,7 @@ inline SplatLayout splat_layout_n(uint32_t N, uint32_t n_tiles, size_t n_px, uin
     L.ranges = c.take<int32_t>(size_t(n_tiles) * 2);
     L.final_T = c.take<float>(n_px);
     L.n_contrib = c.take<int32_t>(n_px);
-    L.grad_acc = c.take<float>(size_t(N) * 9);
+    L.grad_acc = c.take<double>(size_t(N) * 9);
     L.blend_rec = c.take<float4>(size_t(N) * 2);
     L.tile_order = c.take<uint32_t>(n_tiles);
     L.tile_cost = c.take<uint32_t>(n_tiles);
@@ -417,7 +417,7 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], int l
 // instead of four (backward 2-3 % shorter at 1080p/1M and 200k/1024^2).
 template <class Frames>
 __global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
-    const float4* __restrict__ rec, const float* __restrict__ rgb, float* __restrict__ acc, const uint32_t* __restrict__ tile_order,
+    const float4* __restrict__ rec, const float* __restrict__ rgb, double* __restrict__ acc, const uint32_t* __restrict__ tile_order,
     const __grid_constant__ Frames frames)
 {
     __shared__ float4 s_r0[256]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
@@ -507,11 +507,14 @@ __global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __re
             if (__any_sync(0xffffffffu, any)) {
                 // reduce-scatter of the 9 partials over the warp (16 shuffles, not
                 // 9 x 5): lane l ends with the warp's sum of partial slot(l) and
-                // the lanes of slots 0..8 add them, one atomic each
+                // the lanes of slots 0..8 add them, one atomic each.  The totals
+                // over warps are double: in float, the order in which the
+                // atomics of many cancelling terms land moved single elements by
+                // ~1e-3 relative from run to run at 200k Gaussians, 1024^2.
                 float w = warp_reduce_scatter9(v, lane);
                 const int slot = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
                 if ((lane & 1) == 0 && slot < 9 && w != 0.f)
-                    atomicAdd(acc + size_t(s_id[j]) * 9 + slot, w);
+                    atomicAdd(acc + size_t(s_id[j]) * 9 + slot, double(w));
             }
         }
     }
@@ -527,7 +530,7 @@ struct SplatBwdGauss {
     const float* rotations;
     const uint8_t* clamped;
     const uint32_t* tiles_touched;
-    const float* acc;
+    const double* acc;
     float* g_sh;
     float* g_weights;
     float* g_centroids;
@@ -558,7 +561,10 @@ __device__ __forceinline__ void bwd_gaussian_one(const SplatBwdGauss& p, const C
 {
     if (p.tiles_touched[o] == 0)
         return;
-    const float* a = p.acc + size_t(o) * 9;
+    float a[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        a[k] = float(p.acc[size_t(o) * 9 + k]);
     const V3<float> mu = { p.centroids[3 * i], p.centroids[3 * i + 1], p.centroids[3 * i + 2] };
     const V3<float> sc = mul3(V3<float> { p.scales[3 * i], p.scales[3 * i + 1], p.scales[3 * i + 2] }, cam.cov_scale_multiplier);
     const float* q = p.rotations + 4 * size_t(i);
@@ -955,7 +961,7 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
-    cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(float), s);
+    cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(double), s);
     k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order,
         single_frame(cam, nullptr, L, grad_framebuffer));
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
@@ -1170,7 +1176,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
     if (n_scene_gaussians == 0)
         return DGMR_OK;
     const int par = tile_sort_parity(plan.tab.n_stiles);
-    cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(float), s);
+    cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(double), s);
     k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order, plan.tab);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
         nullptr, Formulation::Ots };

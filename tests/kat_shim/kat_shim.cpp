@@ -407,7 +407,48 @@ long check_by_pieces(unsigned seed, int trials, long* merges)
     return bad;
 }
 
+// Sample positions of random section sets (built by random insertion
+// sequences; some with very small steps, so that the 128-sample cap cuts a
+// section short) by sample_positions_n and by sample_positions_by_sections:
+// the same bits.  Returns the mismatching sets; *sets counts those compared.
+template <class T>
+long check_samples_by_sections(unsigned seed, int trials, long* sets)
+{
+    std::mt19937 rng(seed);
+    long bad = 0, n_sets = 0;
+    for (int trial = 0; trial < trials; ++trial) {
+        dgmr::SectionSet<16, T> sec;
+        sec.reset(T(rng() % 3) * T(0.5));
+        const bool fine = rng() % 4 == 0;
+        const int n_put = 1 + int(rng() % 40);
+        for (int k = 0; k < n_put; ++k) {
+            T c = T(std::uniform_real_distribution<double>(0.0, 10.0)(rng));
+            T w = T(0.02 + std::uniform_real_distribution<double>(0.0, 2.0)(rng));
+            if (rng() % 2) {
+                c = T(int(c * T(4))) / T(4);
+                w = T(1 + rng() % 8) / T(4);
+            }
+            T dt = (rng() % 3 == 0) ? T(1 + rng() % 4) / T(32) : w / T(31);
+            if (fine)
+                dt = dt / T(16);
+            sec.put(dgmr::Section<T> { c - w, c + w, dt });
+            if (rng() % 3 == 0 || k == n_put - 1) {
+                T a[128], b[128];
+                dgmr::sample_positions_n<128>(sec, a);
+                dgmr::sample_positions_by_sections<128>(sec, b);
+                ++n_sets;
+                bad += std::memcmp(a, b, sizeof a) == 0 ? 0 : 1;
+            }
+        }
+    }
+    *sets = n_sets;
+    return bad;
+}
+
 } // namespace
+
+extern "C" long kat_samples_by_sections_f32(unsigned seed, int trials, long* sets) { return check_samples_by_sections<float>(seed, trials, sets); }
+extern "C" long kat_samples_by_sections_f64(unsigned seed, int trials, long* sets) { return check_samples_by_sections<double>(seed, trials, sets); }
 
 extern "C" long kat_section_by_pieces_f32(unsigned seed, int trials, long* merges)
 {

@@ -386,6 +386,21 @@ def test_insertion_by_pieces_equals_put(shim, suffix):
     assert merges.value > 1000000
 
 
+@pytest.mark.parametrize("suffix", ["f32", "f64"])
+def test_sample_positions_by_sections_equal_the_serial_walk(shim, suffix):
+    """The marcher's warps place a large step's 128 samples section by section
+    (each section's chain on its own lane, after the samples of the sections
+    before it; sample_positions_by_sections is the serial form).  On random
+    section sets, some with steps so small that the 128-sample cap cuts a
+    section short, the positions must be sample_positions_n's, bit for bit."""
+    f = getattr(shim, f"kat_samples_by_sections_{suffix}")
+    f.restype = C.c_long
+    f.argtypes = [C.c_uint, C.c_int, C.POINTER(C.c_long)]
+    sets = C.c_long(0)
+    assert f(13, 30000, C.byref(sets)) == 0
+    assert sets.value > 100000
+
+
 def test_range_specialised_exp_is_bit_identical(shim):
     """The blend's exp_f_nonpos must return exp_f's bits for every input."""
     f = shim.kat_exp_nonpos_mismatches
