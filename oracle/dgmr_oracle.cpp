@@ -222,8 +222,8 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
         const T w = s.weights[i];
         const V3<T> sc = mul(load3(s.scales, size_t(i)), s.cov_scale_multiplier);
         const Gaussian2d<T> g = splat(form_or(Formulation::Ots), w, mu, sc, s.rotations + 4 * size_t(i), cam, T(0.3f));
-        const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(T(3.f) * dgmr_fm::sqrt_f(g.cov.v[0])));
-        const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(T(3.f) * dgmr_fm::sqrt_f(g.cov.v[2])));
+        const int ex = ofm::to_int_rz(ofm::ceil_f(T(3.f) * ofm::sqrt_f(g.cov.v[0])));
+        const int ey = ofm::to_int_rz(ofm::ceil_f(T(3.f) * ofm::sqrt_f(g.cov.v[2])));
         rects[2 * i] = ex;
         rects[2 * i + 1] = ey;
         const URect r = get_rect(float(g.centroid.x), float(g.centroid.y), ex, ey, gx, gy);
@@ -235,7 +235,7 @@ void splat_preprocess(const SceneIn<T>& s, T* rgb, uint8_t* clamped, T* depths, 
         xy[2 * i + 1] = g.centroid.y;
         depths[i] = length(sub(campos, mu));
         const V3<T> v = sub(mu, campos);
-        const V3<T> dir = mul(v, T(1) / dgmr_fm::sqrt_f(dot(v, v)));
+        const V3<T> dir = mul(v, T(1) / ofm::sqrt_f(dot(v, v)));
         V3<T> sh16[16];
         load_sh16(s, unsigned(i), T(0), sh16);
         bool cl[3];
@@ -399,17 +399,17 @@ void vm_preprocess(const SceneIn<T>& s, VmCache<T>& c)
             const T sv = T(-2) * ofm::log_f(isoline / wt);
             if (sv <= T(0))
                 return T(0);
-            return dgmr_fm::sqrt_f(sv * var);
+            return ofm::sqrt_f(sv * var);
         };
-        const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[0], T(1.f / 255.f))));
-        const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso(g.weight, g.cov.v[2], T(1.f / 255.f))));
+        const int ex = ofm::to_int_rz(ofm::ceil_f(iso(g.weight, g.cov.v[0], T(1.f / 255.f))));
+        const int ey = ofm::to_int_rz(ofm::ceil_f(iso(g.weight, g.cov.v[2], T(1.f / 255.f))));
         if (std::is_same<T, float>::value && audit().on.load(std::memory_order_relaxed)) {
             const auto iso_l = [](T wt, T var, T isoline) {
                 const T sv = T(-2) * std::log(isoline / wt);
-                return sv <= T(0) ? T(0) : dgmr_fm::sqrt_f(sv * var);
+                return sv <= T(0) ? T(0) : ofm::sqrt_f(sv * var);
             };
-            const int exl = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso_l(g.weight, g.cov.v[0], T(1.f / 255.f))));
-            const int eyl = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(iso_l(g.weight, g.cov.v[2], T(1.f / 255.f))));
+            const int exl = ofm::to_int_rz(ofm::ceil_f(iso_l(g.weight, g.cov.v[0], T(1.f / 255.f))));
+            const int eyl = ofm::to_int_rz(ofm::ceil_f(iso_l(g.weight, g.cov.v[2], T(1.f / 255.f))));
             const T rx = iso(g.weight, g.cov.v[0], T(1.f / 255.f)), ry = iso(g.weight, g.cov.v[2], T(1.f / 255.f));
             audit_note(AUDIT_RECT, true, ex == exl, double(rx), std::round(double(rx)));
             audit_note(AUDIT_RECT, true, ey == eyl, double(ry), std::round(double(ry)));
@@ -483,7 +483,7 @@ Ray<T> pixel_ray(const T* inv_proj, V3<T> campos, unsigned px, unsigned py, unsi
     v.y = v.y / v.w;
     v.z = v.z / v.w;
     const V3<T> dvec = { v.x - campos.x, v.y - campos.y, v.z - campos.z };
-    const T il = T(1) / dgmr_fm::sqrt_f(dot(dvec, dvec));
+    const T il = T(1) / ofm::sqrt_f(dot(dvec, dvec));
     Ray<T> r;
     r.o = campos;
     r.d = mul(dvec, il);
@@ -507,7 +507,7 @@ void collect_sections(DensityArray<N_LARGE, T>& sections, const Ray<T>& ray, con
         for (int j = 0; j < 6; ++j)
             Q.v[j] = inv_cov[6 * size_t(id) + j];
         const Gauss1d<T> g = intersect_with_ray_inv_C(mu, Q, ray);
-        const T sd = dgmr_fm::sqrt_f(g.C);
+        const T sd = ofm::sqrt_f(g.C);
         if (sections.end() < depths[id])
             break;
         const T mor = g.weight * masses[id];
@@ -520,7 +520,7 @@ void collect_sections(DensityArray<N_LARGE, T>& sections, const Ray<T>& ray, con
             continue;
         if (g.C <= T(0))
             continue;
-        if (dgmr_fm::isnan_f(g.centre))
+        if (ofm::isnan_f(g.centre))
             continue;
         const T start = g.centre - sd * T(RELEVANCE_SIGMA);
         const T end = g.centre + sd * T(RELEVANCE_SIGMA);
@@ -586,7 +586,7 @@ void vm_march(const SceneIn<T>& s, const int32_t* list, VmCache<T>& c, int32_t* 
                         colour = { mass * md, mass * md, mass * md };
                         if (mass == T(0))
                             colour = { T(0), T(1), T(0) };
-                        if (dgmr_fm::isnan_f(mass))
+                        if (ofm::isnan_f(mass))
                             colour = { T(1), T(0), T(0.5) };
                         if (mass < T(0))
                             colour = { T(1), T(0), T(0) };
@@ -904,7 +904,7 @@ void vm_backward_impl(const SceneIn<T>& s, const VmCache<T>& c, const int32_t* l
             const T i2 = integrate_exponential_cov2(cov2d);
             g_w = g_mass * i2;
             const T g_i2 = g_mass * w;
-            const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dcov)) : T(0);
+            const T g_det = (dcov > T(0)) ? g_i2 * two_pi<T>() / (T(2) * ofm::sqrt_f(dcov)) : T(0);
             g_cov2d = { { g_det * cov2d.v[2], g_det * T(-2) * cov2d.v[1], g_det * cov2d.v[0] } };
         } else if (f == Formulation::Mass) {
             g_w = g_mass;
@@ -963,7 +963,7 @@ void grad_splat(Formulation f, T weight, V3<T> mu, V3<T> s, const T* q, const Ca
         // weight2d = w sqrt(max(eps, det c / det(c + filter)))
         const T dcv = det2(c), dn = det2(cov2);
         const T r = dcv / dn;
-        const T factor = dgmr_fm::sqrt_f(max_f(T(0.000025), r));
+        const T factor = ofm::sqrt_f(max_f(T(0.000025), r));
         *g_weight = *g_weight + g_w2 * factor;
         if (T(0.000025) < r) {
             const T g_r = (g_w2 * weight) / (T(2) * factor);
@@ -988,7 +988,7 @@ void grad_splat(Formulation f, T weight, V3<T> mu, V3<T> s, const T* q, const Ca
         g_detSJ = g_w2 * weight * A / i2;
         const T g_A = g_w2 * weight * detSJ / i2;
         const T g_i2 = -g_w2 * weight * detSJ * A / (i2 * i2);
-        const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * dgmr_fm::sqrt_f(dc)) : T(0);
+        const T g_dc = (dc > T(0)) ? g_i2 * two_pi<T>() / (T(2) * ofm::sqrt_f(dc)) : T(0);
         g_cov.v[0] = g_cov.v[0] + g_dc * cov2.v[2];
         g_cov.v[1] = g_cov.v[1] - g_dc * T(2) * cov2.v[1];
         g_cov.v[2] = g_cov.v[2] + g_dc * cov2.v[0];
@@ -1178,7 +1178,7 @@ void splat_backward_impl(const SceneIn<T>& s, const T* rgb, const uint8_t* clamp
             g_q);
         // colour
         const V3<T> v = sub(mu, campos);
-        const T vl = dgmr_fm::sqrt_f(dot(v, v));
+        const T vl = ofm::sqrt_f(dot(v, v));
         const V3<T> dir = mul(v, T(1) / vl);
         V3<T> sh16[16];
         load_sh16(s, unsigned(i), T(0), sh16);
@@ -1287,8 +1287,8 @@ void vr_preprocess(const SceneIn<float>& s, VrCache& c)
         filtered.v[5] = filtered.v[5] + fks2;
         // weight_to_mass<Ots> of the scales plus the squared filter size (vol_raster_forward.cu:106)
         c.masses[i] = weight_to_mass(form_or(Formulation::Ots), w, V3<float> { sc.x + fks2, sc.y + fks2, sc.z + fks2 }, g.cov);
-        const int ex = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[0])));
-        const int ey = dgmr_fm::to_int_rz(dgmr_fm::ceil_f(3.f * dgmr_fm::sqrt_f(g.cov.v[2])));
+        const int ex = ofm::to_int_rz(ofm::ceil_f(3.f * ofm::sqrt_f(g.cov.v[0])));
+        const int ey = ofm::to_int_rz(ofm::ceil_f(3.f * ofm::sqrt_f(g.cov.v[2])));
         c.rects[2 * i] = ex;
         c.rects[2 * i + 1] = ey;
         const URect r = get_rect(g.centroid.x, g.centroid.y, ex, ey, gx, gy);
@@ -1300,7 +1300,7 @@ void vr_preprocess(const SceneIn<float>& s, VrCache& c)
         c.xy[2 * i + 1] = g.centroid.y;
         c.depths[i] = length(sub(campos, mu));
         const V3<float> v = sub(mu, campos);
-        const V3<float> dir = mul(v, 1.f / dgmr_fm::sqrt_f(dot(v, v)));
+        const V3<float> dir = mul(v, 1.f / ofm::sqrt_f(dot(v, v)));
         V3<float> sh16[16];
         load_sh16(s, unsigned(i), 0.f, sh16);
         bool cl[3];
@@ -1333,7 +1333,7 @@ Ray<float> vr_pixel_ray(const float* inv_proj, V3<float> campos, unsigned px, un
     v.y = v.y / v.w;
     v.z = v.z / v.w;
     const V3<float> dvec = { v.x - campos.x, v.y - campos.y, v.z - campos.z };
-    const float il = 1.f / dgmr_fm::sqrt_f(dot(dvec, dvec));
+    const float il = 1.f / ofm::sqrt_f(dot(dvec, dvec));
     Ray<float> r;
     r.o = campos;
     r.d = mul(dvec, il);
@@ -1372,7 +1372,7 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                         continue;
                     if (g.C + 0.f <= 0.f)
                         continue;
-                    sizer.add(mor, g.centre, dgmr_fm::sqrt_f(g.C + 0.f));
+                    sizer.add(mor, g.centre, ofm::sqrt_f(g.C + 0.f));
                     if (sizer.saturated())
                         break;
                 }
@@ -1387,10 +1387,10 @@ void vr_render(const SceneIn<float>& s, const VrCache& c, const int32_t* ranges,
                     const Gauss1d<float> g = intersect_with_ray_inv_C(load3(s.centroids, id), Q, ray);
                     const float centre = g.centre;
                     const float variance = g.C + 0.f;
-                    const float sd = dgmr_fm::sqrt_f(variance);
+                    const float sd = ofm::sqrt_f(variance);
                     const float inv_sd = 1.f / sd;
                     const float weight = g.weight * c.masses[id];
-                    if (variance <= 0.f || dgmr_fm::isnan_f(variance) || dgmr_fm::isnan_f(weight) || weight > 100000.f)
+                    if (variance <= 0.f || ofm::isnan_f(variance) || ofm::isnan_f(weight) || weight > 100000.f)
                         continue;
                     if (weight * integrate_normalised_inv_SD(centre, inv_sd, 0.f, sizer.upper(VR_BINS - 1)) <= 0.001f)
                         continue;
@@ -1761,9 +1761,9 @@ void orc_fmath_f32(int which, const float* x, float* y, int n)
 {
     for (int i = 0; i < n; ++i)
         switch (which) { // 0-2: the shared fixed-sequence routines; 3-5: the host libm
-        case 0: y[i] = dgmr_fm::exp_f(x[i]); break;
-        case 1: y[i] = dgmr_fm::log_f(x[i]); break;
-        case 2: y[i] = dgmr_fm::erf_f(x[i]); break;
+        case 0: y[i] = ofm::exp_f(x[i]); break;
+        case 1: y[i] = ofm::log_f(x[i]); break;
+        case 2: y[i] = ofm::erf_f(x[i]); break;
         case 3: y[i] = std::exp(x[i]); break;
         case 4: y[i] = std::log(x[i]); break;
         default: y[i] = std::erf(x[i]); break;

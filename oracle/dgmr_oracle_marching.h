@@ -173,14 +173,14 @@ inline void sample_gaussian(T mass, V3<T> rgb, V3<T> pos, const S3<T>& inv_cov, 
 {
     const Gauss1d<T> g = intersect_with_ray_inv_C(pos, inv_cov, ray);
     const T centre = g.centre;
-    const T sd = dgmr_fm::sqrt_f(g.C);
+    const T sd = ofm::sqrt_f(g.C);
     const T inv_sd = T(1) / sd;
     const T mass_on_ray = g.weight * mass;
-    if (dgmr_fm::isnan_f(centre))
+    if (ofm::isnan_f(centre))
         return;
     if (mass_on_ray < T(1.0f / 255.f) || mass_on_ray > T(1000))
         return;
-    if (sd <= T(0.0001) || dgmr_fm::isnan_f(sd) || dgmr_fm::isnan_f(mass_on_ray) || mass_on_ray > T(100000))
+    if (sd <= T(0.0001) || ofm::isnan_f(sd) || ofm::isnan_f(mass_on_ray) || mass_on_ray > T(100000))
         return;
     const T mass_in_bins = mass_on_ray * integrate_normalised_inv_SD(centre, inv_sd, borders[0], borders[NB]);
     if (mass_in_bins < T(0.0001f))
@@ -266,7 +266,7 @@ inline void grad_intersect_with_ray_inv_C(V3<T> mu, const S3<T>& Q, const Ray<T>
     const T e = k - b * centre;
     const T detQ = det_sym3(Q);
     const T r = detQ / a;
-    const T sr = dgmr_fm::sqrt_f(r);
+    const T sr = ofm::sqrt_f(r);
     const T weight = (sr * T(0.15915494309189533577)) * ofm::exp_f(T(-0.5) * e);
 
     const T g_e = g_weight * (T(-0.5) * weight);
@@ -306,14 +306,14 @@ inline void grad_sample_gaussian(T mass, V3<T> rgb, V3<T> pos, const S3<T>& inv_
     const Gauss1d<T> g = intersect_with_ray_inv_C(pos, inv_cov, ray);
     const T centre = g.centre;
     const T var = g.C;
-    const T sd = dgmr_fm::sqrt_f(var);
+    const T sd = ofm::sqrt_f(var);
     const T inv_sd = T(1) / sd;
     const T mass_on_ray = g.weight * mass;
-    if (dgmr_fm::isnan_f(centre))
+    if (ofm::isnan_f(centre))
         return;
     if (mass_on_ray < T(1.0f / 255.f) || mass_on_ray > T(1000))
         return;
-    if (sd <= T(0.0001) || dgmr_fm::isnan_f(sd) || dgmr_fm::isnan_f(mass_on_ray) || mass_on_ray > T(100000))
+    if (sd <= T(0.0001) || ofm::isnan_f(sd) || ofm::isnan_f(mass_on_ray) || mass_on_ray > T(100000))
         return;
     const T mass_in_bins = mass_on_ray * integrate_normalised_inv_SD(centre, inv_sd, borders[0], borders[NB]);
     if (mass_in_bins < T(0.0001f))

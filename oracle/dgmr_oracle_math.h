@@ -14,7 +14,8 @@
 // Matrices use glm's memory layout: m[c*4 + r] is row r, column c.
 // Operation order is fixed and written out; the CUDA kernels follow the same
 // order so float results agree bit for bit (both sides are compiled without
-// FMA contraction; transcendental functions come from dgmr_fmath.h).
+// FMA contraction; the oracle's exp / log / erf are its own restatement of
+// the same published methods, dgmr_oracle_fmath.h).
 #pragma once
 
 #include <atomic>
@@ -22,12 +23,13 @@
 #include <cstdint>
 #include <cstring>
 
-#include "../differentiable_gaussian_mixture_renderer_b200/csrc/dgmr_fmath.h"
+#include "dgmr_oracle_fmath.h"
 
-// The oracle's exp / log / erf.  By default the fixed-sequence routines of
-// dgmr_fmath.h, which the CUDA kernels use too, so that every threshold
-// decision (alpha >= 1/255, section mass >= 1/255, the ceil of a
-// log-derived radius) comes out the same on both sides.  Built with
+// The oracle's exp / log / erf.  By default its own fixed-sequence routines
+// (dgmr_oracle_fmath.h): the CUDA kernels follow the same published methods
+// with the same roundings, so that every threshold decision (alpha >= 1/255,
+// section mass >= 1/255, the ceil of a log-derived radius) comes out the same
+// on both sides.  Built with
 // -DDGMR_ORACLE_LIBM, the host C library's expf / logf / erff instead: the
 // nearest stand-in here for the CUDA expf / erff the reference calls, used
 // only to measure how far that choice moves images and decisions.
@@ -40,11 +42,14 @@ inline double exp_f(double x) { return std::exp(x); }
 inline double log_f(double x) { return std::log(x); }
 inline double erf_f(double x) { return std::erf(x); }
 #else
-using dgmr_fm::erf_f;
-using dgmr_fm::exp_f;
-using dgmr_fm::log_f;
+using ofm_rs::erf_f;
+using ofm_rs::exp_f;
+using ofm_rs::log_f;
 #endif
-using dgmr_fm::sqrt_f;
+using ofm_rs::ceil_f;
+using ofm_rs::isnan_f;
+using ofm_rs::sqrt_f;
+using ofm_rs::to_int_rz;
 } // namespace ofm
 
 namespace orc {
@@ -80,9 +85,9 @@ inline void audit_note(AuditKind k, bool shared, bool libm, double value, double
         a.near[k].fetch_add(1, std::memory_order_relaxed);
 }
 
-using dgmr_fm::clamp_f;
-using dgmr_fm::max_f;
-using dgmr_fm::min_f;
+using ofm_rs::clamp_f;
+using ofm_rs::max_f;
+using ofm_rs::min_f;
 
 template <class T>
 struct V2 {
@@ -125,7 +130,7 @@ inline V3<T> mul(V3<T> a, T s) { return { a.x * s, a.y * s, a.z * s }; }
 template <class T>
 inline T dot(V3<T> a, V3<T> b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 template <class T>
-inline T length(V3<T> a) { return dgmr_fm::sqrt_f(dot(a, a)); }
+inline T length(V3<T> a) { return ofm::sqrt_f(dot(a, a)); }
 
 template <class T>
 inline int sym3_idx(int i, int j)
@@ -301,7 +306,7 @@ template <class T>
 inline T integrate_exponential3(V3<T> s) { return ((two_pi_pow_1_5<T>() * s.x) * s.y) * s.z; }
 // stroke::gaussian::integrate_exponential(Cov2): integral of exp(-x^T C^-1 x / 2)
 template <class T>
-inline T integrate_exponential_cov2(const S2<T>& c) { return two_pi<T>() * dgmr_fm::sqrt_f(det2(c)); }
+inline T integrate_exponential_cov2(const S2<T>& c) { return two_pi<T>() * ofm::sqrt_f(det2(c)); }
 
 // math.h:112-155
 template <class T>
@@ -423,7 +428,7 @@ inline Gaussian2d<T> splat(Formulation f, T weight, V3<T> centroid, V3<T> s, con
         S2<T> nc = g.cov;
         nc.v[0] = nc.v[0] + filter;
         nc.v[2] = nc.v[2] + filter;
-        const T factor = dgmr_fm::sqrt_f(max_f(T(0.000025), det2(g.cov) / det2(nc)));
+        const T factor = ofm::sqrt_f(max_f(T(0.000025), det2(g.cov) / det2(nc)));
         g.cov = nc;
         g.weight = weight * factor;
         break;
@@ -597,10 +602,10 @@ inline URect get_rect(float px, float py, int ex, int ey, unsigned gx, unsigned 
 {
     const auto clampu = [](unsigned g, int v) { return v < 0 ? 0u : (unsigned(v) < g ? unsigned(v) : g); };
     URect r;
-    r.x0 = clampu(gx, dgmr_fm::to_int_rz((px - float(ex)) / 16.0f));
-    r.y0 = clampu(gy, dgmr_fm::to_int_rz((py - float(ey)) / 16.0f));
-    r.x1 = clampu(gx, dgmr_fm::to_int_rz((((px + float(ex)) + 16.0f) - 1.0f) / 16.0f));
-    r.y1 = clampu(gy, dgmr_fm::to_int_rz((((py + float(ey)) + 16.0f) - 1.0f) / 16.0f));
+    r.x0 = clampu(gx, ofm::to_int_rz((px - float(ex)) / 16.0f));
+    r.y0 = clampu(gy, ofm::to_int_rz((py - float(ey)) / 16.0f));
+    r.x1 = clampu(gx, ofm::to_int_rz((((px + float(ex)) + 16.0f) - 1.0f) / 16.0f));
+    r.y1 = clampu(gy, ofm::to_int_rz((((py + float(ey)) + 16.0f) - 1.0f) / 16.0f));
     return r;
 }
 
@@ -648,7 +653,7 @@ inline Gauss1d<T> intersect_with_ray_inv_C(V3<T> mu, const S3<T>& Q, const Ray<T
     g.C = T(1) / a;
     g.centre = b / a;
     const T e = k - b * g.centre;
-    g.weight = (dgmr_fm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * ofm::exp_f(T(-0.5) * e);
+    g.weight = (ofm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * ofm::exp_f(T(-0.5) * e);
     return g;
 }
 
@@ -665,7 +670,7 @@ inline T intersect_weight_libm(V3<T> mu, const S3<T>& Q, const Ray<T>& ray)
     const T k = dot(c, Qc);
     const T centre = b / a;
     const T e = k - b * centre;
-    return (dgmr_fm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * std::exp(T(-0.5) * e);
+    return (ofm::sqrt_f(det_sym3(Q) / a) * T(0.15915494309189533577)) * std::exp(T(-0.5) * e);
 }
 
 // cdf of N(c, 1/inv_sd^2) at x

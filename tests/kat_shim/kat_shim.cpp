@@ -5,7 +5,11 @@
 // __host__ __device__ math on the host.  The oracle's separate restatement
 // of the bin sizer and bin fit (oracle/dgmr_oracle_volume_fit.h) is exposed
 // beside them, so the same tests pin both and a randomised comparison checks
-// that the two codings agree bit for bit.
+// that the two codings agree bit for bit.  The same holds for the elementary
+// functions: the product's csrc/dgmr_fmath.h and the oracle's own
+// oracle/dgmr_oracle_fmath.h are compared over a sweep of float bit patterns.
+#include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <random>
@@ -488,6 +492,59 @@ extern "C" long kat_exp_nonpos_mismatches(float lo, float hi, unsigned stride)
             u = 0u;
         std::memcpy(&x, &u, sizeof(u));
     }
+    return bad;
+}
+
+// The product's exp / log / erf (csrc/dgmr_fmath.h) against the oracle's own
+// coding of the same methods (oracle/dgmr_oracle_fmath.h): every float bit
+// pattern u = first, first + stride, ... below 2^32 (both signs, every
+// exponent, NaNs and infinities included), plus every pattern of [lo, hi]
+// exhaustively.  which: 0 exp, 1 log, 2 erf.  Returns the count of inputs
+// whose results differ in any bit (NaN payloads aside); *checked = inputs seen.
+extern "C" long kat_fmath_mismatches(int which, unsigned first, unsigned stride, float lo, float hi, long* checked)
+{
+    auto same = [](float a, float b) {
+        if (a != a && b != b)
+            return true;
+        return std::memcmp(&a, &b, sizeof(float)) == 0;
+    };
+    auto eval = [which](float x, float* a, float* b) {
+        switch (which) {
+        case 0:
+            *a = dgmr_fm::exp_f(x);
+            *b = ofm_rs::exp_f(x);
+            break;
+        case 1:
+            *a = dgmr_fm::log_f(x);
+            *b = ofm_rs::log_f(x);
+            break;
+        default:
+            *a = dgmr_fm::erf_f(x);
+            *b = ofm_rs::erf_f(x);
+            break;
+        }
+    };
+    long bad = 0, n = 0;
+    for (uint64_t u = first; u < (uint64_t(1) << 32); u += stride) {
+        const uint32_t w = uint32_t(u);
+        float x, a, b;
+        std::memcpy(&x, &w, sizeof(x));
+        eval(x, &a, &b);
+        bad += !same(a, b);
+        ++n;
+    }
+    if (lo <= hi) {
+        for (float x = lo;;) {
+            float a, b;
+            eval(x, &a, &b);
+            bad += !same(a, b);
+            ++n;
+            if (x >= hi)
+                break;
+            x = std::nextafter(x, hi);
+        }
+    }
+    *checked = n;
     return bad;
 }
 

@@ -1,8 +1,9 @@
 """What sharing exp / log / erf between the CUDA kernels and the oracle hides.
 
-The kernels and the default oracle build use the same fixed-sequence float
-routines (csrc/dgmr_fmath.h), so GPU and oracle take every threshold decision
-the same way.  The reference calls CUDA's expf / erff instead.  The oracle is
+The kernels and the default oracle build use fixed-sequence float routines
+that give the same bits (csrc/dgmr_fmath.h, and the oracle's own coding of
+the same methods, oracle/dgmr_oracle_fmath.h), so GPU and oracle take every
+threshold decision the same way.  The reference calls CUDA's expf / erff instead.  The oracle is
 therefore also built with the host libm's expf / logf / erff (the nearest
 stand-in available here), and these tests measure the difference:
 
@@ -14,7 +15,7 @@ stand-in available here), and these tests measure the difference:
   (marcher) and isoline-radius ceil (marcher rectangle) decision taken with
   both functions on the same argument: none flips, and the decisions within
   16 float ulps of their threshold -- the only ones any exp / log within 16
-  ulps of the shared routines could flip -- are a few per ten million.
+  ulps of the fixed-sequence routines could flip -- are a few per ten million.
 Measured when written: splat image 1.8e-7, marcher crop 5.8e-6; 4 of 13.6M
 alpha decisions, 4 of 12.2M section-mass decisions and 4 of 200k radii near
 their thresholds, no flips.

@@ -8,6 +8,10 @@
   conservation of create_approximation, volume_integrate against a 1e6-step
   numeric integral within 1/256 (product header dgmr_volume_fit.h).
 * unittests/raster_bin_sizer.cpp -- the RasterBinSizer property sections.
+
+The elementary functions are pinned here too: the oracle's own exp / log / erf
+(oracle/dgmr_oracle_fmath.h) and the CUDA library's (csrc/dgmr_fmath.h) are
+separate codings of the same published methods and must agree bit for bit.
 """
 import ctypes as C
 import json
@@ -353,6 +357,39 @@ def test_deterministic_exp_log_erf_error_bounds():
     refe = np.array([math.erf(float(v)) for v in xe])
     gote = O.fmath("erf", xe).astype(np.float64)
     assert np.max(np.abs(gote - refe)) < 2.5e-7  # Abramowitz & Stegun 7.1.26 bound 1.5e-7 plus float rounding
+
+
+# windows swept ulp by ulp: the 1/255 cutoffs (exp near ln(1/255), log near
+# 255), the branch points of each routine (log's sqrt(2) split and 1, erf's
+# series / Hastings switch at 1 and its saturation at 3.92) and the ends of
+# exp's range (its reduction's rounding switch at +-ln2/2, gradual underflow,
+# the 2^127 split, overflow).  Every float input was also compared once, all
+# 2^32 of them, with no difference.
+FMATH_WINDOWS = {
+    "exp": [(-5.6, -5.5), (-0.36, -0.33), (0.33, 0.36), (-88.0, -86.9), (-104.1, -103.9), (88.3, 88.75)],
+    "log": [(0.99, 1.01), (1.41, 1.42), (0.70, 0.71), (254.0, 256.0), (1e-39, 2e-38)],
+    "erf": [(-1.01, -0.99), (0.99, 1.01), (3.91, 3.93), (-3.93, -3.91)],
+}
+
+
+@pytest.mark.parametrize("which", ["exp", "log", "erf"])
+def test_oracle_and_product_elementary_functions_agree(shim, which):
+    """The oracle compiles no product source: its exp / log / erf are its own
+    coding (oracle/dgmr_oracle_fmath.h) of the methods csrc/dgmr_fmath.h
+    follows.  Every 257th float bit pattern (both signs, every exponent, NaN,
+    infinities; ~16.7M inputs) and every float of the windows above must give
+    the same bits from both (NaN payloads aside)."""
+    f = shim.kat_fmath_mismatches
+    f.restype = C.c_long
+    f.argtypes = [C.c_int, C.c_uint, C.c_uint, C.c_float, C.c_float, C.POINTER(C.c_long)]
+    w = {"exp": 0, "log": 1, "erf": 2}[which]
+    n = C.c_long(0)
+    assert f(w, 0, 257, 1.0, 0.0, C.byref(n)) == 0
+    total = n.value
+    for lo, hi in FMATH_WINDOWS[which]:
+        assert f(w, 0, 0xFFFFFFFF, lo, hi, C.byref(n)) == 0, (lo, hi)
+        total += n.value
+    assert total > 16_000_000
 
 
 @pytest.mark.parametrize("suffix", ["f32", "f64"])
