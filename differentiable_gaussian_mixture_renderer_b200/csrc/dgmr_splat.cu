@@ -277,8 +277,11 @@ __global__ void __launch_bounds__(256, 5) k_splat_blend(const int32_t* __restric
     const FrameRef f = frames.frame(tile);
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u);
-    const unsigned py = ty * kTile + (threadIdx.x >> 4);
+    // warp w covers the 8x4 pixel block (8 (w & 1), 4 (w >> 1)) of the tile:
+    // a compact footprint, so fewer records pass some lane's cutoff than over
+    // a 16x2 strip (a record no lane needs costs one vote)
+    const unsigned px = tx * kTile + 8u * ((threadIdx.x >> 5) & 1u) + (threadIdx.x & 7u);
+    const unsigned py = ty * kTile + 4u * (threadIdx.x >> 6) + ((threadIdx.x >> 3) & 3u);
     PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py < H) };
     const bool in0 = !p0.done;
     int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
@@ -432,7 +435,9 @@ __global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __re
         return;
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
-    const unsigned px = tx * kTile + (threadIdx.x & 15u), py = ty * kTile + (threadIdx.x >> 4);
+    // the forward's pixel blocks: warp w covers the 8x4 block (8 (w & 1), 4 (w >> 1))
+    const unsigned px = tx * kTile + 8u * ((threadIdx.x >> 5) & 1u) + (threadIdx.x & 7u);
+    const unsigned py = ty * kTile + 4u * (threadIdx.x >> 6) + ((threadIdx.x >> 3) & 3u);
     const bool inside = px < W && py < H;
     const int32_t b = ranges[2 * tile];
     const size_t pix = size_t(py) * W + px;
