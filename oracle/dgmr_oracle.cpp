@@ -1770,6 +1770,19 @@ void orc_fmath_f32(int which, const float* x, float* y, int n)
         }
 }
 
+// math.h:112-155 larger2 / smaller2 (the Ots / Ols mass formulations), for
+// the reference's known answers (unittests/math.cpp:96-117): which = 0 larger2,
+// 1 smaller2; n vec3 in v, n vec2 out.
+void orc_pick2_f32(int which, const float* v, float* out, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        const V3<float> a { v[3 * i], v[3 * i + 1], v[3 * i + 2] };
+        const V2<float> r = which == 0 ? larger2(a) : smaller2(a);
+        out[2 * i] = r.x;
+        out[2 * i + 1] = r.y;
+    }
+}
+
 // Decision audit: on = 1 resets the counters and starts counting, 0 stops;
 // out10 = (seen, flipped, near threshold) of alpha, section-mass and rect
 // decisions, then the marcher's bin fills.

@@ -118,6 +118,8 @@ def _declare(L):
     L.orc_set_const_samples.argtypes = [C.c_int, _f64p]
     L.orc_fmath_f32.restype = None
     L.orc_fmath_f32.argtypes = [C.c_int, _f32p, _f32p, C.c_int]
+    L.orc_pick2_f32.restype = None
+    L.orc_pick2_f32.argtypes = [C.c_int, _f32p, _f32p, C.c_int]
 
 
 def num_threads() -> int:
@@ -329,6 +331,14 @@ def fmath(which: str, x, libm: bool = False):
     y = np.zeros_like(x)
     lib().orc_fmath_f32({"exp": 0, "log": 1, "erf": 2}[which] + (3 if libm else 0), x, y, x.size)
     return y
+
+
+def pick2(which: str, v):
+    """math.h:112-155 on float rows of 3: "larger" or "smaller" two components."""
+    v = _c(np.asarray(v, np.float32).reshape(-1, 3), np.float32)
+    out = np.zeros((v.shape[0], 2), np.float32)
+    lib().orc_pick2_f32({"larger": 0, "smaller": 1}[which], v, out, v.shape[0])
+    return out
 
 
 @contextlib.contextmanager

@@ -8,6 +8,10 @@
   conservation of create_approximation, volume_integrate against a 1e6-step
   numeric integral within 1/256 (product header dgmr_volume_fit.h).
 * unittests/raster_bin_sizer.cpp -- the RasterBinSizer property sections.
+* unittests/math.cpp -- larger2 / smaller2 (the two largest / smallest scales,
+  used by the Ots / Ols mass formulations).  Its other cases test
+  rotation_matrix_from, orient_filter_kernel and
+  gaussian_to_point_distance_bounds, which nothing on the rendering path calls.
 
 The elementary functions are pinned here too: the oracle's own exp / log / erf
 (oracle/dgmr_oracle_fmath.h) and the CUDA library's (csrc/dgmr_fmath.h) are
@@ -338,6 +342,33 @@ def test_oracle_and_product_bin_fits_agree(shim):
     """200k random four-channel bin fits: all five parameters of every
     channel, bit for bit."""
     assert shim.kat_compare_fits(11, 200000) == 0
+
+
+# ---------------------------------------------------------------- math.h helpers
+@pytest.mark.parametrize("which,inputs", [
+    # unittests/math.cpp:96-106: every permutation of (1, 2, 3) -> {2, 3}
+    ("larger", [(1, 2, 3), (1, 3, 2), (2, 3, 1), (2, 1, 3), (3, 2, 1), (3, 1, 2)]),
+    # unittests/math.cpp:107-117: every permutation of (2, 3, 4) -> {2, 3}
+    ("smaller", [(4, 2, 3), (4, 3, 2), (2, 3, 4), (2, 4, 3), (3, 2, 4), (3, 4, 2)]),
+])
+def test_larger2_smaller2_kats(which, inputs):
+    """The oracle's larger2 / smaller2 (math.h:112-155) on the reference's
+    known answers: the pair is (2, 3) in either order."""
+    out = O.pick2(which, inputs)
+    for row in out:
+        assert sorted(row.tolist()) == [2.0, 3.0]
+
+
+def test_larger2_smaller2_pick_the_extremes():
+    """On random scale triples (ties included) larger2 drops a smallest
+    component and smaller2 a largest one, as the Ots / Ols formulations use
+    them (math.h:284-293)."""
+    rng = np.random.default_rng(5)
+    v = rng.integers(1, 5, size=(4000, 3)).astype(np.float32)
+    lg, sm = O.pick2("larger", v), O.pick2("smaller", v)
+    srt = np.sort(v, axis=1)
+    assert np.array_equal(np.sort(lg, axis=1), srt[:, 1:])
+    assert np.array_equal(np.sort(sm, axis=1), srt[:, :2])
 
 
 # ---------------------------------------------------------------- elementary functions
