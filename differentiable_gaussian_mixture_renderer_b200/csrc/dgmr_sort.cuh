@@ -221,14 +221,23 @@ static __global__ void k_radix_hist(uint32_t* __restrict__ keys, const uint32_t*
             (&h[0][0])[i] = 0;
         __syncthreads();
         const uint32_t base = tile * kSortTile + warp * (kSortTile / kSortWarps);
-        // per-warp histograms keep shared-memory atomic contention inside one warp
+        // the tile's keys (and live flags) are all requested before the first
+        // is used, so their latencies overlap; per-warp histograms keep
+        // shared-memory atomic contention inside one warp
+        uint32_t kv[kSortItemsPerThread], lv[kSortItemsPerThread];
+#pragma unroll
+        for (int r = 0; r < kSortItemsPerThread; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
+            kv[r] = idx < n ? keys[idx] : 0u;
+            lv[r] = (rb && idx < n) ? live[idx] : 0u;
+        }
 #pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
             const uint32_t idx = base + r * 32 + lane;
             if (idx < n) {
-                uint32_t k = keys[idx];
+                uint32_t k = kv[r];
                 if (rb) {
-                    k = live[idx] ? k - kmin : kspan;
+                    k = lv[r] ? k - kmin : kspan;
                     keys[idx] = k;
                 }
                 atomicAdd(&h[warp][(k >> shift) & mask], 1u);
@@ -290,6 +299,24 @@ static __global__ void k_radix_scan_rows(uint32_t* __restrict__ hist, const uint
         digit_total[blockIdx.x] = carry;
 }
 
+// Lanes of the warp holding the same digit as this lane (a digit of at most
+// 8 bits; lanes without an item match each other only): one ballot per digit
+// bit, on the ALU pipe, instead of __match_any_sync.
+__device__ __forceinline__ uint32_t warp_same_digit(uint32_t d, bool valid, uint32_t mask)
+{
+    const uint32_t v = __ballot_sync(0xffffffffu, valid);
+    uint32_t peers = valid ? v : ~v;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        if (!((mask >> b) & 1u))
+            break; // mask is 2^bits - 1, the same on every lane
+        const bool one = valid && ((d >> b) & 1u);
+        const uint32_t ones = __ballot_sync(0xffffffffu, one);
+        peers &= one ? ones : ~ones;
+    }
+    return peers;
+}
+
 // Stable scatter: warp w of a tile owns a contiguous 256-item slice and ranks
 // its items in order with __match_any_sync, so equal digits keep input order.
 // The tile is first rearranged in shared memory into digit order, then written
@@ -310,9 +337,23 @@ static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __
     const uint32_t n = dev_count(n_dev, n_static, capacity);
     if (pass_is_copy(range, shift)) {
         // every key has digit 0 here and in every later pass: the order stays and
-        // no later pass reads the keys, so only the values move
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-            vals_out[i] = vals_in[i];
+        // no later pass reads the keys, so only the values move (eight loads in
+        // flight per thread before the stores)
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 8u * stride) {
+            uint32_t v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint32_t i = i0 + uint32_t(r) * stride;
+                v[r] = i < n ? vals_in[i] : 0u;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const uint32_t i = i0 + uint32_t(r) * stride;
+                if (i < n)
+                    vals_out[i] = v[r];
+            }
+        }
         return;
     }
     const uint32_t n_tiles = (n + kSortTile - 1) / kSortTile;
@@ -343,20 +384,27 @@ static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __
     __syncthreads();
 
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        for (int i = threadIdx.x; i < kSortWarps * kSortBins; i += kSortThreads)
-            (&wcount[0][0])[i] = 0;
-        __syncthreads();
+        // every global load of the tile is issued before the first is used:
+        // this tile's start of digit threadIdx.x, then the keys and values
+        const uint32_t hrow = hist[threadIdx.x * tile_stride + tile];
         const uint32_t tile_base = tile * kSortTile;
         const uint32_t base = tile_base + warp * (kSortTile / kSortWarps);
         uint32_t k[kSortItemsPerThread], v[kSortItemsPerThread], rank[kSortItemsPerThread];
 #pragma unroll
         for (int r = 0; r < kSortItemsPerThread; ++r) {
             const uint32_t idx = base + r * 32 + lane;
+            k[r] = idx < n ? keys_in[idx] : 0u;
+            v[r] = idx < n ? vals_in[idx] : 0u;
+        }
+        for (int i = threadIdx.x; i < kSortWarps * kSortBins; i += kSortThreads)
+            (&wcount[0][0])[i] = 0;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kSortItemsPerThread; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
             const bool valid = idx < n;
-            k[r] = valid ? keys_in[idx] : 0u;
-            v[r] = valid ? vals_in[idx] : 0u;
             const uint32_t d = valid ? ((k[r] >> shift) & mask) : 0xffffffffu;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t peers = warp_same_digit(d, valid, mask);
             rank[r] = (valid ? wcount[warp][d] : 0u) + __popc(peers & lt_mask);
             __syncwarp();
             if (valid && lane == __ffs(peers) - 1)
@@ -374,7 +422,7 @@ static __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __
                 wcount[w][d] = count;
                 count += t;
             }
-            gbase[d] = dbase[d] + hist[d * tile_stride + tile];
+            gbase[d] = dbase[d] + hrow;
         }
         lbase[threadIdx.x] = block_excl_scan(count);
         __syncthreads();
