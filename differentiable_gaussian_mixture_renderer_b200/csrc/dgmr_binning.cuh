@@ -185,6 +185,18 @@ struct SingleGrid {
     __device__ __forceinline__ TileGrid super_grid(uint32_t) const { return TileGrid { gx, gy, 0u, 0u }; }
 };
 
+// Two consecutive values in one load (the address is aligned to their size).
+__device__ __forceinline__ V2<float> load_pair(const float* p)
+{
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    return V2<float> { v.x, v.y };
+}
+__device__ __forceinline__ V2<double> load_pair(const double* p)
+{
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    return V2<double> { v.x, v.y };
+}
+
 // A Gaussian's tile rectangle (util.h:42-52 on the cached rect and centroid),
 // checked against its tile count; empty when the count is 0 or disagrees.
 template <class T>
@@ -192,9 +204,13 @@ __device__ __forceinline__ TileRect checked_rect(uint32_t g, const uint32_t* __r
     const T* __restrict__ xy, const TileGrid& tg, uint32_t* __restrict__ stats)
 {
     TileRect r = { 0, 0, 0, 0 };
+    // the count, rectangle and centre are requested together (8-byte loads for
+    // the pairs), not one after the other
     const uint32_t c = tiles_touched[g];
+    const int2 e = reinterpret_cast<const int2*>(rects)[g];
+    const V2<T> p = load_pair(xy + 2 * size_t(g));
     if (c > 0) {
-        r = get_rect(float(xy[2 * g]), float(xy[2 * g + 1]), rects[2 * g], rects[2 * g + 1], tg.gx, tg.gy);
+        r = get_rect(float(p.x), float(p.y), e.x, e.y, tg.gx, tg.gy);
         if ((r.x1 - r.x0) * (r.y1 - r.y0) != c) {
             flag_bounds(stats, 0x22u);
             r = { 0, 0, 0, 0 };
@@ -698,24 +714,35 @@ static __global__ void k_tile_ranges(const uint32_t* __restrict__ tiles_sorted, 
     uint32_t* __restrict__ stats, int shift)
 {
     const uint32_t n = *n_dev;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        const uint32_t cur = tiles_sorted[idx] >> shift;
-        const uint32_t prev_t = idx ? tiles_sorted[idx - 1] >> shift : 0u;
-        if (cur >= n_tiles || prev_t >= n_tiles) {
-            flag_bounds(stats, 0x25u);
-            continue;
+    // four items per thread and step, every load issued before the first is used
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4u * stride) {
+        uint32_t cur_v[4], prev_v[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t idx = i0 + uint32_t(r) * stride;
+            cur_v[r] = idx < n ? tiles_sorted[idx] >> shift : 0u;
+            prev_v[r] = (idx < n && idx) ? tiles_sorted[idx - 1] >> shift : 0u;
         }
-        if (idx == 0)
-            ranges[2 * cur] = 0;
-        else {
-            const uint32_t prev = prev_t;
-            if (cur != prev) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t idx = i0 + uint32_t(r) * stride;
+            if (idx >= n)
+                break;
+            const uint32_t cur = cur_v[r], prev = prev_v[r];
+            if (cur >= n_tiles || prev >= n_tiles) {
+                flag_bounds(stats, 0x25u);
+                continue;
+            }
+            if (idx == 0)
+                ranges[2 * cur] = 0;
+            else if (cur != prev) {
                 ranges[2 * prev + 1] = int32_t(idx);
                 ranges[2 * cur] = int32_t(idx);
             }
+            if (idx == n - 1)
+                ranges[2 * cur + 1] = int32_t(n);
         }
-        if (idx == n - 1)
-            ranges[2 * cur + 1] = int32_t(n);
     }
 }
 

@@ -171,12 +171,23 @@ __device__ __forceinline__ bool pass_is_copy(const uint32_t* range, int shift)
 static __global__ void k_key_range(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ live, uint32_t n, uint32_t* __restrict__ range)
 {
     uint32_t lo = 0xffffffffu, hi = 0u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (live[i]) {
-            const uint32_t k = keys[i];
-            lo = k < lo ? k : lo;
-            hi = k > hi ? k : hi;
+    // four items per thread and step, every load issued before the first is used
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4u * stride) {
+        uint32_t kv[4], lv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t i = i0 + uint32_t(r) * stride;
+            kv[r] = i < n ? keys[i] : 0u;
+            lv[r] = i < n ? live[i] : 0u;
         }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (lv[r]) {
+                lo = kv[r] < lo ? kv[r] : lo;
+                hi = kv[r] > hi ? kv[r] : hi;
+            }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));

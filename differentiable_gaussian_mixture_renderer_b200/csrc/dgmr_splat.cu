@@ -692,11 +692,27 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_blend_tile_order(const int
             const float x0 = float(tx * kTile), y0 = float(ty * kTile);
             const int n = min(e - b, kSample);
             float hit[4] = { 0.f, 0.f, 0.f, 0.f };
-            for (int k = lane; k < n; k += 32) {
-                const uint32_t g = list[b + k];
-                if (g >= N)
+            // the sample's list entries, then their records, all requested
+            // before the first is used (kSample / 32 entries per lane)
+            constexpr int kPerLane = kSample / 32;
+            uint32_t gs[kPerLane];
+#pragma unroll
+            for (int i = 0; i < kPerLane; ++i) {
+                const int k = lane + 32 * i;
+                gs[i] = k < n ? list[b + k] : 0xffffffffu;
+            }
+            float4 r0s[kPerLane], r1s[kPerLane];
+#pragma unroll
+            for (int i = 0; i < kPerLane; ++i) {
+                const size_t g = gs[i] < N ? gs[i] : 0u;
+                r0s[i] = rec[2 * g];
+                r1s[i] = rec[2 * g + 1];
+            }
+#pragma unroll
+            for (int i = 0; i < kPerLane; ++i) {
+                if (gs[i] >= N)
                     continue;
-                const float4 r0 = rec[2 * size_t(g)], r1 = rec[2 * size_t(g) + 1];
+                const float4 r0 = r0s[i], r1 = r1s[i];
 #pragma unroll
                 for (int qd = 0; qd < 4; ++qd) {
                     const float dx = x0 + ((qd & 1) ? 12.f : 4.f) - r0.x;
