@@ -515,7 +515,7 @@ def _gpu_common():
 def measure_batched(dev, steps: int = 5, warmup: int = 3):
     """3 resident scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras each,
     resolutions cycling 256x256 / 800x600 / 1920x1080, forward + backward of
-    all 48 views per step: autotuned batch depth under CUDA graphs, against the
+    all 48 views per step: autotuned batch depth and blend block under CUDA graphs, against the
     plain per-view calls (forward, pair count read back, backward)."""
     import torch
     from differentiable_gaussian_mixture_renderer_b200 import scene as S
@@ -532,7 +532,7 @@ def measure_batched(dev, steps: int = 5, warmup: int = 3):
             views.append((k, S.random_cameras(1, w, h, seed=100 * j + v)[0]))
     px = sum(c.width * c.height for _, c in views)
     r = BatchRenderer(scenes, dev)
-    best, timings = autotune(r, views, depths=(1, 4, 16, 48), backward=True, reps=2)
+    (best, block), timings = autotune(r, views, depths=(1, 4, 16, 48), backward=True, reps=2)
     plans = [r.capture(r.plan(c, backward=True), backward=True) for c in chunks(views, best)]
     gen = torch.Generator(device=dev).manual_seed(2)
     for p in plans:
@@ -578,8 +578,9 @@ def measure_batched(dev, steps: int = 5, warmup: int = 3):
     plain_ms = sum(lat)
     return {"workload": "3 scenes (50k, 300k, 1.5M Gaussians) x 16 random cameras (r=2.5-4), resolutions cycling "
                         "256x256 / 800x600 / 1920x1080, forward + backward",
-            "views": len(views), "megapixels_per_step": px / 1e6, "batch_depth": best, "ms_per_step": ms,
-            "views_per_s": len(views) / (ms * 1e-3), "mpix_per_s": px / 1e6 / (ms * 1e-3), "autotune_ms": timings,
+            "views": len(views), "megapixels_per_step": px / 1e6, "batch_depth": best, "blend_block": block, "ms_per_step": ms,
+            "views_per_s": len(views) / (ms * 1e-3), "mpix_per_s": px / 1e6 / (ms * 1e-3),
+            "autotune_ms": {f"depth {d}, blend block {b}x{b}": t for (d, b), t in timings.items()},
             "plain_per_view": {"views_per_s": len(views) / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                                "note": "one view per call: forward (pair count read back) + backward, workspaces kept"},
             "batched_over_plain": plain_ms / ms, "pair_overflow": overflow, "graph_replays": steps * len(plans)}

@@ -77,7 +77,7 @@ BATCH_MAX_VIEWS, BATCH_MAX_SCENES = 64, 16
 
 
 class BatchView(C.Structure):
-    _fields_ = [("scene", C.c_int32), ("reserved", C.c_int32), ("camera", Camera), ("framebuffer", C.c_void_p),
+    _fields_ = [("scene", C.c_int32), ("blend_block", C.c_int32), ("camera", Camera), ("framebuffer", C.c_void_p),
                 ("grad_framebuffer", C.c_void_p)]
 
 

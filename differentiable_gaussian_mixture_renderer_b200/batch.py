@@ -1,7 +1,8 @@
 """Batched multi-view rendering: many cameras of several resident scenes,
 uneven Gaussian counts and resolutions, in one launch sequence, optionally
-captured in a CUDA graph, with an autotuner over the batch depth -- for the
-splat renderer (``kind="splat"``) and the volume marcher (``kind="march"``).
+captured in a CUDA graph, with an autotuner over the batch depth and, for
+the splat renderer, the blend's pixel-block size -- for the splat renderer
+(``kind="splat"``) and the volume marcher (``kind="march"``).
 
 The reference renders one view per call (splat_forward.cu:30-338; its
 vol_marcher.apply, python_bindings/vol_marcher.py:19-65, marches one camera);
@@ -59,14 +60,21 @@ class BatchRenderer:
     (``kind="splat"``) or the volume marcher (``kind="march"``, float32,
     full render mode)."""
 
-    def __init__(self, scenes: dict, device=None, capacity_margin: float = 1.1, kind: str = "splat"):
+    # sides of the splat blend's pixel blocks (dgmr_batch_view.blend_block);
+    # 0 leaves the choice to the library
+    BLEND_BLOCKS = (8, 16)
+
+    def __init__(self, scenes: dict, device=None, capacity_margin: float = 1.1, kind: str = "splat", blend_block: int = 0):
         if kind not in ("splat", "march"):
             raise ValueError("kind must be 'splat' or 'march'")
+        if blend_block not in (0,) + self.BLEND_BLOCKS:
+            raise ValueError(f"blend_block must be 0 or one of {self.BLEND_BLOCKS}")
         self.device = torch.device(device or "cuda")
         self.scenes: dict = scenes
         self.lib = N.lib()
         self.margin = capacity_margin
         self.kind = kind
+        self.blend_block = blend_block
         pre = "dgmr_splat_batch_" if kind == "splat" else "dgmr_vm_batch_"
         self._c_size = getattr(self.lib, pre + "workspace_size")
         self._c_pre = getattr(self.lib, pre + "preprocess")
@@ -85,6 +93,7 @@ class BatchRenderer:
         c_views = (N.BatchView * len(views))()
         for k, (sid, cam) in enumerate(views):
             c_views[k].scene = scene_ids.index(sid)
+            c_views[k].blend_block = self.blend_block if self.kind == "splat" else 0
             c_views[k].camera = camera_struct(cam)
         return scene_ids, c_scenes, c_views
 
@@ -191,14 +200,21 @@ def chunks(views, depth: int):
     return out
 
 
-def autotune(renderer: BatchRenderer, views, depths=(1, 4, 8, 16, 32, 48, 64), backward: bool = False, reps: int = 3):
-    """Times the whole view set, captured per chunk, for each batch depth; returns
-    (best_depth, {depth: ms}).  Identical results for every depth; only the
-    launch structure changes."""
+def autotune(renderer: BatchRenderer, views, depths=(1, 4, 8, 16, 32, 48, 64), backward: bool = False, reps: int = 3,
+             blend_blocks=None):
+    """Times the whole view set, captured per chunk, for each batch depth and
+    (splat renderer) each blend block side; returns ((best_depth, best_block),
+    {(depth, block): ms}) and leaves ``renderer.blend_block`` at the best side.
+    ``blend_blocks`` defaults to BatchRenderer.BLEND_BLOCKS for the splat
+    renderer and (0,) for the marcher.  Identical results for every setting;
+    only the launch structure changes."""
+    if blend_blocks is None:
+        blend_blocks = BatchRenderer.BLEND_BLOCKS if renderer.kind == "splat" else (0,)
     timings = {}
-    for d in depths:
+    for blk, d in ((b, d) for b in blend_blocks for d in depths):
         if d > N.BATCH_MAX_VIEWS:
             continue
+        renderer.blend_block = blk
         plans = [renderer.capture(renderer.plan(c, backward=backward), backward) for c in chunks(views, d)]
         torch.cuda.synchronize(renderer.device)
         s = plans[0].stream
@@ -218,8 +234,9 @@ def autotune(renderer: BatchRenderer, views, depths=(1, 4, 8, 16, 32, 48, 64), b
             e1.record(s)
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))
-        timings[d] = best
+        timings[(d, blk)] = best
         del plans
         torch.cuda.empty_cache()
-    best_d = min(timings, key=timings.get)
-    return best_d, timings
+    best = min(timings, key=timings.get)
+    renderer.blend_block = best[1]
+    return best, timings

@@ -256,15 +256,29 @@ struct SingleFrame {
     __device__ __forceinline__ FrameRef frame(uint32_t tile) const { return FrameRef { W, H, gx, tile, bg0, bg1, bg2, fb, final_T, n_contrib, grad_fb }; }
 };
 
-// __launch_bounds__(256, 5): at most 48 registers (no spills), five blocks per
-// SM instead of four at the 52 the compiler picks unbounded -- 3 % shorter
-// launches over 8 cameras at 1080p/1M, +2.3 % served renders/s.
-template <class Frames>
-__global__ void __launch_bounds__(256, 5) k_splat_blend(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list, const float4* __restrict__ rec,
-    const float* __restrict__ rgb, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats, const uint32_t* __restrict__ tile_order,
-    const __grid_constant__ Frames frames)
+// Block shapes of the blend: a 16x16 tile per block of 256 threads, or an 8x8
+// quarter of a tile per block of 64 threads (four blocks walk the same tile
+// list, each culling against its own quarter and stopping when its own pixels
+// are saturated; every pixel sees the same records in the same order, so the
+// results are the same bits).  __launch_bounds__ keeps both at 48 registers:
+// for 16x16, five blocks per SM instead of four at the 52 the compiler picks
+// unbounded -- 3 % shorter launches over 8 cameras at 1080p/1M, +2.3 % served
+// renders/s.
+template <int kSide>
+struct BlendShape {
+    static_assert(kSide == 16 || kSide == 8, "blend blocks of 16x16 or 8x8 pixels");
+    static constexpr int kThreads = kSide * kSide;
+    static constexpr int kMinBlocks = kSide == 16 ? 5 : 20;
+    static constexpr int kPerTile = (int(kTile) / kSide) * (int(kTile) / kSide); // blocks per 16x16 tile
+};
+
+template <int kSide, class Frames>
+__global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>::kMinBlocks) k_splat_blend(const int32_t* __restrict__ ranges,
+    const uint32_t* __restrict__ list, const float4* __restrict__ rec, const float* __restrict__ rgb, uint32_t N, uint32_t cap, uint32_t* __restrict__ stats,
+    const uint32_t* __restrict__ tile_order, const __grid_constant__ Frames frames)
 {
-    constexpr int kThreads = 256;
+    constexpr int kThreads = BlendShape<kSide>::kThreads;
+    constexpr int kPerTile = BlendShape<kSide>::kPerTile;
     constexpr int kBatch = kThreads;
     constexpr int kWarps = kThreads / 32;
     constexpr int kGroup = 4;
@@ -273,15 +287,20 @@ __global__ void __launch_bounds__(256, 5) k_splat_blend(const int32_t* __restric
     __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
     __shared__ float s_rgb[3][kBatch];
     __shared__ int s_warp_tot[kWarps];
-    const unsigned tile = tile_order ? tile_order[blockIdx.x] : blockIdx.x;
+    const unsigned slot = blockIdx.x / kPerTile, part = blockIdx.x % kPerTile;
+    const unsigned tile = tile_order ? tile_order[slot] : slot;
     const FrameRef f = frames.frame(tile);
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
-    // warp w covers the 8x4 pixel block (8 (w & 1), 4 (w >> 1)) of the tile:
-    // a compact footprint, so fewer records pass some lane's cutoff than over
-    // a 16x2 strip (a record no lane needs costs one vote)
-    const unsigned px = tx * kTile + 8u * ((threadIdx.x >> 5) & 1u) + (threadIdx.x & 7u);
-    const unsigned py = ty * kTile + 4u * (threadIdx.x >> 6) + ((threadIdx.x >> 3) & 3u);
+    // the block's pixels start at (ox, oy) of the tile; warp w covers the 8x4
+    // pixel block (8 (w % kRow), 4 (w / kRow)) of them: a compact footprint, so
+    // fewer records pass some lane's cutoff than over a 16x2 strip (a record
+    // no lane needs costs one vote)
+    constexpr unsigned kRow = unsigned(kSide) / 8u;
+    const unsigned ox = unsigned(kSide) * (part % (kTile / unsigned(kSide))), oy = unsigned(kSide) * (part / (kTile / unsigned(kSide)));
+    const unsigned wb = threadIdx.x >> 5;
+    const unsigned px = tx * kTile + ox + 8u * (wb % kRow) + (threadIdx.x & 7u);
+    const unsigned py = ty * kTile + oy + 4u * (wb / kRow) + ((threadIdx.x >> 3) & 3u);
     PixelState p0 { 1.f, 0.f, 0.f, 0.f, 0, !(px < W && py < H) };
     const bool in0 = !p0.done;
     int32_t b = ranges[2 * tile], e = ranges[2 * tile + 1];
@@ -290,7 +309,7 @@ __global__ void __launch_bounds__(256, 5) k_splat_blend(const int32_t* __restric
             flag_bounds(stats, 0x31u);
         b = e = 0;
     }
-    const float fx0 = float(tx * kTile), fx1 = fx0 + 15.f, fy0 = float(ty * kTile), fy1 = fy0 + 15.f;
+    const float fx0 = float(tx * kTile + ox), fx1 = fx0 + float(kSide - 1), fy0 = float(ty * kTile + oy), fy1 = fy0 + float(kSide - 1);
     const float fpx = float(px), fpy = float(py);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int32_t base = b; base < e; base += kBatch) {
@@ -386,6 +405,24 @@ __global__ void __launch_bounds__(256, 5) k_splat_blend(const int32_t* __restric
     }
 }
 
+// The blend over n_tiles tiles with blocks of side x side pixels (16 or 8).
+// Single frames use 8x8 blocks: at 1080p with 1M Gaussians the blend takes
+// 0.1725 ms against 0.198 ms with 16x16 blocks (the same bits); batches take
+// the side from their views (dgmr_batch_view.blend_block).
+constexpr int kBlendSide = 8;
+template <class Frames>
+void launch_blend(int side, uint32_t n_tiles, const int32_t* ranges, const uint32_t* list, const float4* rec, const float* rgb, uint32_t N, uint32_t cap,
+    uint32_t* stats, const uint32_t* tile_order, const Frames& frames, cudaStream_t s)
+{
+    if (n_tiles == 0)
+        return;
+    if (side == 8)
+        k_splat_blend<8, Frames><<<n_tiles * BlendShape<8>::kPerTile, BlendShape<8>::kThreads, 0, s>>>(ranges, list, rec, rgb, N, cap, stats, tile_order, frames);
+    else
+        k_splat_blend<16, Frames><<<n_tiles, BlendShape<16>::kThreads, 0, s>>>(ranges, list, rec, rgb, N, cap, stats, tile_order, frames);
+    note_launch();
+}
+
 // Sums of 9 per-lane values over a warp, scattered: halve the slots each lane
 // holds at every butterfly level (16 -> 8 -> 4 -> 2 -> 1, the upper half kept
 // by the lanes whose level bit is set), then add the partner's copy.  Lane l
@@ -416,28 +453,37 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], int l
 // summed over the warp with shuffles before one atomic per value.  Tiles run
 // in the forward's launch order (heaviest predicted walk first): a tile's
 // backward walks the same list up to its last contributor.
-// __launch_bounds__(256, 5): 48 registers instead of 53, five blocks per SM
-// instead of four (backward 2-3 % shorter at 1080p/1M and 200k/1024^2).
-template <class Frames>
-__global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __restrict__ ranges, const uint32_t* __restrict__ list,
-    const float4* __restrict__ rec, const float* __restrict__ rgb, double* __restrict__ acc, const uint32_t* __restrict__ tile_order,
-    const __grid_constant__ Frames frames)
+// The block shapes of the forward (BlendShape): with 8x8 blocks each block
+// walks only up to the last contributor of its own 64 pixels.
+// __launch_bounds__: 48 registers (for 16x16, instead of 53: five blocks per
+// SM instead of four, backward 2-3 % shorter at 1080p/1M and 200k/1024^2).
+template <int kSide, class Frames>
+__global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>::kMinBlocks) k_splat_bwd_pixels(const int32_t* __restrict__ ranges,
+    const uint32_t* __restrict__ list, const float4* __restrict__ rec, const float* __restrict__ rgb, double* __restrict__ acc,
+    const uint32_t* __restrict__ tile_order, const __grid_constant__ Frames frames)
 {
-    __shared__ float4 s_r0[256]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
-    __shared__ float4 s_r1[256];
-    __shared__ float s_rgb[3][256];
-    __shared__ uint32_t s_id[256];
+    constexpr int kThreads = BlendShape<kSide>::kThreads;
+    constexpr int kPerTile = BlendShape<kSide>::kPerTile;
+    __shared__ float4 s_r0[kThreads]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
+    __shared__ float4 s_r1[kThreads];
+    __shared__ float s_rgb[3][kThreads];
+    __shared__ uint32_t s_id[kThreads];
     __shared__ int s_max;
-    const unsigned ordered = tile_order ? tile_order[blockIdx.x] : blockIdx.x;
-    const unsigned tile = ordered < gridDim.x ? ordered : blockIdx.x; // the order is a permutation of the tiles
+    const unsigned slot = blockIdx.x / kPerTile, part = blockIdx.x % kPerTile, n_tiles = gridDim.x / kPerTile;
+    const unsigned ordered = tile_order ? tile_order[slot] : slot;
+    const unsigned tile = ordered < n_tiles ? ordered : slot; // the order is a permutation of the tiles
     const FrameRef f = frames.frame(tile);
     if (!f.grad_fb) // a view without an image gradient (batched renders that only asked for the image)
         return;
     const unsigned W = f.W, H = f.H;
     const unsigned tx = f.tile % f.gx, ty = f.tile / f.gx;
-    // the forward's pixel blocks: warp w covers the 8x4 block (8 (w & 1), 4 (w >> 1))
-    const unsigned px = tx * kTile + 8u * ((threadIdx.x >> 5) & 1u) + (threadIdx.x & 7u);
-    const unsigned py = ty * kTile + 4u * (threadIdx.x >> 6) + ((threadIdx.x >> 3) & 3u);
+    // the forward's pixel blocks: the block's pixels start at (ox, oy) of the
+    // tile, warp w covers the 8x4 block (8 (w % kRow), 4 (w / kRow)) of them
+    constexpr unsigned kRow = unsigned(kSide) / 8u;
+    const unsigned ox = unsigned(kSide) * (part % (kTile / unsigned(kSide))), oy = unsigned(kSide) * (part / (kTile / unsigned(kSide)));
+    const unsigned wb = threadIdx.x >> 5;
+    const unsigned px = tx * kTile + ox + 8u * (wb % kRow) + (threadIdx.x & 7u);
+    const unsigned py = ty * kTile + oy + 4u * (wb / kRow) + ((threadIdx.x >> 3) & 3u);
     const bool inside = px < W && py < H;
     const int32_t b = ranges[2 * tile];
     const size_t pix = size_t(py) * W + px;
@@ -460,8 +506,8 @@ __global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __re
     float a0 = 0.f, a1 = 0.f, a2 = 0.f; // accumulated colour behind the current splat
     const float fpx = float(px), fpy = float(py);
     const int lane = threadIdx.x & 31;
-    for (int32_t hi = max_n; hi > 0; hi -= 256) {
-        const int32_t lo = hi > 256 ? hi - 256 : 0;
+    for (int32_t hi = max_n; hi > 0; hi -= kThreads) {
+        const int32_t lo = hi > kThreads ? hi - kThreads : 0;
         __syncthreads();
         const int32_t k = lo + int32_t(threadIdx.x);
         if (k < hi) {
@@ -523,6 +569,19 @@ __global__ void __launch_bounds__(256, 5) k_splat_bwd_pixels(const int32_t* __re
             }
         }
     }
+}
+
+// The per-pixel adjoint over n_tiles tiles with the forward's block shape.
+template <class Frames>
+void launch_blend_bwd(int side, uint32_t n_tiles, const int32_t* ranges, const uint32_t* list, const float4* rec, const float* rgb, double* acc,
+    const uint32_t* tile_order, const Frames& frames, cudaStream_t s)
+{
+    if (n_tiles == 0)
+        return;
+    if (side == 8)
+        k_splat_bwd_pixels<8, Frames><<<n_tiles * BlendShape<8>::kPerTile, BlendShape<8>::kThreads, 0, s>>>(ranges, list, rec, rgb, acc, tile_order, frames);
+    else
+        k_splat_bwd_pixels<16, Frames><<<n_tiles, BlendShape<16>::kThreads, 0, s>>>(ranges, list, rec, rgb, acc, tile_order, frames);
 }
 
 struct SplatBwdGauss {
@@ -832,8 +891,7 @@ void launch_render(const dgmr_scene* scene, const CameraT<float>& cam, float* fb
     const int par
         = run_binning<float>(N, cam.gx, cam.gy, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev, num_sms(), s, true);
     launch_tile_order(L, par, N, cap, cam.gx * cam.gy, single_frame(cam, fb, L), s);
-    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, N, cap, st_dev, L.tile_order, single_frame(cam, fb, L));
-    note_launch();
+    launch_blend(kBlendSide, cam.gx * cam.gy, L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, N, cap, st_dev, L.tile_order, single_frame(cam, fb, L), s);
 }
 
 } // namespace
@@ -955,9 +1013,8 @@ dgmr_status dgmr_splat_blend(const dgmr_camera* camera, int32_t n_gaussians, flo
     const CameraT<float> cam = make_camera<float>(*camera);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
-    k_splat_blend<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
-        L.tile_order, single_frame(cam, framebuffer, L));
-    note_launch();
+    launch_blend(kBlendSide, cam.gx * cam.gy, L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, uint32_t(n_gaussians), uint32_t(pair_capacity), L.stats,
+        L.tile_order, single_frame(cam, framebuffer, L), s);
     return launch_status();
 }
 
@@ -983,8 +1040,8 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
     const CameraT<float> cam = make_camera<float>(*camera);
     const int par = tile_sort_parity(super_count(cam.gx, cam.gy));
     cudaMemsetAsync(L.grad_acc, 0, size_t(N) * 9 * sizeof(double), s);
-    k_splat_bwd_pixels<<<cam.gx * cam.gy, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order,
-        single_frame(cam, nullptr, L, grad_framebuffer));
+    launch_blend_bwd(kBlendSide, cam.gx * cam.gy, L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order,
+        single_frame(cam, nullptr, L, grad_framebuffer), s);
     SplatBwdGauss p { N, static_cast<const float*>(scene->centroids), static_cast<const float*>(scene->sh), scene->sh_stride, scene->sh_degree,
         static_cast<const float*>(scene->weights), static_cast<const float*>(scene->scales), static_cast<const float*>(scene->rotations), L.clamped,
         L.tiles_touched, L.grad_acc, grad_sh, grad_weights, grad_centroids, grad_scales, grad_rotations, scene_formulation(scene, Formulation::Ots) };
@@ -1064,6 +1121,7 @@ struct BatchPlan {
     BatchTable tab;
     SplatLayout L;
     size_t px_total;
+    int blend_side; // the blend's block side (dgmr_batch_view.blend_block)
 };
 
 // Validates the batch and builds its table and workspace layout.  grads may be
@@ -1077,6 +1135,13 @@ dgmr_status make_batch(const dgmr_scene* scenes, int32_t n_scenes, const dgmr_ba
     const dgmr_status st = build_batch_table(scenes, n_scenes, views, n_views, grads, Formulation::Ots, t);
     if (st != DGMR_OK)
         return st;
+    const int side = views[0].blend_block;
+    if (side != 0 && side != 8 && side != 16)
+        return DGMR_ERR_BAD_ARG;
+    for (int v = 1; v < n_views; ++v)
+        if (views[v].blend_block != 0 && views[v].blend_block != side)
+            return DGMR_ERR_BAD_ARG;
+    plan.blend_side = side ? side : kBlendSide;
     plan.px_total = t.px_total;
     plan.L = splat_layout_n(t.G, t.n_tiles, plan.px_total, uint32_t(pair_capacity), frame_ws, pair_ws);
     t.final_T = plan.L.final_T;
@@ -1172,7 +1237,7 @@ dgmr_status dgmr_splat_batch_forward(const dgmr_scene* scenes, int32_t n_scenes,
     const int par = run_binning_grids<float>(G, plan.tab.n_tiles, plan.tab.n_stiles, plan.tab, L.tiles_touched, L.point_offsets, L.rects, L.xy, cap, L.bin, L.ranges, st_dev,
         num_sms(), s, true);
     launch_tile_order(L, par, G, cap, plan.tab.n_tiles, plan.tab, s);
-    k_splat_blend<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab);
+    launch_blend(plan.blend_side, plan.tab.n_tiles, L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, G, cap, st_dev, L.tile_order, plan.tab, s);
     note_launch();
     return launch_status();
 }
@@ -1198,7 +1263,7 @@ dgmr_status dgmr_splat_batch_backward(const dgmr_scene* scenes, int32_t n_scenes
         return DGMR_OK;
     const int par = tile_sort_parity(plan.tab.n_stiles);
     cudaMemsetAsync(L.grad_acc, 0, size_t(G) * 9 * sizeof(double), s);
-    k_splat_bwd_pixels<<<plan.tab.n_tiles, 256, 0, s>>>(L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order, plan.tab);
+    launch_blend_bwd(plan.blend_side, plan.tab.n_tiles, L.ranges, L.bin.pair_val[par], L.blend_rec, L.rgb, L.grad_acc, L.tile_order, plan.tab, s);
     SplatBwdGauss state { 0, nullptr, nullptr, 1, 0, nullptr, nullptr, nullptr, L.clamped, L.tiles_touched, L.grad_acc, nullptr, nullptr, nullptr, nullptr,
         nullptr, Formulation::Ots };
     k_batch_bwd_gaussians<<<(n_scene_gaussians + 127) / 128, 128, 0, s>>>(state, plan.tab);

@@ -187,7 +187,10 @@ dgmr_status dgmr_splat_backward(const dgmr_scene* scene, const dgmr_camera* came
 
 typedef struct dgmr_batch_view {
     int32_t scene; /* index into the scenes array */
-    int32_t reserved;
+    int32_t blend_block; /* splat batches: side of the blend's pixel blocks, 8 or 16 (0 = the library default, 8); the
+                            first view's value holds for the batch, and later views carry 0 or the same value.  Every
+                            block shape gives the same bits (each pixel sees the same splats in the same order); only
+                            the speed differs.  The volume marcher ignores it. */
     dgmr_camera camera;
     float* framebuffer; /* [3,H,W] device, written by the forward */
     const float* grad_framebuffer; /* [3,H,W] device, read by the backward; NULL = no gradient for this view */

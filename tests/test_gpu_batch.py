@@ -106,9 +106,46 @@ def test_batch_capacity_overflow_is_flagged(cuda):
     assert p.n_pairs() > 100
 
 
-def test_autotune_picks_a_depth(cuda):
+def test_autotune_picks_a_depth_and_a_blend_block(cuda):
     from differentiable_gaussian_mixture_renderer_b200.batch import autotune
     r, scenes, views = _setup(cuda)
     best, timings = autotune(r, views, depths=(1, 2, 5), reps=1)
-    assert best in (1, 2, 5) and set(timings) == {1, 2, 5}
+    assert set(timings) == {(d, b) for d in (1, 2, 5) for b in (8, 16)}
+    assert best in timings and r.blend_block == best[1]
     assert all(t > 0 for t in timings.values())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("backward", [False, True])
+def test_blend_block_sides_give_the_same_bits(cuda, backward):
+    """The blend's 8x8 and 16x16 pixel blocks (the autotuner's block knob) walk
+    the same tile lists: images, transmittance-derived contributor counts and
+    point lists are the same bits; gradients agree up to the order of the
+    per-pixel atomics."""
+    from differentiable_gaussian_mixture_renderer_b200.batch import BatchRenderer
+    r, scenes, views = _setup(cuda)
+    out = {}
+    for blk in (8, 16):
+        rb = BatchRenderer(scenes, cuda, blend_block=blk)
+        p = rb.plan(views, backward=backward)
+        if backward:
+            gen = torch.Generator(device=cuda).manual_seed(4)
+            for g in p.grad_framebuffers:
+                g.copy_(torch.randn(g.shape, generator=gen, device=cuda))
+        rb.forward(p)
+        if backward:
+            rb.backward(p)
+        torch.cuda.synchronize()
+        out[blk] = ([fb.clone() for fb in p.framebuffers], {k: [t.clone() for t in v] for k, v in p.grads.items()})
+    for a, b in zip(out[8][0], out[16][0]):
+        assert torch.equal(a, b)
+    for sid in out[8][1]:
+        for a, b in zip(out[8][1][sid], out[16][1][sid]):
+            scale = float(b.abs().max()) + 1e-30
+            assert float((a - b).abs().max()) <= 1e-5 * scale
+
+
+def test_blend_block_must_be_8_or_16(cuda):
+    from differentiable_gaussian_mixture_renderer_b200.batch import BatchRenderer
+    with pytest.raises(ValueError):
+        BatchRenderer({}, cuda, blend_block=32)
