@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
     static_assert(kBatch % kGroup == 0, "a group never reads past the batch");
     __shared__ float4 s_r0[kBatch];
     __shared__ float4 s_r1[kBatch]; // (2b, opacity, q_cut, 1-based list index as int bits)
-    __shared__ float s_rgb[3][kBatch];
+    __shared__ float4 s_rgb[kBatch]; // (r, g, b, .): one 16-byte load per record that a warp blends
     __shared__ int s_warp_tot[kWarps];
     const unsigned slot = blockIdx.x / kPerTile, part = blockIdx.x % kPerTile;
     const unsigned tile = tile_order ? tile_order[slot] : slot;
@@ -352,9 +352,7 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
         if (keep) {
             s_r0[slot] = r0;
             s_r1[slot] = r1;
-            s_rgb[0][slot] = rgb[3 * size_t(id)];
-            s_rgb[1][slot] = rgb[3 * size_t(id) + 1];
-            s_rgb[2][slot] = rgb[3 * size_t(id) + 2];
+            s_rgb[slot] = make_float4(rgb[3 * size_t(id)], rgb[3 * size_t(id) + 1], rgb[3 * size_t(id) + 2], 0.f);
         }
         // the slots after the last record up to the group boundary: a cutoff below
         // every quadratic form (q = 0 here), so no lane ever uses them
@@ -386,7 +384,8 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
                         continue;
                     const float ex = u[i] ? dgmr_fm::exp_f_nonpos(-0.5f * q[i]) : 0.f;
                     const float4 a1 = s_r1[j + i];
-                    blend_alpha_select(p0, u[i], ex, a1.y, s_rgb[0][j + i], s_rgb[1][j + i], s_rgb[2][j + i], __float_as_int(a1.w));
+                    const float4 c = s_rgb[j + i];
+                    blend_alpha_select(p0, u[i], ex, a1.y, c.x, c.y, c.z, __float_as_int(a1.w));
                 }
                 if (__all_sync(0xffffffffu, p0.done))
                     break;
