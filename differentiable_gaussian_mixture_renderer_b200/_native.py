@@ -155,6 +155,10 @@ _SIGNATURES = {
     "dgmr_vm_batch_backward": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
                                          C.POINTER(SceneGrads), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
                                          C.c_int64, C.c_void_p, C.c_void_p]),
+    "dgmr_batch_autotune": (C.c_int, [C.c_int32, C.POINTER(Scene), C.c_int32, C.POINTER(BatchView), C.c_int32,
+                                      C.POINTER(SceneGrads), C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
+                                      C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int64,
+                                      C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
     "dgmr_vr_frame_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "dgmr_vr_pair_workspace_size": (C.c_size_t, [C.c_int32, C.c_int64]),
     "dgmr_vr_preprocess": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),

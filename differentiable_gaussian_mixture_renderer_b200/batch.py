@@ -202,41 +202,33 @@ def chunks(views, depth: int):
 
 def autotune(renderer: BatchRenderer, views, depths=(1, 4, 8, 16, 32, 48, 64), backward: bool = False, reps: int = 3,
              blend_blocks=None):
-    """Times the whole view set, captured per chunk, for each batch depth and
-    (splat renderer) each blend block side; returns ((best_depth, best_block),
+    """Picks the batch depth and (splat renderer) the blend block side for a
+    view set of at most 64 views with the library's autotuner
+    (``dgmr_batch_autotune``): each candidate renders the whole set, cut into
+    consecutive batches of at most ``depth`` views, forward (and backward),
+    timed with CUDA events on one stream.  Returns ((best_depth, best_block),
     {(depth, block): ms}) and leaves ``renderer.blend_block`` at the best side.
     ``blend_blocks`` defaults to BatchRenderer.BLEND_BLOCKS for the splat
     renderer and (0,) for the marcher.  Identical results for every setting;
     only the launch structure changes."""
     if blend_blocks is None:
         blend_blocks = BatchRenderer.BLEND_BLOCKS if renderer.kind == "splat" else (0,)
-    timings = {}
-    for blk, d in ((b, d) for b in blend_blocks for d in depths):
-        if d > N.BATCH_MAX_VIEWS:
-            continue
-        renderer.blend_block = blk
-        plans = [renderer.capture(renderer.plan(c, backward=backward), backward) for c in chunks(views, d)]
-        torch.cuda.synchronize(renderer.device)
-        s = plans[0].stream
-        for p in plans[1:]:
-            s.wait_stream(p.stream)
-        best = float("inf")
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize(renderer.device)
-            e0.record(s)
-            for p in plans:
-                p.stream.wait_event(e0)
-                with torch.cuda.stream(p.stream):
-                    p.graph.replay()
-            for p in plans:
-                s.wait_stream(p.stream)
-            e1.record(s)
-            e1.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        timings[(d, blk)] = best
-        del plans
-        torch.cuda.empty_cache()
-    best = min(timings, key=timings.get)
-    renderer.blend_block = best[1]
-    return best, timings
+    depths = [d for d in depths if d <= N.BATCH_MAX_VIEWS]
+    if not depths or not blend_blocks:
+        raise ValueError("autotune needs at least one depth and one blend block")
+    p = renderer.plan(views, backward=backward)
+    d_arr = (C.c_int32 * len(depths))(*depths)
+    b_arr = (C.c_int32 * len(blend_blocks))(*blend_blocks)
+    ms = (C.c_float * (len(depths) * len(blend_blocks)))()
+    best_d, best_b = C.c_int32(0), C.c_int32(0)
+    kind = N.SERVE_SPLAT if renderer.kind == "splat" else N.SERVE_MARCH
+    N.check(renderer.lib.dgmr_batch_autotune(kind, p.c_scenes, len(p.c_scenes), p.c_views, p.n_views,
+                                             p.c_grads if backward else None, d_arr, len(depths), b_arr,
+                                             len(blend_blocks), reps, N.ptr(p.frame_ws), p.frame_ws.numel(),
+                                             N.ptr(p.pair_ws), p.pair_ws.numel(), p.capacity, ms, C.byref(best_d),
+                                             C.byref(best_b), N.stream_handle()), "batch autotune")
+    timings = {(d, b): float(ms[i * len(blend_blocks) + j]) for i, d in enumerate(depths)
+               for j, b in enumerate(blend_blocks)}
+    renderer.blend_block = int(best_b.value)
+    del p
+    return (int(best_d.value), int(best_b.value)), timings

@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(OUT_DIR, "libdgmr_b200.so")
-SOURCES = ["dgmr_splat.cu", "dgmr_marcher.cu", "dgmr_raster.cu", "dgmr_server.cpp"]
+SOURCES = ["dgmr_splat.cu", "dgmr_marcher.cu", "dgmr_raster.cu", "dgmr_server.cpp", "dgmr_autotune.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INCLUDE = os.path.join(HERE, "..", "include")
 VIEWER_SRC = os.path.join(HERE, "viewer", "headless_view.cpp")

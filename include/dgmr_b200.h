@@ -258,6 +258,28 @@ dgmr_status dgmr_vm_batch_backward(const dgmr_scene* scenes, int32_t n_scenes, c
     const dgmr_scene_grads* grads, void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes,
     int64_t pair_capacity, dgmr_frame_stats* stats, dgmr_stream stream);
 
+/* ------------------------------------------------------ batch autotuner */
+
+/* Picks the launch structure of a view set (no reference counterpart: the
+ * reference renders one view per call).  For every candidate (depths[d],
+ * blend_blocks[b]) the views are cut into consecutive batches of at most
+ * depths[d] views (each batch passing only the scenes its views use) with
+ * that blend block, and the whole set is rendered -- forward, and backward
+ * when grads != NULL -- once untimed and reps times timed with CUDA events on
+ * stream.  ms[d * n_blocks + b] receives the candidate's best time,
+ * *best_depth and *best_block the fastest candidate.  kind is
+ * DGMR_SERVE_SPLAT (blend blocks 0, 8 or 16) or DGMR_SERVE_MARCH (the marcher
+ * has no blend block: pass 0).  Every candidate gives the same images and
+ * gradients; the runs overwrite the views' framebuffers and the gradient
+ * outputs.  The workspaces are those of one batch of all the views (at most
+ * DGMR_BATCH_MAX_VIEWS, sized by the kind's *_batch_workspace_size with the
+ * pair capacity of the whole set).  The call waits for the stream (it reads
+ * the events), so it cannot be captured in a CUDA graph. */
+dgmr_status dgmr_batch_autotune(int32_t kind, const dgmr_scene* scenes, int32_t n_scenes, const dgmr_batch_view* views, int32_t n_views,
+    const dgmr_scene_grads* grads, const int32_t* depths, int32_t n_depths, const int32_t* blend_blocks, int32_t n_blocks, int32_t reps,
+    void* frame_workspace, size_t frame_workspace_bytes, void* pair_workspace, size_t pair_workspace_bytes, int64_t pair_capacity, float* ms,
+    int32_t* best_depth, int32_t* best_block, dgmr_stream stream);
+
 /* ---------------------------------------------------------- vol_raster */
 
 /* Replaces dgmr::vol_raster_forward(VolRasterForwardData&)

@@ -111,8 +111,17 @@ def test_autotune_picks_a_depth_and_a_blend_block(cuda):
     r, scenes, views = _setup(cuda)
     best, timings = autotune(r, views, depths=(1, 2, 5), reps=1)
     assert set(timings) == {(d, b) for d in (1, 2, 5) for b in (8, 16)}
-    assert best in timings and r.blend_block == best[1]
+    assert best in timings and r.blend_block == best[1] and timings[best] == min(timings.values())
     assert all(t > 0 for t in timings.values())
+    # with the backward, and the images of the picked setting still those of single views
+    best, timings = autotune(r, views, depths=(2, 5), backward=True, reps=1)
+    assert set(timings) == {(d, b) for d in (2, 5) for b in (8, 16)}
+    p = r.plan(views)
+    r.forward(p)
+    torch.cuda.synchronize()
+    for (sid, cam), fb in zip(views, p.framebuffers):
+        want, _ = _single(scenes[sid], cam)
+        assert torch.equal(fb, want)
 
 
 @pytest.mark.gpu

@@ -118,3 +118,19 @@ def test_batch_march_graph_replay(cuda):
         _close(f"replay.{name}", b, a)
     sid, cam = views[1]
     assert torch.equal(first[1], cpp_binding.forward(*_args(scenes[sid], cam, cuda))[0])
+
+
+def test_batch_march_autotune_picks_a_depth(cuda):
+    """The native autotuner (dgmr_batch_autotune) on marcher batches, forward
+    and backward: one time per depth (no blend block: 0), the best among them,
+    and the renders afterwards still equal the single views."""
+    from differentiable_gaussian_mixture_renderer_b200.batch import autotune
+    r, scenes, views = _setup(cuda)
+    (depth, block), timings = autotune(r, views, depths=(1, 2, 5), backward=True, reps=1)
+    assert set(timings) == {(1, 0), (2, 0), (5, 0)} and block == 0
+    assert timings[(depth, 0)] == min(timings.values()) and all(t > 0 for t in timings.values())
+    p = r.plan(views)
+    r.forward(p)
+    for (sid, cam), fb in zip(views, p.framebuffers):
+        want = cpp_binding.forward(*_args(scenes[sid], cam, cuda))[0]
+        assert torch.equal(fb, want)
