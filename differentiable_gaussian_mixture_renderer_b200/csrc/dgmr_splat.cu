@@ -463,10 +463,12 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
 {
     constexpr int kThreads = BlendShape<kSide>::kThreads;
     constexpr int kPerTile = BlendShape<kSide>::kPerTile;
-    __shared__ float4 s_r0[kThreads]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, .)
+    constexpr int kWarps = kThreads / 32;
+    __shared__ float4 s_r0[kThreads]; // the blend records: (x, y, a, c), (2b, opacity, q_cut, list index as int bits)
     __shared__ float4 s_r1[kThreads];
     __shared__ float s_rgb[3][kThreads];
     __shared__ uint32_t s_id[kThreads];
+    __shared__ int s_warp_tot[kWarps];
     __shared__ int s_max;
     const unsigned slot = blockIdx.x / kPerTile, part = blockIdx.x % kPerTile, n_tiles = gridDim.x / kPerTile;
     const unsigned ordered = tile_order ? tile_order[slot] : slot;
@@ -504,34 +506,64 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
     float Tr = Tf;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f; // accumulated colour behind the current splat
     const float fpx = float(px), fpy = float(py);
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float fx0 = float(tx * kTile + ox), fx1 = fx0 + float(kSide - 1), fy0 = float(ty * kTile + oy), fy1 = fy0 + float(kSide - 1);
     for (int32_t hi = max_n; hi > 0; hi -= kThreads) {
         const int32_t lo = hi > kThreads ? hi - kThreads : 0;
         __syncthreads();
+        // the batch's records that can reach a pixel of this block (the
+        // forward's exact rectangle cull), compacted in list order with their
+        // list positions; the others add nothing to any pixel here
         const int32_t k = lo + int32_t(threadIdx.x);
+        uint32_t id = 0;
+        float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
+        int keep = 0;
         if (k < hi) {
-            const uint32_t id = list[b + k];
-            s_id[threadIdx.x] = id;
-            s_r0[threadIdx.x] = rec[2 * size_t(id)];
-            s_r1[threadIdx.x] = rec[2 * size_t(id) + 1];
-            s_rgb[0][threadIdx.x] = rgb[3 * id];
-            s_rgb[1][threadIdx.x] = rgb[3 * id + 1];
-            s_rgb[2][threadIdx.x] = rgb[3 * id + 2];
+            id = list[b + k];
+            r0 = rec[2 * size_t(id)];
+            r1 = rec[2 * size_t(id) + 1];
+            const float qmin = rect_min_q(r0.x, r0.y, r0.z, 0.5f * r1.x, r0.w, fx0, fx1, fy0, fy1);
+            keep = !(qmin > r1.z * 1.001f + 0.01f);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0)
+            s_warp_tot[warp] = __popc(m);
+        __syncthreads();
+        int pos = __popc(m & ((1u << lane) - 1u));
+        int n = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const int t = s_warp_tot[w];
+            pos += (w < warp) ? t : 0;
+            n += t;
+        }
+        if (keep) {
+            r1.w = __int_as_float(k);
+            s_id[pos] = id;
+            s_r0[pos] = r0;
+            s_r1[pos] = r1;
+            s_rgb[0][pos] = rgb[3 * size_t(id)];
+            s_rgb[1][pos] = rgb[3 * size_t(id) + 1];
+            s_rgb[2][pos] = rgb[3 * size_t(id) + 2];
         }
         __syncthreads();
-        for (int32_t kk = hi - 1; kk >= lo; --kk) {
-            const int j = kk - lo;
+        for (int j = n - 1; j >= 0; --j) {
             float v[9] = { 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f };
             bool any = false;
-            if (kk < my_n) {
-                // the forward's cutoff: past q_cut alpha < 1/255, so exp is not needed
-                float dx, dy;
-                const float4 r0 = s_r0[j], r1 = s_r1[j];
-                const float q = splat_q(r0, r1.x, fpx, fpy, &dx, &dy);
+            const float4 r0 = s_r0[j], r1 = s_r1[j];
+            const int32_t kk = __float_as_int(r1.w);
+            float dx, dy;
+            const float q = splat_q(r0, r1.x, fpx, fpy, &dx, &dy);
+            // the forward's cutoff: past q_cut alpha < 1/255, so exp is not
+            // needed; a record no lane of the warp needs costs one vote
+            const bool need = kk < my_n && !(q > r1.z);
+            if (!__any_sync(0xffffffffu, need))
+                continue;
+            if (need) {
                 const float4 co = make_float4(r0.z, 0.5f * r1.x, r0.w, r1.y); // conic a, b, c and opacity
-                const float g = q > r1.z ? 0.f : dgmr_fm::exp_f_nonpos(-0.5f * q);
+                const float g = dgmr_fm::exp_f_nonpos(-0.5f * q);
                 const float alpha = min_f(0.99f, co.w * g);
-                if (!(q > r1.z) && !(alpha < 1.0f / 255.0f)) {
+                if (!(alpha < 1.0f / 255.0f)) {
                     any = true;
                     Tr = Tr / (1.f - alpha);
                     const float c0 = s_rgb[0][j], c1 = s_rgb[1][j], c2 = s_rgb[2][j];
