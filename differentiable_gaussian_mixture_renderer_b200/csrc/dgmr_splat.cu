@@ -565,13 +565,15 @@ __global__ void __launch_bounds__(BlendShape<kSide>::kThreads, BlendShape<kSide>
                 const float alpha = min_f(0.99f, co.w * g);
                 if (!(alpha < 1.0f / 255.0f)) {
                     any = true;
-                    Tr = Tr / (1.f - alpha);
+                    // T before this splat, and the background term's 1 / (1 - alpha): one reciprocal
+                    const float inv = 1.f / (1.f - alpha);
+                    Tr = Tr * inv;
                     const float c0 = s_rgb[0][j], c1 = s_rgb[1][j], c2 = s_rgb[2][j];
                     const float aT = alpha * Tr;
                     v[6] = aT * g0;
                     v[7] = aT * g1;
                     v[8] = aT * g2;
-                    const float g_alpha = Tr * (((c0 - a0) * g0 + (c1 - a1) * g1) + (c2 - a2) * g2) - Tf * bg_dot / (1.f - alpha);
+                    const float g_alpha = Tr * (((c0 - a0) * g0 + (c1 - a1) * g1) + (c2 - a2) * g2) - (Tf * bg_dot) * inv;
                     a0 = alpha * c0 + (1.f - alpha) * a0;
                     a1 = alpha * c1 + (1.f - alpha) * a1;
                     a2 = alpha * c2 + (1.f - alpha) * a2;

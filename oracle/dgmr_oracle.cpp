@@ -1103,13 +1103,15 @@ void splat_backward_impl(const SceneIn<T>& s, const T* rgb, const uint8_t* clamp
                     const T alpha = splat_alpha(co, xy + 2 * size_t(id), T(float(px)), T(float(py)), &g, &dx, &dy);
                     if (alpha < T(1.0f / 255.0f))
                         continue;
-                    Tr = Tr / (T(1) - alpha);
+                    // T before this splat, and the background term's 1 / (1 - alpha): one reciprocal
+                    const T inv = T(1) / (T(1) - alpha);
+                    Tr = Tr * inv;
                     const V3<T> c = load3(rgb, id);
                     double* a = my + size_t(id) * 9;
                     a[6] += double(alpha * Tr * gout.x);
                     a[7] += double(alpha * Tr * gout.y);
                     a[8] += double(alpha * Tr * gout.z);
-                    const T g_alpha = Tr * ((c.x - accum.x) * gout.x + (c.y - accum.y) * gout.y + (c.z - accum.z) * gout.z) - Tf * bg_dot / (T(1) - alpha);
+                    const T g_alpha = Tr * ((c.x - accum.x) * gout.x + (c.y - accum.y) * gout.y + (c.z - accum.z) * gout.z) - (Tf * bg_dot) * inv;
                     accum = { alpha * c.x + (T(1) - alpha) * accum.x, alpha * c.y + (T(1) - alpha) * accum.y, alpha * c.z + (T(1) - alpha) * accum.z };
                     const T og = co[3] * g;
                     if (!(og < T(0.99f)))
