@@ -548,6 +548,21 @@ extern "C" long kat_fmath_mismatches(int which, unsigned first, unsigned stride,
     return bad;
 }
 
+// dgmr_fm::recip_hastings against the correctly rounded 1.0f / d for every
+// float d in [lo, hi]; returns the count that differ in any bit, *checked the
+// inputs seen.
+extern "C" long kat_recip_mismatches(float lo, float hi, long* checked)
+{
+    long bad = 0, n = 0;
+    for (float d = lo; d <= hi; d = std::nextafter(d, 2.0f * hi)) {
+        const float a = 1.0f / d, b = dgmr_fm::recip_hastings(d);
+        bad += std::memcmp(&a, &b, sizeof(float)) != 0;
+        ++n;
+    }
+    *checked = n;
+    return bad;
+}
+
 // Random insertion sequences into a set sitting in front of a guard region:
 // returns how many insertions left more than 16 sections or wrote past the
 // set.  (The marcher keeps one set per warp in shared memory, next to other

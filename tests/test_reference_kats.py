@@ -423,6 +423,19 @@ def test_oracle_and_product_elementary_functions_agree(shim, which):
     assert total > 16_000_000
 
 
+def test_erf_reciprocal_is_the_correctly_rounded_division(shim):
+    """erf_f's 7.1.26 branch takes 1 / (1 + 0.3275911 |x|) for 1 <= |x| < 3.92
+    from fused multiply-adds (recip_hastings): for every float in a range that
+    holds all those divisors it must equal 1.0f / d bit for bit, so erf_f gives
+    the same bits as with the division (and as the oracle, which divides)."""
+    f = shim.kat_recip_mismatches
+    f.restype = C.c_long
+    f.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_long)]
+    n = C.c_long(0)
+    assert f(1.326, 2.286, C.byref(n)) == 0
+    assert n.value > 6_000_000
+
+
 @pytest.mark.parametrize("suffix", ["f32", "f64"])
 def test_insertions_claimed_unchanged_leave_the_set_unchanged(shim, suffix):
     """The volume marcher skips a section insertion that
