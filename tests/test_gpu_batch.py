@@ -11,7 +11,7 @@ from differentiable_gaussian_mixture_renderer_b200 import splat
 
 pytestmark = pytest.mark.gpu
 
-RES = [(64, 48), (96, 96), (80, 128), (128, 72), (48, 64)]
+RES = [(64, 48), (96, 96), (83, 125), (128, 72), (48, 64)]  # 83 x 125: partial blend blocks at the edges
 
 
 def _setup(cuda):

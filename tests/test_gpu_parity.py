@@ -100,9 +100,12 @@ def test_splat_pair_overflow_is_flagged(cuda):
     assert np.abs(fb2.cpu().numpy() - ref["fb"]).max() <= IMAGE_TOL
 
 
-def test_splat_backward_matches_oracle(cuda):
+# 150 x 93: the frame's last tile row and column hold partial 8x8 blend blocks
+# and whole blocks outside the frame
+@pytest.mark.parametrize("w,h", [(160, 128), (150, 93)])
+def test_splat_backward_matches_oracle(cuda, w, h):
     sc = S.make_scene(4000, seed=5, extent=1.0, sh_degree=2)
-    cam = S.make_camera(160, 128, eye=(0.4, -0.3, -3.0))
+    cam = S.make_camera(w, h, eye=(0.4, -0.3, -3.0))
     rng = np.random.default_rng(2)
     G = rng.normal(size=(3, cam.height, cam.width)).astype(np.float32)
     bg = (0.1, 0.2, 0.3)
