@@ -329,7 +329,7 @@ __device__ __forceinline__ uint32_t warp_same_digit(uint32_t d, bool valid, uint
 }
 
 // Stable scatter: warp w of a tile owns a contiguous 256-item slice and ranks
-// its items in order with __match_any_sync, so equal digits keep input order.
+// its items in order (warp_same_digit's ballots), so equal digits keep input order.
 // The tile is first rearranged in shared memory into digit order, then written
 // out so that consecutive threads store consecutive addresses of each digit's
 // run (coalesced), instead of every lane storing into a different bucket.
