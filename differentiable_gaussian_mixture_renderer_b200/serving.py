@@ -366,7 +366,7 @@ class ContinuousServer:
     """Continuous batching of render and gradient requests over resident scenes."""
 
     def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
-                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3):
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 2.0):
         self.device = torch.device(device or "cuda")
         self.scenes = scenes
         self.lib = N.lib()
@@ -584,7 +584,7 @@ class NativeServer:
     completed request's results equal the plain call's."""
 
     def __init__(self, scenes: dict, device=None, n_slots: int = 4, max_batch: int = 8,
-                 hbm_budget_bytes: int | None = None, capacity_margin: float = 1.3, max_batch_pixels: int = 0):
+                 hbm_budget_bytes: int | None = None, capacity_margin: float = 2.0, max_batch_pixels: int = 0):
         self.device = torch.device(device or "cuda")
         self.lib = N.lib()
         cfg = N.ServerConfig(self.device.index if self.device.index is not None else torch.cuda.current_device(),

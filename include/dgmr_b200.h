@@ -417,7 +417,7 @@ typedef struct dgmr_server_config {
     int32_t max_views; /* views per batch, <= DGMR_BATCH_MAX_VIEWS (0 = 8) */
     int32_t reserved;
     size_t hbm_budget_bytes; /* device memory held for work in flight (0 = 80 % of free memory at creation) */
-    double capacity_margin; /* pair capacity = pairs seen x margin + 1024 (<= 0 = 1.3; below 1 forces re-renders) */
+    double capacity_margin; /* pair capacity = pairs seen x margin + 1024 (<= 0 = 2.0; below 1 forces re-renders) */
     int64_t max_batch_pixels; /* a batch takes no further view once its pixels would pass this (0 = no limit; a
                                  batch always takes one); large frames gain nothing from sharing a launch sequence */
 } dgmr_server_config;
